@@ -1,0 +1,335 @@
+#!/usr/bin/env python3
+"""Steady solves per second on the drag-curve sweep, on N GPUs.
+
+Workload (one step): the 16 cases of the drag curve - a tangent ogive of
+fineness 3 on a 4-caliber cylinder at Mach 1.5, 1.6, ..., 3.0, 160 x 80 cells
+each - every case marched from the free stream by LU-SGS at CFL 5 until its
+RMS density residual d(rho)/dt (the reference's densityResidualNorm, FP64) is
+at most 1e-6. The cases are independent: with N GPUs every rank solves its
+own copy of the sweep (weak scaling, no data-path collective).
+
+`value` is the device time of the solves (CUDA events on the library's
+stream, inputs resident in HBM, L2 flushed between steps); `e2e` is the same
+throughput through the public batch API with the host-to-device upload of the
+starting field and the device-to-host read of each case's drag inside the
+timed region. `--impl reference` times the CPU restatement of the reference's
+FP64 engine (the oracle) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "steady solves/s to RMS density residual 1e-6 (drag curve, LU-SGS CFL 5)"
+UNIT = "solves/s"
+TOLERANCE = 1e-6
+CFL = 5.0
+OMEGA = 1.5
+MAX_STEPS = 20000
+CHECK_EVERY = 20
+# Algorithmic bytes per cell of each LU-SGS kernel launch: every array
+# element a pass reads or writes, counted once (FP64 state, FP32 LU-SGS
+# arrays, float4 face metrics), halo re-reads not counted.
+#   residual/diagonal pass: state 32 + i-face 16 + j-face 16 + cell 8
+#                           + residual 16 + state copy 16 + diagonal 4 = 108
+#   sweeps: forward  residual 16 + state copy 16 + diagonal 4 + faces 32
+#                    + dQ* 16 = 84
+#           backward dQ* 16 + state copy 16 + diagonal 4 + faces 32
+#                    + state read 32 + state write 32 = 132
+BYTES_PREPARE = 108
+BYTES_SWEEP = 216
+
+
+def workload_config() -> dict:
+    return {
+        "workload": "drag curve: tangent ogive fineness 3 + 4-caliber cylinder, "
+                    "Mach 1.5..3.0 step 0.1 (16 cases), 160x80 cells each, "
+                    "LU-SGS CFL 5 omega 1.5 from free stream to RMS d(rho)/dt <= 1e-6",
+        "cases_per_gpu": 16,
+        "grid": "160x80",
+        "precision": "FP64 state and residual; FP32 metrics and LU-SGS operator",
+        "l2": "flushed between timed steps (512 MiB device write)",
+        "scheme": "HLLC, van Albada with scaled shared factor (MUSCL), axisymmetric",
+    }
+
+
+def dist_env() -> tuple[int, int, int]:
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class Clocks:
+    """nvidia-smi clock and throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_solve(cases, threads: int) -> tuple[float, list[float], list[int]]:
+    """The FP64 oracle (CPU restatement of the reference engine) on the same
+    cases, one case per host thread; returns (seconds, drags, steps)."""
+    from oracle.oracle import OracleEuler2D, parallel_solve
+
+    engines = []
+    for c in cases:
+        o = OracleEuler2D(c.config)
+        o.set_uniform(c.free.state)
+        engines.append(o)
+    t0 = time.perf_counter()
+    status, steps, res, init = parallel_solve(engines, "lusgs", TOLERANCE, MAX_STEPS, CHECK_EVERY,
+                                              cfl=CFL, omega=OMEGA, relative=False, threads=threads)
+    dt = time.perf_counter() - t0
+    drags = [o.forebody_drag(c.free.pressure, c.free.dynamic_pressure, c.body.nose.base_radius)
+             for o, c in zip(engines, cases)]
+    return dt, drags, [int(s) for s in steps]
+
+
+def run_reference(args, world, rank) -> None:
+    if rank != 0:
+        return
+    from bowshock_b200.workloads import drag_sweep_cases
+
+    cases = drag_sweep_cases()
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_solve(cases, threads)
+    times = []
+    for _ in range(args.steps):
+        dt, _, _ = cpu_solve(cases, threads)
+        times.append(dt)
+    total = sum(times)
+    value = len(cases) * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": "the full 16-case sweep per step, one case per host thread "
+                                   "(C++ FP64 restatement of src/engine-cpu/euler2d.ts)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args, world, rank, local) -> None:
+    import torch
+    import torch.distributed as dist
+
+    from bowshock_b200 import _native
+    from bowshock_b200.batch import CudaBatch
+    from bowshock_b200.workloads import drag_sweep_cases
+
+    torch.cuda.set_device(local)
+    lib = _native.load()
+    _native.check(lib.bs_set_device(local), lib)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    cases = drag_sweep_cases()
+    n = len(cases)
+    batch = CudaBatch([c.config for c in cases], precision=64)
+    flush = torch.empty(512 * 2**20 // 4, dtype=torch.int32, device=f"cuda:{local}")
+    start_fields = [np.tile(np.array([c.free.state.rho, c.free.state.u, c.free.state.v,
+                                      c.free.state.p]), c.config.grid.ni * c.config.grid.nj)
+                    for c in cases]
+
+    def one_step() -> tuple[float, int, list]:
+        batch.set_free_stream()
+        res = batch.solve("lusgs", TOLERANCE, relative=False, max_steps=MAX_STEPS,
+                          check_every=CHECK_EVERY, cfl=CFL, omega=OMEGA)
+        ms, launches = batch.last_solve_timing()
+        return ms, launches, res
+
+    for _ in range(args.warmup):
+        one_step()
+    # Timed region: device time of each solve, L2 flushed between steps.
+    clocks = Clocks(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    device_ms = []
+    launches = 0
+    results = None
+    for _ in range(args.steps):
+        flush.fill_(0)
+        torch.cuda.synchronize()
+        ms, nl, results = one_step()
+        device_ms.append(ms)
+        launches += nl
+    torch.cuda.synchronize()
+    barrier()
+    clock_info = clocks.stop()
+    total_ms = sum(device_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * n * args.steps / (total_ms / 1000)
+    converged = all(r.status == 0 for r in results)
+    steps_taken = [r.steps for r in results]
+
+    # End to end through the public API: upload the starting field from host
+    # memory, solve, read back every case's drag.
+    h2d = sum(f.nbytes for f in start_fields)
+    d2h = n * 8 + n * 32
+    barrier()
+    torch.cuda.synchronize()
+    e2e_times = []
+    drags = []
+    for _ in range(args.steps):
+        flush.fill_(0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k, f in enumerate(start_fields):
+            batch.set_primitives(k, f)
+        batch.solve("lusgs", TOLERANCE, relative=False, max_steps=MAX_STEPS,
+                    check_every=CHECK_EVERY, cfl=CFL, omega=OMEGA)
+        drags = [batch.forebody_drag(k, c.free, c.body.nose.base_radius) for k, c in enumerate(cases)]
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_total = sum(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_total], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * n * args.steps / e2e_total
+
+    # Roofline of the dominant kernel, timed with CUDA events on the
+    # library's stream over the same solve from the free stream.
+    batch.set_free_stream()
+    prep_ms, sweep_ms = batch.kernel_times("lusgs", CFL, OMEGA, iterations=50)
+    cells = sum(c.config.grid.ni * c.config.grid.nj for c in cases)
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    kernels = {
+        "lusgs_sweep": (sweep_ms, BYTES_SWEEP * cells),
+        "lusgs_prepare": (prep_ms, BYTES_PREPARE * cells),
+    }
+    dominant = max(kernels, key=lambda k: kernels[k][0])
+    kms, kbytes = kernels[dominant]
+    achieved = kbytes / (kms / 1000) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        try:
+            traffic = json.loads(tfile.read_text()).get(dominant)
+        except ValueError:
+            traffic = None
+
+    if rank == 0:
+        cpu = None
+        cd_err = None
+        if world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            sec, cpu_drags, cpu_steps = cpu_solve(cases, threads)
+            cpu = {"value": n / sec, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"the full 16-case sweep once ({sum(cpu_steps)} LU-SGS steps), one "
+                             "case per host thread (C++ FP64 restatement of the reference engine)"}
+            cd_err = max(abs(a / b - 1) for a, b in zip(drags, cpu_drags))
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_config(),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": hbm,
+                         "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": traffic,
+                         "kernel_ms": {k: v[0] for k, v in kernels.items()},
+                         "bytes_per_cell": {"lusgs_sweep": BYTES_SWEEP, "lusgs_prepare": BYTES_PREPARE}},
+            "cpu_baseline": cpu,
+            "clocks": clock_info,
+            "accuracy": {"converged": converged, "lusgs_steps": steps_taken,
+                         "cd_max_rel_err_vs_fp64_oracle": cd_err},
+        }
+        print(json.dumps(line), flush=True)
+    batch.destroy()
+    del flush
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    run_gpu(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,141 @@
+"""Loads lib/libbowshock_b200.so and declares its C entry points
+(include/bowshock.h). Raises if the library has not been built: there is no
+fallback implementation."""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+from . import abi
+
+LIB_DIR = Path(__file__).resolve().parent / "lib"
+LIB_PATH = LIB_DIR / "libbowshock_b200.so"
+
+
+class NativeLibraryMissing(ImportError):
+    pass
+
+
+class BowshockError(RuntimeError):
+    """A failed C entry point: `status` is its bs_status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{abi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class NonPhysicalStateError(BowshockError):
+    """The reference's NonPhysicalStateError (src/solver/errors.ts:2)."""
+
+
+class GridQualityError(BowshockError):
+    """The reference's GridQualityError (src/grid/body-grid.ts:57-59)."""
+
+
+class BusyError(BowshockError):
+    """An overlapping call on the same engine (ExclusiveRunner,
+    src/engine-gpu/gpu-common.ts:122-140)."""
+
+
+class NotConvergedError(BowshockError):
+    pass
+
+
+_ERRORS = {
+    abi.BS_NON_PHYSICAL: NonPhysicalStateError,
+    abi.BS_GRID_QUALITY: GridQualityError,
+    abi.BS_BUSY: BusyError,
+    abi.BS_NOT_CONVERGED: NotConvergedError,
+}
+
+_lib: C.CDLL | None = None
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+_vp = C.c_void_p
+
+# name -> argument types; every one returns bs_status.
+SIGNATURES: dict[str, list] = {
+    "bs_device_count": [_ip],
+    "bs_set_device": [C.c_int32],
+    "bs_engine_create": [C.POINTER(abi.Config), _dp, _dp, C.POINTER(_vp)],
+    "bs_engine_create_ex": [C.POINTER(abi.Config), _dp, _dp, C.c_int32, C.POINTER(_vp)],
+    "bs_engine_time_steps": [_vp, _dp],
+    "bs_engine_destroy": [_vp],
+    "bs_engine_centroids": [_vp, _dp, _dp],
+    "bs_engine_set_primitives": [_vp, _dp],
+    "bs_engine_iterate": [_vp, C.c_int32],
+    "bs_engine_set_implicit_cfl": [_vp, C.c_double],
+    "bs_engine_iterate_implicit": [_vp, C.c_int32, C.c_double, C.c_double, C.c_double],
+    "bs_engine_density_residual_norm": [_vp, _dp],
+    "bs_engine_residual": [_vp, _dp],
+    "bs_engine_boundary_fluxes": [_vp, C.c_int32, C.POINTER(abi.FaceFlux)],
+    "bs_engine_forebody_drag": [_vp, C.c_double, C.c_double, C.c_double, _dp],
+    "bs_engine_read_state": [_vp, _fp],
+    "bs_engine_read_primitives": [_vp, _dp],
+    "bs_engine_steps": [_vp, C.POINTER(C.c_int64)],
+    "bs_engine_solve": [_vp, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32,
+                        C.c_int32, C.c_int32, C.POINTER(abi.SolveResult)],
+    "bs_batch_create": [C.c_int32, C.POINTER(abi.Config), C.POINTER(_dp), C.POINTER(_dp),
+                        C.c_int32, C.POINTER(_vp)],
+    "bs_batch_destroy": [_vp],
+    "bs_batch_size": [_vp, _ip],
+    "bs_batch_set_primitives": [_vp, C.c_int32, _dp],
+    "bs_batch_set_free_stream": [_vp],
+    "bs_batch_solve": [_vp, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                       C.c_int32, C.POINTER(abi.SolveResult)],
+    "bs_batch_forebody_drag": [_vp, C.c_int32, C.c_double, C.c_double, C.c_double, _dp],
+    "bs_batch_read_primitives": [_vp, C.c_int32, _dp],
+    "bs_batch_density_residual_norms": [_vp, _dp],
+    "bs_batch_last_solve_timing": [_vp, _dp, C.POINTER(C.c_int64)],
+    "bs_batch_kernel_times": [_vp, C.c_int32, C.c_double, C.c_double, C.c_int32, _dp],
+    "bs_body_grid": [C.POINTER(abi.Body), C.POINTER(abi.BodyGridOptions), C.POINTER(_vp)],
+    "bs_ramp_grid": [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
+                     C.c_double, C.POINTER(_vp)],
+    "bs_grid_dims": [_vp, _ip, _ip],
+    "bs_grid_nodes": [_vp, _dp, _dp],
+    "bs_grid_info": [_vp, _ip, _dp],
+    "bs_grid_destroy": [_vp],
+    "bs_grid_quality_of": [C.c_int32, C.c_int32, _dp, _dp, C.POINTER(abi.GridQuality)],
+    "bs_taylor_maccoll": [C.c_double, C.c_double, C.c_double, C.c_double,
+                          C.POINTER(abi.ConeFlow)],
+    "bs_oblique_shock": [C.c_double, C.c_double, C.c_double, C.POINTER(abi.Shock)],
+    "bs_normal_shock": [C.c_double, C.c_double, C.POINTER(abi.Shock)],
+}
+
+
+def _declare(lib: C.CDLL) -> None:
+    lib.bs_last_error.restype = C.c_char_p
+    lib.bs_last_error.argtypes = []
+    lib.bs_version.restype = C.c_char_p
+    lib.bs_version.argtypes = []
+    for name, args in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = C.c_int
+
+
+def load(path: Path | str | None = None) -> C.CDLL:
+    """The native library, loaded once. Raises NativeLibraryMissing if it has
+    not been built (python -c 'import __graft_entry__; __graft_entry__.build()')."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise NativeLibraryMissing(
+            f"{p} is missing: build the CUDA library first (bowshock_b200.build.build())"
+        )
+    lib = C.CDLL(str(p))
+    _declare(lib)
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def check(status: int, lib: C.CDLL | None = None) -> None:
+    if status != abi.BS_OK:
+        L = lib or load()
+        message = L.bs_last_error().decode()
+        raise _ERRORS.get(status, BowshockError)(status, message)

@@ -1,0 +1,99 @@
+"""Many cases of uneven size solved together on one GPU: every launch covers
+all active cases, and each case stops at its own tolerance."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native, abi
+from .config import Euler2DConfig, FreeStream
+
+_dp = C.POINTER(C.c_double)
+
+
+class CudaBatch:
+    def __init__(self, configs: list[Euler2DConfig], precision: int = 64):
+        self._lib = _native.load()
+        self.configs = list(configs)
+        n = len(self.configs)
+        self._abi = (abi.Config * n)(*[c.to_abi() for c in self.configs])
+        self._xs = [c.grid.x for c in self.configs]
+        self._ys = [c.grid.y for c in self.configs]
+        xs = (_dp * n)(*[x.ctypes.data_as(_dp) for x in self._xs])
+        ys = (_dp * n)(*[y.ctypes.data_as(_dp) for y in self._ys])
+        h = C.c_void_p()
+        _native.check(self._lib.bs_batch_create(n, self._abi, xs, ys, precision, C.byref(h)), self._lib)
+        self._h = h
+        self.n = n
+
+    def destroy(self) -> None:
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _native.check(self._lib.bs_batch_destroy(h), self._lib)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+    def _call(self, name: str, *args) -> None:
+        if self._h is None:
+            raise RuntimeError("the batch has been destroyed")
+        _native.check(getattr(self._lib, name)(self._h, *args), self._lib)
+
+    def set_free_stream(self) -> None:
+        self._call("bs_batch_set_free_stream")
+
+    def set_primitives(self, c: int, w: np.ndarray) -> None:
+        w = np.ascontiguousarray(w, dtype=np.float64).reshape(-1)
+        g = self.configs[c].grid
+        if w.size != 4 * g.ni * g.nj:
+            raise ValueError("four values per cell are needed")
+        self._call("bs_batch_set_primitives", c, w.ctypes.data_as(_dp))
+
+    def solve(self, method: str = "lusgs", tolerance: float = 1e-6, relative: bool = False,
+              max_steps: int = 100000, check_every: int = 20, cfl: float = 5.0,
+              omega: float = 1.5) -> list[abi.SolveResult]:
+        out = (abi.SolveResult * self.n)()
+        self._call("bs_batch_solve", 1 if method == "lusgs" else 0, cfl, omega, tolerance,
+                   1 if relative else 0, max_steps, check_every, out)
+        return list(out)
+
+    def forebody_drag(self, c: int, free: FreeStream, base_radius: float) -> float:
+        cd = C.c_double()
+        self._call("bs_batch_forebody_drag", c, free.pressure, free.dynamic_pressure,
+                   float(base_radius), C.byref(cd))
+        return cd.value
+
+    def primitives(self, c: int) -> np.ndarray:
+        g = self.configs[c].grid
+        w = np.empty(4 * g.ni * g.nj)
+        self._call("bs_batch_read_primitives", c, w.ctypes.data_as(_dp))
+        return w.reshape(-1, 4)
+
+    def residual_norms(self) -> np.ndarray:
+        r = np.empty(self.n)
+        self._call("bs_batch_density_residual_norms", r.ctypes.data_as(_dp))
+        return r
+
+    def last_solve_timing(self) -> tuple[float, int]:
+        ms = C.c_double()
+        launches = C.c_int64()
+        self._call("bs_batch_last_solve_timing", C.byref(ms), C.byref(launches))
+        return ms.value, launches.value
+
+    def kernel_times(self, method: str = "lusgs", cfl: float = 5.0, omega: float = 1.5,
+                     iterations: int = 20) -> tuple[float, float]:
+        ms = np.empty(2)
+        self._call("bs_batch_kernel_times", 1 if method == "lusgs" else 0, cfl, omega, iterations,
+                   ms.ctypes.data_as(_dp))
+        return float(ms[0]), float(ms[1])

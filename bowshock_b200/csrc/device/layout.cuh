@@ -1,0 +1,147 @@
+// Device data layout of a batch of cases (one engine is a batch of one).
+//
+// Every case's arrays live in shared arenas at per-case offsets:
+//   state      SoA, one array per conserved component (rho, rho u, rho v, E),
+//              ni nj cells of the case at `cell`, cell (i, j) at i + j ni;
+//   i-faces    float4 (nx, ny, area, 0), (ni + 1) nj at `iface`;
+//   j-faces    float4 (nx, ny, area, 0), ni (nj + 1) at `jface`;
+//   cells      float2 (volume, planar area) at `cell`.
+// Metrics are computed in FP64 on the host and stored as FP32. The state is
+// stored in the solve's arithmetic type R: double for the steady solves
+// (the residual that decides convergence is evaluated in FP64), float for
+// the reference GPU engine's all-FP32 arithmetic.
+#pragma once
+
+#include <cstdint>
+
+#include "scheme.cuh"
+
+namespace bsd {
+
+// Tile of the fused cell kernels: TI cells along i by TJ along j, one
+// thread per cell.
+constexpr int TI = 32;
+constexpr int TJ = 8;
+constexpr int TILE_THREADS = TI * TJ;
+
+// Per-case status bits.
+constexpr unsigned STATUS_NON_PHYSICAL = 1u;
+
+struct CaseDev {
+  int32_t ni, nj;
+  int64_t cell;   // offset of the case's cell arrays
+  int64_t iface;  // offset of its i-face arrays
+  int64_t jface;  // offset of its j-face arrays
+  int32_t bc[4];  // bs_bc_kind per side
+  int32_t flux, limiter, recon, axisym;
+  int32_t integrator, local_dt;
+  double gamma;   // rounded to FP32 for FP32 cases
+  double cfl;     // explicit CFL number
+  double inflow_prim[4][4];  // (rho, u, v, p) outside each inflow / far-field side
+  double inflow_cons[4][4];  // the same as conserved variables
+};
+
+template <class R>
+struct StateView {
+  R* rho;
+  R* mu;
+  R* mv;
+  R* e;
+  __device__ __forceinline__ Cons<R> load(int64_t k) const { return {rho[k], mu[k], mv[k], e[k]}; }
+  __device__ __forceinline__ void store(int64_t k, const Cons<R>& q) const {
+    rho[k] = q.rho;
+    mu[k] = q.mu;
+    mv[k] = q.mv;
+    e[k] = q.e;
+  }
+};
+
+struct MetricsView {
+  const float4* iface;  // (nx, ny, area, 0)
+  const float4* jface;
+  const float2* cell;   // (volume, planar area)
+};
+
+// The conserved state of cell (i, j) of a case, for i in [-2, ni + 1] with j in
+// range or j in [-2, nj + 1] with i in range: interior cells from `at(k)`,
+// ghost cells from the side's boundary condition as fillGhosts builds them
+// (src/engine-cpu/euler2d.ts:1361-1423): ghost layer g mirrors interior
+// layer g (outflow, wall with the momentum reflected about the boundary
+// face), wraps (periodic), or holds the inflow / far-field state.
+// `inflow_from_prim` rebuilds the inflow ghost from its primitives with this
+// gamma instead of using the stored conserved copy.
+template <class R, class At>
+__device__ __forceinline__ Cons<R> cell_or_ghost(const CaseDev& cd, const MetricsView& m, int i,
+                                                 int j, R gamma, bool inflow_from_prim, At&& at) {
+  const int ni = cd.ni, nj = cd.nj;
+  if (i >= 0 && i < ni && j >= 0 && j < nj) return at(cd.cell + i + int64_t(j) * ni);
+  int side, mi, mj, wi, wj, ii, ij;
+  float4 f;
+  if (i < 0) {
+    side = BS_IMIN;
+    mi = -1 - i; mj = j; wi = i + ni; wj = j; ii = 0; ij = j;
+    f = m.iface[cd.iface + int64_t(j) * (ni + 1)];
+  } else if (i >= ni) {
+    side = BS_IMAX;
+    mi = 2 * ni - 1 - i; mj = j; wi = i - ni; wj = j; ii = ni - 1; ij = j;
+    f = m.iface[cd.iface + ni + int64_t(j) * (ni + 1)];
+  } else if (j < 0) {
+    side = BS_JMIN;
+    mi = i; mj = -1 - j; wi = i; wj = j + nj; ii = i; ij = 0;
+    f = m.jface[cd.jface + i];
+  } else {
+    side = BS_JMAX;
+    mi = i; mj = 2 * nj - 1 - j; wi = i; wj = j - nj; ii = i; ij = nj - 1;
+    f = m.jface[cd.jface + i + int64_t(nj) * ni];
+  }
+  const int kind = cd.bc[side];
+  if (kind == BS_BC_INFLOW) {
+    if (inflow_from_prim) {
+      const double* s = cd.inflow_prim[side];
+      return to_cons(Prim<R>{R(s[0]), R(s[1]), R(s[2]), R(s[3])}, gamma);
+    }
+    const double* s = cd.inflow_cons[side];
+    return {R(s[0]), R(s[1]), R(s[2]), R(s[3])};
+  }
+  if (kind == BS_BC_FAR_FIELD) {
+    // Both ghost layers take the face's state from the first interior cell.
+    const Prim<R> inside = to_prim(at(cd.cell + ii + int64_t(ij) * ni), gamma);
+    const double* s = cd.inflow_prim[side];
+    const Prim<R> fr{R(s[0]), R(s[1]), R(s[2]), R(s[3])};
+    const R sgn = (side == BS_IMIN || side == BS_JMIN) ? R(-1) : R(1);
+    return to_cons(far_field_state(inside, fr, sgn * R(f.x), sgn * R(f.y), gamma), gamma);
+  }
+  if (kind == BS_BC_PERIODIC) return at(cd.cell + wi + int64_t(wj) * ni);
+  Cons<R> c = at(cd.cell + mi + int64_t(mj) * ni);
+  if (kind == BS_BC_WALL) {
+    const R nx = R(f.x), ny = R(f.y);
+    const R mn = c.mu * nx + c.mv * ny;
+    c.mu = c.mu - R(2) * mn * nx;
+    c.mv = c.mv - R(2) * mn * ny;
+  }
+  return c;
+}
+
+template <class R>
+__device__ __forceinline__ Cons<R> load_cell(const CaseDev& cd, const StateView<R>& q,
+                                             const MetricsView& m, int i, int j) {
+  return cell_or_ghost<R>(cd, m, i, j, R(cd.gamma), false,
+                          [&](int64_t k) { return q.load(k); });
+}
+
+// -1 / +1 when face index `at` on a line of `n` cells is a wall face on the
+// minimum / maximum side, else 0.
+__device__ __forceinline__ int wall_side(const CaseDev& cd, int at, int n, int min_side,
+                                         int max_side) {
+  if (at == 0 && cd.bc[min_side] == BS_BC_WALL) return -1;
+  if (at == n && cd.bc[max_side] == BS_BC_WALL) return 1;
+  return 0;
+}
+
+// Warp-level FP64 sum; lane 0 holds the result.
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace bsd

@@ -1,0 +1,147 @@
+// C ABI of the host-side grid generator and exact solutions.
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "../common.hpp"
+#include "bowshock.h"
+#include "gasdyn.hpp"
+#include "grids.hpp"
+
+struct bs_grid {
+  bs::Grid g;
+};
+
+namespace {
+
+bs::Body to_body(const bs_body& b) {
+  bs::Body body;
+  body.nose.kind = b.nose_kind;
+  body.nose.parameter = b.parameter;
+  body.nose.length = b.nose_length;
+  body.nose.base_radius = b.base_radius;
+  body.cylinder_length = b.cylinder_length;
+  return body;
+}
+
+}  // namespace
+
+extern "C" {
+
+bs_status bs_body_grid(const bs_body* body, const bs_body_grid_options* options, bs_grid** out) {
+  if (body == nullptr || options == nullptr || out == nullptr)
+    return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  bs::BodyGridOptions o;
+  o.nj = options->nj;
+  o.refinement = options->refinement <= 0 ? 1 : options->refinement;
+  o.ni = options->ni;
+  o.mach = options->mach;
+  o.gamma = options->gamma;
+  auto* g = new (std::nothrow) bs_grid;
+  if (g == nullptr) return bs::fail(BS_MEMORY_LIMIT, "out of host memory");
+  bool quality = false;
+  const std::string e = bs::body_grid(to_body(*body), o, &g->g, &quality);
+  if (!e.empty()) {
+    delete g;
+    return bs::fail(quality ? BS_GRID_QUALITY : BS_INVALID_ARGUMENT, e);
+  }
+  *out = g;
+  return bs::ok();
+}
+
+bs_status bs_ramp_grid(int32_t ni, int32_t nj, double x_min, double x_corner, double x_max,
+                       double height, double angle, bs_grid** out) {
+  if (out == nullptr || ni < 1 || nj < 1) return bs::fail(BS_INVALID_ARGUMENT, "invalid argument");
+  auto* g = new (std::nothrow) bs_grid;
+  if (g == nullptr) return bs::fail(BS_MEMORY_LIMIT, "out of host memory");
+  const std::string e = bs::ramp_grid(ni, nj, x_min, x_corner, x_max, height, angle, &g->g);
+  if (!e.empty()) {
+    delete g;
+    return bs::fail(BS_INVALID_ARGUMENT, e);
+  }
+  *out = g;
+  return bs::ok();
+}
+
+bs_status bs_grid_dims(const bs_grid* grid, int32_t* ni, int32_t* nj) {
+  if (grid == nullptr || ni == nullptr || nj == nullptr)
+    return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  *ni = grid->g.ni;
+  *nj = grid->g.nj;
+  return bs::ok();
+}
+
+bs_status bs_grid_nodes(const bs_grid* grid, double* x, double* y) {
+  if (grid == nullptr || x == nullptr || y == nullptr)
+    return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  std::memcpy(x, grid->g.x.data(), grid->g.x.size() * sizeof(double));
+  std::memcpy(y, grid->g.y.data(), grid->g.y.size() * sizeof(double));
+  return bs::ok();
+}
+
+bs_status bs_grid_info(const bs_grid* grid, int32_t* i_tip, double* outer_angle) {
+  if (grid == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  if (i_tip) *i_tip = grid->g.i_tip;
+  if (outer_angle) *outer_angle = grid->g.outer_angle;
+  return bs::ok();
+}
+
+bs_status bs_grid_destroy(bs_grid* grid) {
+  delete grid;
+  return bs::ok();
+}
+
+bs_status bs_grid_quality_of(int32_t ni, int32_t nj, const double* x, const double* y,
+                             bs_grid_quality* out) {
+  if (x == nullptr || y == nullptr || out == nullptr || ni < 1 || nj < 1)
+    return bs::fail(BS_INVALID_ARGUMENT, "invalid argument");
+  const bs::GridQuality q = bs::grid_quality(ni, nj, x, y);
+  out->min_angle = q.min_angle;
+  out->min_wall_angle = q.min_wall_angle;
+  out->max_size_ratio = q.max_size_ratio;
+  out->max_aspect_ratio = q.max_aspect_ratio;
+  out->min_area = q.min_area;
+  return bs::ok();
+}
+
+bs_status bs_taylor_maccoll(double mach, double cone_angle, double gamma, double tolerance,
+                            bs_cone_flow* out) {
+  if (out == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  bs::ConeFlow f;
+  const std::string e =
+      bs::taylor_maccoll(mach, cone_angle, gamma, tolerance > 0 ? tolerance : 1e-13, &f);
+  if (!e.empty()) return bs::fail(BS_INVALID_ARGUMENT, e);
+  out->shock_angle = f.shock_angle;
+  out->post_shock_mach = f.post_shock_mach;
+  out->post_shock_pressure_ratio = f.post_shock_pressure_ratio;
+  out->surface_mach = f.surface_mach;
+  out->surface_pressure_ratio = f.surface_pressure_ratio;
+  out->surface_pressure_coefficient = f.surface_pressure_coefficient;
+  return bs::ok();
+}
+
+bs_status bs_oblique_shock(double mach, double theta, double gamma, bs_shock* out) {
+  if (out == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  bs::ObliqueShock s;
+  const std::string e = bs::oblique_shock(mach, theta, gamma, &s);
+  if (!e.empty()) return bs::fail(BS_INVALID_ARGUMENT, e);
+  out->beta = s.beta;
+  out->pressure_ratio = s.pressure_ratio;
+  out->density_ratio = s.density_ratio;
+  out->downstream_mach = s.downstream_mach;
+  return bs::ok();
+}
+
+bs_status bs_normal_shock(double mach, double gamma, bs_shock* out) {
+  if (out == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  bs::NormalShock s;
+  const std::string e = bs::normal_shock(mach, gamma, &s);
+  if (!e.empty()) return bs::fail(BS_INVALID_ARGUMENT, e);
+  out->beta = M_PI / 2;
+  out->pressure_ratio = s.pressure_ratio;
+  out->density_ratio = s.density_ratio;
+  out->downstream_mach = s.downstream_mach;
+  return bs::ok();
+}
+
+}  // extern "C"

@@ -1,0 +1,63 @@
+// Structured grids around bodies of revolution and their quality measures:
+// src/grid/body-grid.ts (H topology, sharp noses), src/grid/spacing.ts
+// (column placement), src/grid/quality.ts (quality gates),
+// src/grid/shapes.ts (ramp grids for validation).
+#pragma once
+
+#include <cmath>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "geometry.hpp"
+
+namespace bs {
+
+struct Grid {
+  int ni = 0, nj = 0;
+  std::vector<double> x, y;  // (ni + 1)(nj + 1) nodes, node (i, j) at i + j (ni + 1)
+  int i_tip = 0;
+  double outer_angle = 0;
+};
+
+struct GridQuality {  // src/grid/quality.ts:6-21
+  double min_angle, min_wall_angle, max_size_ratio, max_aspect_ratio, min_area;
+};
+
+struct QualityLimits {  // src/grid/quality.ts:24-38
+  double min_angle = 12 * M_PI / 180;
+  double min_wall_angle = 60 * M_PI / 180;
+  double max_size_ratio = 1.3;
+  double max_aspect_ratio = 10;
+};
+
+GridQuality grid_quality(int ni, int nj, const double* x, const double* y);
+std::vector<std::string> quality_failures(const GridQuality& q, const QualityLimits& limits);
+
+// columnPositions (src/grid/spacing.ts:31-71), without the slope limiter of
+// the blunt grids. When `total` > 0 the whole line gets exactly `total`
+// intervals, apportioned to the breakpoint intervals by their integrated
+// density (largest remainders, at least one each) instead of rounding each
+// interval's own count: the batched configurations name ni exactly.
+std::vector<double> column_positions(const std::vector<double>& breakpoints,
+                                     const std::function<double(double)>& density, int refinement,
+                                     int total);
+
+struct BodyGridOptions {
+  int nj = 20;          // least cells across on the base grid
+  int refinement = 1;   // 1, 2, 4, ...
+  int ni = 0;           // exact cells along the body when > 0 (refinement must be 1)
+  double mach = 2;
+  double gamma = 1.4;
+};
+
+// bodyGrid (src/grid/body-grid.ts:76-181). Returns "" or the error; a grid
+// failing the quality gates sets *quality_error.
+std::string body_grid(const Body& body, const BodyGridOptions& options, Grid* out,
+                      bool* quality_error);
+
+// rampGrid (src/grid/shapes.ts:30-52).
+std::string ramp_grid(int ni, int nj, double x_min, double x_corner, double x_max, double height,
+                      double angle, Grid* out);
+
+}  // namespace bs

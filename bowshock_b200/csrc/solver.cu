@@ -1,0 +1,871 @@
+// GPU solve of a batch of cases: device arenas, kernel launches, CUDA-graph
+// replay of the step loop, convergence checks with one small device-to-host
+// read per check, and the FP64 boundary evaluations.
+#include "solver.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "common.hpp"
+#include "device/sweep.cuh"
+#include "device/tile.cuh"
+#include "device/wall.cuh"
+
+namespace bs {
+
+std::string validate_config(const bs_config& c) {
+  if (!(c.cfl > 0 && c.cfl <= 1)) return "cfl must be in (0, 1]";
+  if (c.ni < 2 || c.nj < 2) return "the grid needs at least 2 x 2 cells";
+  if (c.nj > 512) return "the GPU engine takes at most 512 cells across (nj)";
+  if (c.ni > (1 << 24)) return "too many cells along the grid (ni)";
+  if (!(c.gamma > 1)) return "gamma must exceed 1";
+  if (c.geometry != BS_PLANAR && c.geometry != BS_AXISYMMETRIC) return "unknown geometry";
+  if (c.flux != BS_FLUX_HLLC && c.flux != BS_FLUX_RUSANOV)
+    return "the GPU engine has only the hllc and rusanov fluxes";
+  if (c.limiter < BS_LIMITER_FIRST_ORDER || c.limiter > BS_LIMITER_UNLIMITED_CENTRAL)
+    return "unknown limiter";
+  if (c.reconstruction < BS_RECON_PER_VARIABLE || c.reconstruction > BS_RECON_SHARED_SCALED)
+    return "unknown reconstruction";
+  if ((c.reconstruction == BS_RECON_SHARED || c.reconstruction == BS_RECON_SHARED_SCALED) &&
+      c.limiter != BS_LIMITER_VAN_ALBADA)
+    return "shared reconstruction requires the 'vanAlbada' limiter";
+  if (c.integrator < BS_FORWARD_EULER || c.integrator > BS_SSPRK3) return "unknown time integrator";
+  if (c.time_stepping != BS_TIME_LOCAL && c.time_stepping != BS_TIME_GLOBAL)
+    return "unknown time stepping";
+  for (int s = 0; s < 4; s++) {
+    const bs_boundary& b = c.boundaries[s];
+    if (b.kind < BS_BC_INFLOW || b.kind > BS_BC_PERIODIC) return "unknown boundary kind";
+    if (b.kind == BS_BC_INFLOW || b.kind == BS_BC_FAR_FIELD) {
+      const bs_primitive& w = b.state;
+      if (!(w.rho > 0 && w.p > 0 && std::isfinite(w.u) && std::isfinite(w.v)))
+        return "a boundary state must have positive density and pressure";
+    }
+  }
+  if ((c.boundaries[0].kind == BS_BC_PERIODIC) != (c.boundaries[1].kind == BS_BC_PERIODIC))
+    return "periodic boundaries must be used on both iMin and iMax";
+  if ((c.boundaries[2].kind == BS_BC_PERIODIC) != (c.boundaries[3].kind == BS_BC_PERIODIC))
+    return "periodic boundaries must be used on both jMin and jMax";
+  return "";
+}
+
+namespace {
+
+bs_status cuda_fail(cudaError_t e, const char* what) {
+  cudaGetLastError();  // clear a non-sticky error
+  if (e == cudaErrorMemoryAllocation)
+    return fail(BS_MEMORY_LIMIT, std::string("device memory exhausted (") + what + ")");
+  return fail(BS_EXECUTION, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define BS_CUDA(expr)                                   \
+  do {                                                  \
+    const cudaError_t e_ = (expr);                      \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #expr); \
+  } while (0)
+
+#define BS_TRY(expr)                       \
+  do {                                     \
+    const bs_status s_ = (expr);           \
+    if (s_ != BS_OK) return s_;            \
+  } while (0)
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p != nullptr) cudaFree(p);
+  }
+  cudaError_t alloc(size_t count) {
+    if (p != nullptr) {
+      cudaFree(p);
+      p = nullptr;
+    }
+    n = count;
+    return cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(count, 1) * sizeof(T));
+  }
+};
+
+struct GraphKey {
+  int method, count, norm_last;
+  bool operator<(const GraphKey& o) const {
+    if (method != o.method) return method < o.method;
+    if (count != o.count) return count < o.count;
+    return norm_last < o.norm_last;
+  }
+};
+
+constexpr int kMethodExplicit = 0;
+constexpr int kMethodImplicit = 1;
+
+template <class R>
+class Solver final : public SolverBase {
+ public:
+  explicit Solver(std::vector<HostCase>&& cases) : cases_(std::move(cases)) {}
+
+  ~Solver() override {
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    if (ev0_ != nullptr) cudaEventDestroy(ev0_);
+    if (ev1_ != nullptr) cudaEventDestroy(ev1_);
+    if (stream_ != nullptr) cudaStreamDestroy(stream_);
+  }
+
+  bs_status init() {
+    n_ = int(cases_.size());
+    BS_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    BS_CUDA(cudaEventCreate(&ev0_));
+    BS_CUDA(cudaEventCreate(&ev1_));
+    std::vector<bsd::CaseDev> hc(n_);
+    std::vector<int2> tiles;
+    int64_t cell = 0, ifc = 0, jfc = 0, bfc = 0;
+    boundary_off_.resize(n_);
+    cell_off_.resize(n_);
+    for (int c = 0; c < n_; c++) {
+      cell_off_[c] = cell;
+      const HostCase& h = cases_[c];
+      const bs_config& cfg = h.cfg;
+      bsd::CaseDev& d = hc[c];
+      d.ni = cfg.ni;
+      d.nj = cfg.nj;
+      d.cell = cell;
+      d.iface = ifc;
+      d.jface = jfc;
+      for (int s = 0; s < 4; s++) d.bc[s] = cfg.boundaries[s].kind;
+      d.flux = cfg.flux;
+      d.limiter = cfg.limiter;
+      d.recon = cfg.reconstruction;
+      d.axisym = cfg.geometry == BS_AXISYMMETRIC;
+      d.integrator = cfg.integrator;
+      d.local_dt = cfg.time_stepping == BS_TIME_LOCAL;
+      any_global_dt_ = any_global_dt_ || !d.local_dt;
+      d.gamma = solve_gamma(cfg.gamma);
+      d.cfl = cfg.cfl;
+      for (int s = 0; s < 4; s++) {
+        const bs_primitive& w = cfg.boundaries[s].state;
+        d.inflow_prim[s][0] = w.rho;
+        d.inflow_prim[s][1] = w.u;
+        d.inflow_prim[s][2] = w.v;
+        d.inflow_prim[s][3] = w.p;
+        const double g = d.gamma;
+        d.inflow_cons[s][0] = w.rho;
+        d.inflow_cons[s][1] = w.rho * w.u;
+        d.inflow_cons[s][2] = w.rho * w.v;
+        d.inflow_cons[s][3] = w.p / (g - 1) + 0.5 * w.rho * (w.u * w.u + w.v * w.v);
+      }
+      const int ti = (cfg.ni + bsd::TI - 1) / bsd::TI, tj = (cfg.nj + bsd::TJ - 1) / bsd::TJ;
+      for (int t = 0; t < ti * tj; t++) tiles.push_back(make_int2(c, t));
+      boundary_off_[c] = bfc;
+      bfc += 2 * int64_t(cfg.ni + cfg.nj);
+      cell += int64_t(cfg.ni) * cfg.nj;
+      ifc += int64_t(cfg.ni + 1) * cfg.nj;
+      jfc += int64_t(cfg.ni) * (cfg.nj + 1);
+      max_nj_ = std::max(max_nj_, cfg.nj);
+      max_along_ = std::max(max_along_, std::max(cfg.ni, cfg.nj));
+    }
+    total_cells_ = cell;
+    n_tiles_ = int(tiles.size());
+    steps_.assign(n_, 0);
+    active_h_.assign(n_, 1);
+
+    BS_CUDA(d_cases_.alloc(n_));
+    BS_CUDA(cudaMemcpy(d_cases_.p, hc.data(), n_ * sizeof(bsd::CaseDev), cudaMemcpyHostToDevice));
+    BS_CUDA(d_tiles_.alloc(tiles.size()));
+    BS_CUDA(cudaMemcpy(d_tiles_.p, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    std::vector<int> list(n_);
+    for (int c = 0; c < n_; c++) list[c] = c;
+    BS_CUDA(d_case_list_.alloc(n_));
+    BS_CUDA(cudaMemcpy(d_case_list_.p, list.data(), n_ * sizeof(int), cudaMemcpyHostToDevice));
+    BS_CUDA(d_active_.alloc(n_));
+    BS_CUDA(cudaMemcpy(d_active_.p, active_h_.data(), n_ * sizeof(int), cudaMemcpyHostToDevice));
+    for (int v = 0; v < 4; v++) BS_CUDA(q_[v].alloc(total_cells_));
+    BS_CUDA(dt_.alloc(total_cells_));
+    BS_CUDA(iface_.alloc(ifc));
+    BS_CUDA(jface_.alloc(jfc));
+    BS_CUDA(cellm_.alloc(total_cells_));
+    BS_CUDA(norm_.alloc(n_));
+    BS_CUDA(status_.alloc(n_));
+    BS_CUDA(dtmin_.alloc(n_));
+    BS_CUDA(cfl_.alloc(n_));
+    BS_CUDA(cflmax_.alloc(n_));
+    BS_CUDA(growth_.alloc(n_));
+    BS_CUDA(omega_.alloc(n_));
+    BS_CUDA(bgeom_.alloc(3 * bfc));
+    BS_CUDA(bflux_.alloc(4 * size_t(max_along_)));
+    BS_CUDA(force_.alloc(1));
+    BS_CUDA(cudaMemset(status_.p, 0, n_ * sizeof(unsigned)));
+    std::vector<float> ones(n_, 1.f), fifteen(n_, 1.5f);
+    BS_CUDA(cudaMemcpy(cfl_.p, ones.data(), n_ * sizeof(float), cudaMemcpyHostToDevice));
+    BS_CUDA(cudaMemcpy(cflmax_.p, ones.data(), n_ * sizeof(float), cudaMemcpyHostToDevice));
+    BS_CUDA(cudaMemcpy(growth_.p, ones.data(), n_ * sizeof(float), cudaMemcpyHostToDevice));
+    BS_CUDA(cudaMemcpy(omega_.p, fifteen.data(), n_ * sizeof(float), cudaMemcpyHostToDevice));
+    // Metrics, FP64 on the host, stored FP32 on the device.
+    std::vector<float4> fi, fj;
+    std::vector<float2> cm;
+    std::vector<double> bg(3 * bfc);
+    for (int c = 0; c < n_; c++) {
+      const Metrics64& m = cases_[c].m;
+      const int ni = m.ni, nj = m.nj;
+      fi.resize(size_t(ni + 1) * nj);
+      for (size_t k = 0; k < fi.size(); k++)
+        fi[k] = make_float4(float(m.inx[k]), float(m.iny[k]), float(m.iarea[k]), 0.f);
+      fj.resize(size_t(ni) * (nj + 1));
+      for (size_t k = 0; k < fj.size(); k++)
+        fj[k] = make_float4(float(m.jnx[k]), float(m.jny[k]), float(m.jarea[k]), 0.f);
+      cm.resize(size_t(ni) * nj);
+      for (size_t k = 0; k < cm.size(); k++)
+        cm[k] = make_float2(float(m.volume[k]), float(m.planar[k]));
+      BS_CUDA(cudaMemcpy(iface_.p + hc[c].iface, fi.data(), fi.size() * sizeof(float4),
+                         cudaMemcpyHostToDevice));
+      BS_CUDA(cudaMemcpy(jface_.p + hc[c].jface, fj.data(), fj.size() * sizeof(float4),
+                         cudaMemcpyHostToDevice));
+      BS_CUDA(cudaMemcpy(cellm_.p + hc[c].cell, cm.data(), cm.size() * sizeof(float2),
+                         cudaMemcpyHostToDevice));
+      // FP64 boundary geometry, sides in order iMin, iMax, jMin, jMax.
+      double* g = bg.data() + 3 * boundary_off_[c];
+      for (int s = 0; s < 4; s++) {
+        const int along = s < 2 ? nj : ni;
+        for (int t = 0; t < along; t++) {
+          size_t f;
+          if (s < 2) {
+            f = (s == 0 ? 0 : ni) + size_t(t) * (ni + 1);
+            g[0] = m.inx[f]; g[1] = m.iny[f]; g[2] = m.iarea[f];
+          } else {
+            f = t + size_t(s == 2 ? 0 : nj) * ni;
+            g[0] = m.jnx[f]; g[1] = m.jny[f]; g[2] = m.jarea[f];
+          }
+          g += 3;
+        }
+      }
+    }
+    BS_CUDA(cudaMemcpy(bgeom_.p, bg.data(), bg.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return BS_OK;
+  }
+
+  int n_cases() const override { return n_; }
+  const HostCase& host_case(int c) const override { return cases_[c]; }
+  int64_t steps(int c) const override { return steps_[c]; }
+  cudaStream_t stream() const override { return stream_; }
+  double last_solve_ms() const override { return last_solve_ms_; }
+  int64_t last_solve_launches() const override { return last_solve_launches_; }
+
+  bs_status set_primitives(int c, const double* prim) override {
+    const HostCase& h = cases_[c];
+    const size_t n = size_t(h.cfg.ni) * h.cfg.nj;
+    const double g = solve_gamma(h.cfg.gamma);
+    std::vector<R> comp[4];
+    for (int v = 0; v < 4; v++) comp[v].resize(n);
+    for (size_t k = 0; k < n; k++) {
+      const double rho = prim[4 * k], u = prim[4 * k + 1], v = prim[4 * k + 2], p = prim[4 * k + 3];
+      if (!(rho > 0 && p > 0 && std::isfinite(u) && std::isfinite(v)))
+        return fail(BS_NON_PHYSICAL, "non-physical state for cell " + std::to_string(k) +
+                                         " (i " + std::to_string(k % h.cfg.ni) + ", j " +
+                                         std::to_string(k / h.cfg.ni) + ")");
+      comp[0][k] = R(rho);
+      comp[1][k] = R(rho * u);
+      comp[2][k] = R(rho * v);
+      comp[3][k] = R(p / (g - 1) + 0.5 * rho * (u * u + v * v));
+    }
+    const int64_t off = cell_offset(c);
+    for (int v = 0; v < 4; v++)
+      BS_CUDA(cudaMemcpyAsync(q_[v].p + off, comp[v].data(), n * sizeof(R), cudaMemcpyHostToDevice,
+                              stream_));
+    unsigned zero = 0;
+    BS_CUDA(cudaMemcpyAsync(status_.p + c, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    steps_[c] = 0;
+    return BS_OK;
+  }
+
+  bs_status set_free_stream() override {
+    for (int c = 0; c < n_; c++) {
+      const bs_config& cfg = cases_[c].cfg;
+      int side = -1;
+      for (int s : {BS_JMAX, BS_IMIN, BS_IMAX, BS_JMIN})
+        if (side < 0 && (cfg.boundaries[s].kind == BS_BC_INFLOW ||
+                         cfg.boundaries[s].kind == BS_BC_FAR_FIELD))
+          side = s;
+      if (side < 0) return fail(BS_INVALID_ARGUMENT, "case " + std::to_string(c) + " has no free stream");
+      const bs_primitive& w = cfg.boundaries[side].state;
+      const size_t n = size_t(cfg.ni) * cfg.nj;
+      std::vector<double> prim(4 * n);
+      for (size_t k = 0; k < n; k++) {
+        prim[4 * k] = w.rho;
+        prim[4 * k + 1] = w.u;
+        prim[4 * k + 2] = w.v;
+        prim[4 * k + 3] = w.p;
+      }
+      BS_TRY(set_primitives(c, prim.data()));
+    }
+    return BS_OK;
+  }
+
+  bs_status kernel_times(int method, double cfl, double omega, int iterations, double* ms) override {
+    if (iterations < 1) return fail(BS_INVALID_ARGUMENT, "iterations must be positive");
+    cudaEvent_t ev[4];
+    for (auto& e : ev) BS_CUDA(cudaEventCreate(&e));
+    double sum[2] = {0, 0};
+    bs_status st = BS_OK;
+    if (method == kMethodImplicit) {
+      st = ensure_implicit();
+      if (st == BS_OK) st = set_implicit_params(cfl, omega, 1.0);
+      if (st == BS_OK) st = set_implicit_cfl(cfl);
+    } else {
+      st = ensure_explicit();
+    }
+    for (int it = 0; it < iterations && st == BS_OK; it++) {
+      cudaEventRecord(ev[0], stream_);
+      if (method == kMethodImplicit) {
+        const bsd::StateView<R> q = q_view();
+        st = launch_tile<bsd::MODE_PREPARE>(q, q, q, 0, 1, false, norm_.p, nullptr, false);
+        cudaEventRecord(ev[1], stream_);
+        cudaEventRecord(ev[2], stream_);
+        if (st == BS_OK) st = launch_sweep();
+      } else {
+        const bsd::StateView<R> q = q_view(), s1 = s1_view(), s2 = s2_view();
+        st = launch_tile<bsd::MODE_STAGE>(q, q, s1, 0.0, 1.0, true, norm_.p, nullptr, false);
+        cudaEventRecord(ev[1], stream_);
+        cudaEventRecord(ev[2], stream_);
+        if (st == BS_OK) st = launch_tile<bsd::MODE_STAGE>(s1, q, s2, 0.75, 0.25, false, nullptr, nullptr, false);
+      }
+      cudaEventRecord(ev[3], stream_);
+      const cudaError_t e = cudaEventSynchronize(ev[3]);
+      if (e != cudaSuccess) {
+        st = cuda_fail(e, "kernel timing");
+        break;
+      }
+      float a = 0, b = 0;
+      cudaEventElapsedTime(&a, ev[0], ev[1]);
+      cudaEventElapsedTime(&b, ev[2], ev[3]);
+      sum[0] += a;
+      sum[1] += b;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (st != BS_OK) return st;
+    ms[0] = sum[0] / iterations;
+    ms[1] = sum[1] / iterations;
+    return BS_OK;
+  }
+
+  bs_status iterate(int steps) override {
+    if (steps < 0) return fail(BS_INVALID_ARGUMENT, "steps must be non-negative");
+    BS_TRY(ensure_explicit());
+    BS_TRY(run_steps(kMethodExplicit, steps, false));
+    count_steps(steps);
+    return check_status();
+  }
+
+  bs_status set_implicit_cfl(double cfl) override {
+    if (!(cfl > 0)) return fail(BS_INVALID_ARGUMENT, "the CFL number must be positive");
+    std::vector<float> v(n_, float(cfl));
+    BS_CUDA(cudaMemcpyAsync(cfl_.p, v.data(), n_ * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    return BS_OK;
+  }
+
+  bs_status iterate_implicit(int steps, double cfl_max, double omega, double growth) override {
+    if (steps < 0) return fail(BS_INVALID_ARGUMENT, "steps must be non-negative");
+    if (!(cfl_max > 0 && omega >= 1 && growth >= 1))
+      return fail(BS_INVALID_ARGUMENT, "implicit steps need cfl > 0, omega >= 1 and growth >= 1");
+    BS_TRY(ensure_implicit());
+    BS_TRY(set_implicit_params(cfl_max, omega, growth));
+    BS_TRY(run_steps(kMethodImplicit, steps, false));
+    count_steps(steps);
+    return check_status();
+  }
+
+  bs_status residual_norms(double* norms) override {
+    BS_CUDA(cudaMemsetAsync(norm_.p, 0, n_ * sizeof(double), stream_));
+    BS_TRY(launch_tile<bsd::MODE_RESIDUAL>(q_view(), q_view(), q_view(), 0, 1, false, norm_.p,
+                                           nullptr, true));
+    std::vector<double> s(n_);
+    BS_CUDA(cudaMemcpyAsync(s.data(), norm_.p, n_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    for (int c = 0; c < n_; c++)
+      norms[c] = std::sqrt(s[c] / (double(cases_[c].cfg.ni) * cases_[c].cfg.nj));
+    return BS_OK;
+  }
+
+  bs_status residual(int c, double* out) override {
+    if (res_out_.p == nullptr) BS_CUDA(res_out_.alloc(4 * size_t(total_cells_)));
+    BS_TRY(launch_tile<bsd::MODE_RESIDUAL>(q_view(), q_view(), q_view(), 0, 1, false, nullptr,
+                                           res_out_.p, true));
+    const size_t n = size_t(cases_[c].cfg.ni) * cases_[c].cfg.nj;
+    BS_CUDA(cudaMemcpyAsync(out, res_out_.p + 4 * cell_offset(c), 4 * n * sizeof(double),
+                            cudaMemcpyDeviceToHost, stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    return BS_OK;
+  }
+
+  bs_status time_steps(int c, double* out) override {
+    bsd::dt_kernel<R><<<n_tiles_, bsd::TILE_THREADS, 0, stream_>>>(
+        d_cases_.p, d_tiles_.p, nullptr, q_view(), metrics(), dt_.p, nullptr);
+    BS_CUDA(cudaGetLastError());
+    const size_t n = size_t(cases_[c].cfg.ni) * cases_[c].cfg.nj;
+    std::vector<float> d(n);
+    BS_CUDA(cudaMemcpyAsync(d.data(), dt_.p + cell_offset(c), n * sizeof(float),
+                            cudaMemcpyDeviceToHost, stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    for (size_t k = 0; k < n; k++) out[k] = d[k];
+    return BS_OK;
+  }
+
+  bs_status boundary_fluxes(int c, int side, bs_face_flux* out) override {
+    if (side < 0 || side > 3) return fail(BS_INVALID_ARGUMENT, "unknown side");
+    const HostCase& h = cases_[c];
+    const int ni = h.cfg.ni, nj = h.cfg.nj;
+    const int along = side < 2 ? nj : ni;
+    BS_TRY(launch_boundary(c, side, 0.0, false));
+    std::vector<double> f(4 * size_t(along));
+    BS_CUDA(cudaMemcpyAsync(f.data(), bflux_.p, f.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                            stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    const int outward = (side == BS_IMIN || side == BS_JMIN) ? -1 : 1;
+    const Metrics64& m = h.m;
+    for (int t = 0; t < along; t++) {
+      size_t n0, n1;
+      double nx, ny, area;
+      if (side < 2) {
+        const int i = side == BS_IMIN ? 0 : ni;
+        const size_t fidx = i + size_t(t) * (ni + 1);
+        n0 = fidx;
+        n1 = fidx + ni + 1;
+        nx = m.inx[fidx]; ny = m.iny[fidx]; area = m.iarea[fidx];
+      } else {
+        const int j = side == BS_JMIN ? 0 : nj;
+        const size_t fidx = t + size_t(j) * ni;
+        n0 = t + size_t(j) * (ni + 1);
+        n1 = n0 + 1;
+        nx = m.jnx[fidx]; ny = m.jny[fidx]; area = m.jarea[fidx];
+      }
+      bs_face_flux& o = out[t];
+      o.x = 0.5 * (h.x[n0] + h.x[n1]);
+      o.y = 0.5 * (h.y[n0] + h.y[n1]);
+      o.nx = outward * nx;
+      o.ny = outward * ny;
+      o.area = area;
+      for (int v = 0; v < 4; v++) o.flux[v] = f[4 * t + v];
+    }
+    return BS_OK;
+  }
+
+  bs_status forebody_drag(int c, double p_inf, double q_inf, double base_radius,
+                          double* drag) override {
+    BS_TRY(launch_boundary(c, BS_JMIN, p_inf, true));
+    double force = 0;
+    BS_CUDA(cudaMemcpyAsync(&force, force_.p, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    *drag = (2 * force) / (q_inf * base_radius * base_radius);
+    return BS_OK;
+  }
+
+  bs_status read_state(int c, float* out) override {
+    const size_t n = size_t(cases_[c].cfg.ni) * cases_[c].cfg.nj;
+    std::vector<R> comp[4];
+    BS_TRY(copy_state(c, comp));
+    for (size_t k = 0; k < n; k++)
+      for (int v = 0; v < 4; v++) out[4 * k + v] = float(comp[v][k]);
+    return BS_OK;
+  }
+
+  bs_status read_primitives(int c, double* out) override {
+    const size_t n = size_t(cases_[c].cfg.ni) * cases_[c].cfg.nj;
+    std::vector<R> comp[4];
+    BS_TRY(copy_state(c, comp));
+    const double g = solve_gamma(cases_[c].cfg.gamma);
+    for (size_t k = 0; k < n; k++) {
+      const double rho = comp[0][k], mu = comp[1][k], mv = comp[2][k], e = comp[3][k];
+      out[4 * k] = rho;
+      out[4 * k + 1] = mu / rho;
+      out[4 * k + 2] = mv / rho;
+      out[4 * k + 3] = (g - 1) * (e - (0.5 * (mu * mu + mv * mv)) / rho);
+    }
+    return BS_OK;
+  }
+
+  bs_status solve(int method, double cfl, double omega, double tolerance, int relative,
+                  int max_steps, int check_every, std::vector<CaseResult>& results) override {
+    if (!(tolerance > 0) || max_steps < 0 || check_every < 1)
+      return fail(BS_INVALID_ARGUMENT, "a solve needs tolerance > 0, max_steps >= 0, check_every >= 1");
+    if (method == kMethodImplicit) {
+      if (!(cfl > 0 && omega >= 1))
+        return fail(BS_INVALID_ARGUMENT, "LU-SGS needs cfl > 0 and omega >= 1");
+      BS_TRY(ensure_implicit());
+      BS_TRY(set_implicit_params(cfl, omega, 1.0));
+      BS_TRY(set_implicit_cfl(cfl));
+    } else {
+      BS_TRY(ensure_explicit());
+    }
+    results.assign(n_, CaseResult{});
+    launches_ = 0;
+    BS_CUDA(cudaEventRecord(ev0_, stream_));
+    std::vector<double> r0(n_);
+    BS_TRY(residual_norms(r0.data()));
+    std::vector<double> target(n_);
+    for (int c = 0; c < n_; c++) {
+      results[c].initial_residual = r0[c];
+      results[c].residual = r0[c];
+      target[c] = relative ? tolerance * r0[c] : tolerance;
+      active_h_[c] = r0[c] <= target[c] ? 0 : 1;
+      results[c].status = active_h_[c] ? BS_NOT_CONVERGED : BS_OK;
+    }
+    BS_TRY(upload_active());
+    std::vector<int64_t> taken(n_, 0);
+    std::vector<double> sums(n_);
+    std::vector<unsigned> status(n_);
+    int done = 0;
+    for (int c = 0; c < n_; c++) done += active_h_[c] == 0;
+    int64_t step = 0;
+    while (done < n_ && step < max_steps) {
+      const int chunk = int(std::min<int64_t>(check_every, max_steps - step));
+      BS_CUDA(cudaMemsetAsync(norm_.p, 0, n_ * sizeof(double), stream_));
+      BS_TRY(run_steps(method, chunk, true));
+      step += chunk;
+      BS_CUDA(cudaMemcpyAsync(sums.data(), norm_.p, n_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+      BS_CUDA(cudaMemcpyAsync(status.data(), status_.p, n_ * sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+      BS_CUDA(cudaStreamSynchronize(stream_));
+      bool changed = false;
+      for (int c = 0; c < n_; c++) {
+        if (!active_h_[c]) continue;
+        taken[c] += chunk;
+        steps_[c] += chunk;
+        // The residual of the state at the start of the chunk's last step.
+        const double r = std::sqrt(sums[c] / (double(cases_[c].cfg.ni) * cases_[c].cfg.nj));
+        results[c].residual = r;
+        if (status[c] & bsd::STATUS_NON_PHYSICAL) {
+          results[c].status = BS_NON_PHYSICAL;
+          active_h_[c] = 0;
+        } else if (!(r == r)) {
+          results[c].status = BS_NON_PHYSICAL;
+          active_h_[c] = 0;
+        } else if (r <= target[c]) {
+          results[c].status = BS_OK;
+          active_h_[c] = 0;
+        }
+        if (!active_h_[c]) {
+          done++;
+          changed = true;
+        }
+      }
+      if (changed) BS_TRY(upload_active());
+    }
+    // The exact residual of each final state.
+    for (int c = 0; c < n_; c++) active_h_[c] = 1;
+    BS_TRY(upload_active());
+    std::vector<double> rf(n_);
+    BS_TRY(residual_norms(rf.data()));
+    BS_CUDA(cudaEventRecord(ev1_, stream_));
+    BS_CUDA(cudaEventSynchronize(ev1_));
+    float ms = 0;
+    BS_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    last_solve_ms_ = ms;
+    last_solve_launches_ = launches_;
+    for (int c = 0; c < n_; c++) {
+      results[c].steps = taken[c];
+      results[c].residual = rf[c];
+      if (results[c].status == BS_OK && !(rf[c] <= target[c] * 1.5)) results[c].status = BS_NOT_CONVERGED;
+    }
+    return BS_OK;
+  }
+
+ private:
+  static double solve_gamma(double gamma) {
+    // An FP32 field is solved with gamma rounded to FP32, as the reference GPU does.
+    return sizeof(R) == 4 ? double(float(gamma)) : gamma;
+  }
+
+  int64_t cell_offset(int c) const { return cell_off_[c]; }
+
+  void count_steps(int steps) {
+    for (int c = 0; c < n_; c++)
+      if (active_h_[c]) steps_[c] += steps;
+  }
+
+  bsd::StateView<R> q_view() const { return {q_[0].p, q_[1].p, q_[2].p, q_[3].p}; }
+  bsd::StateView<R> s1_view() const { return {s1_[0].p, s1_[1].p, s1_[2].p, s1_[3].p}; }
+  bsd::StateView<R> s2_view() const { return {s2_[0].p, s2_[1].p, s2_[2].p, s2_[3].p}; }
+  bsd::MetricsView metrics() const { return {iface_.p, jface_.p, cellm_.p}; }
+
+  bs_status ensure_explicit() {
+    if (s1_[0].p != nullptr) return BS_OK;
+    for (int v = 0; v < 4; v++) {
+      BS_CUDA(s1_[v].alloc(total_cells_));
+      BS_CUDA(s2_[v].alloc(total_cells_));
+    }
+    return BS_OK;
+  }
+
+  bs_status ensure_implicit() {
+    if (r32_.p != nullptr) return BS_OK;
+    BS_CUDA(r32_.alloc(total_cells_));
+    BS_CUDA(q32_.alloc(total_cells_));
+    BS_CUDA(dq_.alloc(total_cells_));
+    BS_CUDA(diag_.alloc(total_cells_));
+    return BS_OK;
+  }
+
+  bs_status set_implicit_params(double cfl_max, double omega, double growth) {
+    std::vector<float> a(n_, float(cfl_max)), b(n_, float(omega)), g(n_, float(growth));
+    BS_CUDA(cudaMemcpyAsync(cflmax_.p, a.data(), n_ * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    BS_CUDA(cudaMemcpyAsync(omega_.p, b.data(), n_ * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    BS_CUDA(cudaMemcpyAsync(growth_.p, g.data(), n_ * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    return BS_OK;
+  }
+
+  bs_status upload_active() {
+    BS_CUDA(cudaMemcpyAsync(d_active_.p, active_h_.data(), n_ * sizeof(int), cudaMemcpyHostToDevice,
+                            stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    return BS_OK;
+  }
+
+  bs_status check_status() {
+    std::vector<unsigned> st(n_);
+    BS_CUDA(cudaMemcpyAsync(st.data(), status_.p, n_ * sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    for (int c = 0; c < n_; c++)
+      if (st[c] & bsd::STATUS_NON_PHYSICAL)
+        return fail(BS_NON_PHYSICAL, "the GPU solution of case " + std::to_string(c) +
+                                         " became non-physical");
+    return BS_OK;
+  }
+
+  template <int MODE>
+  bs_status launch_tile(bsd::StateView<R> src, bsd::StateView<R> u0, bsd::StateView<R> out,
+                        double a, double b, bool first, double* norm, double* res_out,
+                        bool all_cases) {
+    bsd::TileArgs<R> A{};
+    A.cases = d_cases_.p;
+    A.tiles = d_tiles_.p;
+    A.active = all_cases ? nullptr : d_active_.p;
+    A.src = src;
+    A.u0 = u0;
+    A.out = out;
+    A.m = metrics();
+    A.dt = dt_.p;
+    A.dt_global = dtmin_.p;
+    A.norm = norm;
+    A.status = status_.p;
+    A.a = a;
+    A.b = b;
+    A.first_stage = first ? 1 : 0;
+    A.r32 = r32_.p;
+    A.q32 = q32_.p;
+    A.diag = diag_.p;
+    A.cfl = cfl_.p;
+    A.omega = omega_.p;
+    A.res_out = res_out;
+    bsd::tile_kernel<R, MODE><<<n_tiles_, bsd::TILE_THREADS, 0, stream_>>>(A);
+    launches_++;
+    BS_CUDA(cudaGetLastError());
+    return BS_OK;
+  }
+
+  // One explicit step of every active case; `norm` adds the density
+  // residual of the step's starting state to the per-case slots.
+  bs_status record_explicit_step(bool norm) {
+    double a[3], b[3];
+    int n = 3;
+    const int integrator = cases_[0].cfg.integrator;
+    if (integrator == BS_FORWARD_EULER) {
+      n = 1; a[0] = 0; b[0] = 1;
+    } else if (integrator == BS_SSPRK2) {
+      n = 2; a[0] = 0; b[0] = 1; a[1] = 0.5; b[1] = 0.5;
+    } else {
+      a[0] = 0; b[0] = 1; a[1] = 3.0 / 4.0; b[1] = 1.0 / 4.0; a[2] = 1.0 / 3.0; b[2] = 2.0 / 3.0;
+    }
+    if (any_global_dt_) {
+      BS_CUDA(cudaMemsetAsync(dtmin_.p, 0x7f, n_ * sizeof(unsigned), stream_));
+      bsd::dt_kernel<R><<<n_tiles_, bsd::TILE_THREADS, 0, stream_>>>(
+          d_cases_.p, d_tiles_.p, d_active_.p, q_view(), metrics(), dt_.p, dtmin_.p);
+      launches_++;
+      BS_CUDA(cudaGetLastError());
+    }
+    const bsd::StateView<R> q = q_view(), s1 = s1_view(), s2 = s2_view();
+    if (n == 1) {
+      BS_TRY(launch_tile<bsd::MODE_STAGE>(q, q, s1, a[0], b[0], true, norm ? norm_.p : nullptr, nullptr, false));
+      for (int v = 0; v < 4; v++)
+        BS_CUDA(cudaMemcpyAsync(q_[v].p, s1_[v].p, total_cells_ * sizeof(R), cudaMemcpyDeviceToDevice, stream_));
+      return BS_OK;
+    }
+    for (int s = 0; s < n; s++) {
+      const bsd::StateView<R> src = s == 0 ? q : (s == 1 ? s1 : s2);
+      const bsd::StateView<R> out = s == n - 1 ? q : (s == 0 ? s1 : s2);
+      BS_TRY(launch_tile<bsd::MODE_STAGE>(src, q, out, a[s], b[s], s == 0,
+                                          (norm && s == 0) ? norm_.p : nullptr, nullptr, false));
+    }
+    return BS_OK;
+  }
+
+  bs_status record_implicit_step(bool norm) {
+    const bsd::StateView<R> q = q_view();
+    BS_TRY(launch_tile<bsd::MODE_PREPARE>(q, q, q, 0, 1, false, norm ? norm_.p : nullptr, nullptr, false));
+    return launch_sweep();
+  }
+
+  bs_status launch_sweep() {
+    bsd::SweepArgs S{};
+    S.cases = d_cases_.p;
+    S.case_list = d_case_list_.p;
+    S.active = d_active_.p;
+    S.m = metrics();
+    S.r32 = r32_.p;
+    S.q32 = q32_.p;
+    S.diag = diag_.p;
+    S.dq = dq_.p;
+    S.cfl = cfl_.p;
+    S.cfl_max = cflmax_.p;
+    S.growth = growth_.p;
+    S.omega = omega_.p;
+    S.status = status_.p;
+    bsd::UpdateArgs<R> U{q_view()};
+    const int nt = ((max_nj_ + 31) / 32) * 32;
+    const size_t smem = size_t(nt) * (4 * sizeof(float4) + 2 * sizeof(float));
+    bsd::lusgs_sweep_kernel<R><<<n_, nt, smem, stream_>>>(S, U);
+    launches_++;
+    BS_CUDA(cudaGetLastError());
+    return BS_OK;
+  }
+
+  bs_status record_steps(int method, int count, bool norm_last) {
+    for (int s = 0; s < count; s++) {
+      const bool norm = norm_last && s == count - 1;
+      if (method == kMethodExplicit)
+        BS_TRY(record_explicit_step(norm));
+      else
+        BS_TRY(record_implicit_step(norm));
+    }
+    return BS_OK;
+  }
+
+  // Runs `count` steps by replaying captured graphs of up to kChunk steps.
+  bs_status run_steps(int method, int count, bool norm_last) {
+    constexpr int kChunk = 16;
+    int left = count;
+    while (left > 0) {
+      const int n = std::min(left, kChunk);
+      const bool norm = norm_last && n == left;
+      cudaGraphExec_t exec = nullptr;
+      BS_TRY(graph_for(method, n, norm, &exec));
+      BS_CUDA(cudaGraphLaunch(exec, stream_));
+      left -= n;
+    }
+    return BS_OK;
+  }
+
+  bs_status graph_for(int method, int count, bool norm_last, cudaGraphExec_t* out) {
+    const GraphKey key{method, count, norm_last ? 1 : 0};
+    auto it = graphs_.find(key);
+    if (it != graphs_.end()) {
+      *out = it->second;
+      launches_ += graph_launches_[key];
+      return BS_OK;
+    }
+    cudaGraph_t graph = nullptr;
+    const int64_t before = launches_;
+    BS_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    const bs_status st = record_steps(method, count, norm_last);
+    const cudaError_t end = cudaStreamEndCapture(stream_, &graph);
+    if (st != BS_OK) {
+      if (graph != nullptr) cudaGraphDestroy(graph);
+      return st;
+    }
+    BS_CUDA(end);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t inst = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    BS_CUDA(inst);
+    graphs_[key] = exec;
+    graph_launches_[key] = launches_ - before;
+    *out = exec;
+    return BS_OK;
+  }
+
+  bs_status launch_boundary(int c, int side, double p_inf, bool drag) {
+    bsd::BoundaryArgs<R> A{};
+    A.cases = d_cases_.p;
+    A.case_index = c;
+    A.q = q_view();
+    A.m = metrics();
+    A.side = side;
+    const HostCase& h = cases_[c];
+    int64_t off = boundary_off_[c];
+    for (int s = 0; s < side; s++) off += s < 2 ? h.cfg.nj : h.cfg.ni;
+    A.geom = bgeom_.p + 3 * off;
+    A.gamma_eval = h.cfg.gamma;
+    A.flux_out = bflux_.p;
+    A.p_inf = p_inf;
+    A.force_out = drag ? force_.p : nullptr;
+    bsd::boundary_flux_kernel<R><<<1, 256, 0, stream_>>>(A);
+    launches_++;
+    BS_CUDA(cudaGetLastError());
+    return BS_OK;
+  }
+
+  bs_status copy_state(int c, std::vector<R> comp[4]) {
+    const size_t n = size_t(cases_[c].cfg.ni) * cases_[c].cfg.nj;
+    const int64_t off = cell_offset(c);
+    for (int v = 0; v < 4; v++) {
+      comp[v].resize(n);
+      BS_CUDA(cudaMemcpyAsync(comp[v].data(), q_[v].p + off, n * sizeof(R), cudaMemcpyDeviceToHost,
+                              stream_));
+    }
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    return BS_OK;
+  }
+
+  std::vector<HostCase> cases_;
+  int n_ = 0;
+  int64_t total_cells_ = 0;
+  int n_tiles_ = 0;
+  int max_nj_ = 0, max_along_ = 0;
+  bool any_global_dt_ = false;
+  std::vector<int64_t> boundary_off_, cell_off_;
+  std::vector<int64_t> steps_;
+  std::vector<int> active_h_;
+  DevBuf<bsd::CaseDev> d_cases_;
+  DevBuf<int2> d_tiles_;
+  DevBuf<int> d_case_list_, d_active_;
+  DevBuf<R> q_[4], s1_[4], s2_[4];
+  DevBuf<float> dt_, diag_, cfl_, cflmax_, growth_, omega_;
+  DevBuf<float4> iface_, jface_, r32_, q32_, dq_;
+  DevBuf<float2> cellm_;
+  DevBuf<double> norm_, bgeom_, bflux_, force_, res_out_;
+  DevBuf<unsigned> status_, dtmin_;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  std::map<GraphKey, cudaGraphExec_t> graphs_;
+  std::map<GraphKey, int64_t> graph_launches_;
+  int64_t launches_ = 0;
+  double last_solve_ms_ = 0;
+  int64_t last_solve_launches_ = 0;
+};
+
+}  // namespace
+
+bs_status make_solver(std::vector<HostCase>&& cases, int precision,
+                      std::unique_ptr<SolverBase>& out) {
+  if (cases.empty()) return fail(BS_INVALID_ARGUMENT, "a batch needs at least one case");
+  const int integrator = cases[0].cfg.integrator;
+  for (const HostCase& h : cases)
+    if (h.cfg.integrator != integrator)
+      return fail(BS_INVALID_ARGUMENT, "the cases of a batch share one time integrator");
+  if (precision == 64) {
+    auto s = std::make_unique<Solver<double>>(std::move(cases));
+    BS_TRY(s->init());
+    out = std::move(s);
+  } else if (precision == 32) {
+    auto s = std::make_unique<Solver<float>>(std::move(cases));
+    BS_TRY(s->init());
+    out = std::move(s);
+  } else {
+    return fail(BS_INVALID_ARGUMENT, "precision must be 32 or 64");
+  }
+  return BS_OK;
+}
+
+}  // namespace bs

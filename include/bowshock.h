@@ -1,0 +1,393 @@
+/*
+ * bowshock_b200 C ABI: the steady 2D axisymmetric finite-volume Euler solve on
+ * NVIDIA B200 (sm_100a), as a drop-in for the engines behind bowshock's
+ * `SteadyEngine` / `EngineFactory` plug-in boundary
+ * (src/analysis/verified-drag.ts:22-37).
+ *
+ * Conventions (the reference's, src/grid/structured.ts:1-50 and
+ * src/engine-cpu/euler2d.ts:99-113):
+ *   - a block of ni x nj cells between (ni + 1) x (nj + 1) nodes; node (i, j)
+ *     at i + j (ni + 1), cell (i, j) at i + j ni;
+ *   - x is axial and y radial (y >= 0) in axisymmetric geometry;
+ *   - primitive states are (rho, u, v, p), conserved ones (rho, rho u, rho v, E),
+ *     four values per cell, cell c at 4 c.
+ *
+ * Ownership: the caller owns every host array; the library copies inputs in
+ * and results out and keeps no caller pointer after a call returns. The
+ * library owns its device memory until the matching *_destroy.
+ *
+ * Errors: every entry point returns a bs_status; BS_OK is 0. The message of
+ * the last failure on the calling thread is bs_last_error().
+ *
+ * Threading: an engine or batch runs one operation at a time; a call that
+ * overlaps another on the same object returns BS_BUSY. Distinct objects may
+ * be used from different threads; each owns its CUDA stream.
+ */
+#ifndef BOWSHOCK_B200_H
+#define BOWSHOCK_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define BS_API __attribute__((visibility("default")))
+#else
+#define BS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The reference throws RangeError (BS_INVALID_ARGUMENT),
+ * NonPhysicalStateError (BS_NON_PHYSICAL, src/solver/errors.ts:2),
+ * GpuMemoryLimitError / GpuExecutionError (BS_MEMORY_LIMIT / BS_EXECUTION,
+ * src/engine-gpu/gpu-common.ts:7-17); ExclusiveRunner's overlapping-call
+ * error becomes BS_BUSY (gpu-common.ts:122-140); a solve that does not reach
+ * its tolerance within its step budget returns BS_NOT_CONVERGED (the
+ * driver's IterationStalled, src/analysis/verified-drag.ts:202). */
+typedef enum bs_status {
+  BS_OK = 0,
+  BS_INVALID_ARGUMENT = 1,
+  BS_NON_PHYSICAL = 2,
+  BS_MEMORY_LIMIT = 3,
+  BS_EXECUTION = 4,
+  BS_NOT_CONVERGED = 5,
+  BS_BUSY = 6,
+  BS_GRID_QUALITY = 7
+} bs_status;
+
+typedef enum bs_geometry { BS_PLANAR = 0, BS_AXISYMMETRIC = 1 } bs_geometry;
+
+/* Face fluxes available on the GPU (src/engine-gpu/euler2d-gpu.ts:235-239). */
+typedef enum bs_flux { BS_FLUX_HLLC = 0, BS_FLUX_RUSANOV = 1 } bs_flux;
+
+/* LIMITERS (src/scheme/limiters.ts:87-94). */
+typedef enum bs_limiter {
+  BS_LIMITER_FIRST_ORDER = 0,
+  BS_LIMITER_MINMOD = 1,
+  BS_LIMITER_VAN_LEER = 2,
+  BS_LIMITER_VAN_ALBADA = 3,
+  BS_LIMITER_MONOTONIZED_CENTRAL = 4,
+  BS_LIMITER_UNLIMITED_CENTRAL = 5
+} bs_limiter;
+
+/* Reconstruction (src/scheme/reconstruction.ts:43). */
+typedef enum bs_reconstruction {
+  BS_RECON_PER_VARIABLE = 0,
+  BS_RECON_SHARED = 1,
+  BS_RECON_SHARED_SCALED = 2
+} bs_reconstruction;
+
+/* RUNGE_KUTTA_STAGES (src/solver/runge-kutta.ts:17-28). */
+typedef enum bs_integrator {
+  BS_FORWARD_EULER = 0,
+  BS_SSPRK2 = 1,
+  BS_SSPRK3 = 2
+} bs_integrator;
+
+typedef enum bs_time_stepping { BS_TIME_LOCAL = 0, BS_TIME_GLOBAL = 1 } bs_time_stepping;
+
+/* BoundaryCondition2D kinds (src/engine-cpu/euler2d.ts:34-56); the fitted
+ * shock's 'faceStates' is not on this path. */
+typedef enum bs_bc_kind {
+  BS_BC_INFLOW = 0,
+  BS_BC_OUTFLOW = 1,
+  BS_BC_WALL = 2,
+  BS_BC_FAR_FIELD = 3,
+  BS_BC_PERIODIC = 4
+} bs_bc_kind;
+
+/* Side (src/engine-cpu/euler2d.ts:32). */
+typedef enum bs_side { BS_IMIN = 0, BS_IMAX = 1, BS_JMIN = 2, BS_JMAX = 3 } bs_side;
+
+/* Primitive2D (src/scheme/flux.ts:331-336). */
+typedef struct bs_primitive {
+  double rho, u, v, p;
+} bs_primitive;
+
+typedef struct bs_boundary {
+  int32_t kind;       /* bs_bc_kind */
+  int32_t reserved;   /* zero */
+  bs_primitive state; /* inflow / far-field free stream; ignored otherwise */
+} bs_boundary;
+
+/* Euler2DConfig (src/engine-cpu/euler2d.ts:58-81) without the grid nodes,
+ * which are passed beside it, and without the manufactured-solution source
+ * (the GPU engine refuses sources, src/analysis/gpu-engine.ts:21). */
+typedef struct bs_config {
+  int32_t ni, nj;
+  int32_t geometry;       /* bs_geometry */
+  int32_t flux;           /* bs_flux */
+  int32_t limiter;        /* bs_limiter */
+  int32_t reconstruction; /* bs_reconstruction */
+  int32_t integrator;     /* bs_integrator */
+  int32_t time_stepping;  /* bs_time_stepping */
+  double gamma;
+  double cfl;             /* explicit CFL number, in (0, 1] */
+  bs_boundary boundaries[4]; /* indexed by bs_side */
+} bs_config;
+
+/* BoundaryFaceFlux (src/engine-cpu/euler2d.ts:99-113): midpoint, outward
+ * unit normal, area (per radian when axisymmetric) and the flux per unit area
+ * along the outward normal [mass, x momentum, y momentum, energy]. */
+typedef struct bs_face_flux {
+  double x, y, nx, ny, area;
+  double flux[4];
+} bs_face_flux;
+
+/* Outcome of a steady solve. */
+typedef struct bs_solve_result {
+  int32_t status;          /* bs_status of this solve */
+  int32_t steps;           /* steps taken by this solve */
+  double residual;         /* final RMS density residual, FP64 */
+  double initial_residual; /* residual of the state the solve started from */
+  double drag;             /* forebody pressure drag coefficient, FP64 */
+} bs_solve_result;
+
+typedef struct bs_engine bs_engine;
+
+/* Arithmetic of a GPU solve. BS_PRECISION_FP64 (the default): the state and
+ * the residual that decides convergence in FP64, the LU-SGS operator, the
+ * time steps and the grid metrics in FP32 - the FP32 field alone cannot
+ * reach an RMS density residual of 1e-6 (its rounding floor is near 1e-5).
+ * BS_PRECISION_FP32: every field quantity in FP32 with gamma rounded to
+ * FP32, the reference GPU engine's arithmetic
+ * (src/engine-gpu/euler2d-gpu.ts:129-146). */
+typedef enum bs_precision { BS_PRECISION_FP32 = 32, BS_PRECISION_FP64 = 64 } bs_precision;
+
+/* Message of the last failure on this thread ("" if none). */
+BS_API const char *bs_last_error(void);
+
+/* Library version string. */
+BS_API const char *bs_version(void);
+
+/* Number of CUDA devices the library can use (0 without a GPU). */
+BS_API bs_status bs_device_count(int32_t *count);
+
+/* The device this thread's engines and batches are created on (default 0);
+ * objects stay on the device they were created on. */
+BS_API bs_status bs_set_device(int32_t device);
+
+/* ---- single-grid engine: Euler2D / GpuEuler2D --------------------------- */
+
+/* new Euler2D(config) / GpuEuler2D.create (src/engine-cpu/euler2d.ts:318,
+ * src/engine-gpu/euler2d-gpu.ts:217): validates the configuration
+ * (src/solver/config.ts:35-55), computes the grid metrics in FP64
+ * (src/grid/structured.ts:94-168) and uploads them as FP32. x and y hold the
+ * (ni + 1)(nj + 1) nodes. The state starts undefined until set. */
+BS_API bs_status bs_engine_create(const bs_config *config, const double *x, const double *y,
+                           bs_engine **out);
+
+/* bs_engine_create with an explicit bs_precision. */
+BS_API bs_status bs_engine_create_ex(const bs_config *config, const double *x, const double *y,
+                              int32_t precision, bs_engine **out);
+
+/* GpuEuler2D.destroy (src/engine-gpu/euler2d-gpu.ts:673). */
+BS_API bs_status bs_engine_destroy(bs_engine *engine);
+
+/* Cell centroids in FP64 (GridMetrics.centroidX/Y, src/grid/structured.ts:48-49),
+ * ni nj each, for evaluating an initial field on the host. */
+BS_API bs_status bs_engine_centroids(bs_engine *engine, double *cx, double *cy);
+
+/* setCellPrimitives / setInitialCondition (src/engine-gpu/euler2d-gpu.ts:412-459):
+ * four primitives per cell; resets the step count. The energy uses gamma
+ * rounded to FP32, as the reference GPU does. Returns BS_NON_PHYSICAL, with
+ * nothing uploaded, if a state has rho <= 0, p <= 0 or a non-finite value. */
+BS_API bs_status bs_engine_set_primitives(bs_engine *engine, const double *primitives);
+
+/* iterate(count) (src/engine-cpu/euler2d.ts:554-560): explicit SSP-RK steps
+ * with the configured integrator and time stepping. BS_NON_PHYSICAL if a
+ * cell became non-physical (the state then holds the failing step). */
+BS_API bs_status bs_engine_iterate(bs_engine *engine, int32_t steps);
+
+/* setImplicitCfl (src/engine-gpu/euler2d-gpu.ts:681-692): the CFL number the
+ * next implicit step starts from (1 after create). */
+BS_API bs_status bs_engine_set_implicit_cfl(bs_engine *engine, double cfl);
+
+/* iterateImplicit with LU-SGS sweeps (src/engine-cpu/euler2d.ts:581-589,
+ * implicitCorrection :878-1105, applyImplicitUpdate :816-847): each step uses
+ * the current CFL number, which then grows by `growth` up to `cfl_max`
+ * (src/engine-gpu/shaders/euler2d-implicit.wgsl:232-237). growth = 1 with
+ * bs_engine_set_implicit_cfl(cfl_max) is the CPU engine's fixed-CFL form.
+ * The sweeps run as anti-diagonal wavefronts on the GPU. */
+BS_API bs_status bs_engine_iterate_implicit(bs_engine *engine, int32_t steps, double cfl_max,
+                                     double omega, double growth);
+
+/* densityResidualNorm (src/engine-cpu/euler2d.ts:480-491): RMS over the
+ * interior cells of R_rho / V, the residual evaluated on the GPU from the
+ * FP32 state and accumulated in FP64. */
+BS_API bs_status bs_engine_density_residual_norm(bs_engine *engine, double *norm);
+
+/* residualVector (src/engine-cpu/euler2d.ts:456-472): the residual of the
+ * current state, four FP64 values per cell, evaluated on the GPU. */
+BS_API bs_status bs_engine_residual(bs_engine *engine, double *residual);
+
+/* Local time step of every cell (computeTimeSteps, src/engine-cpu/euler2d.ts:1183-1205),
+ * evaluated on the GPU and stored as FP32; ni nj values. */
+BS_API bs_status bs_engine_time_steps(bs_engine *engine, double *dt);
+
+/* boundaryFluxes(side) (src/engine-cpu/euler2d.ts:499-525): wall-face fluxes
+ * evaluated on the GPU in FP64 from the FP32 state; `out` holds ni (j sides)
+ * or nj (i sides) entries. */
+BS_API bs_status bs_engine_boundary_fluxes(bs_engine *engine, int32_t side, bs_face_flux *out);
+
+/* forebodyPressureDrag over the jMin faces (src/analysis/forces.ts:19-30),
+ * computed and reduced in FP64 on the GPU. */
+BS_API bs_status bs_engine_forebody_drag(bs_engine *engine, double p_inf, double q_inf,
+                                  double base_radius, double *drag);
+
+/* readState (src/engine-gpu/euler2d-gpu.ts:549-571): the FP32 conserved
+ * state, four values per cell. */
+BS_API bs_status bs_engine_read_state(bs_engine *engine, float *conserved);
+
+/* cells() (src/analysis/verified-drag.ts:26-27, gpuPrimitive2D
+ * euler2d-gpu.ts:136-146): primitives in FP64 recovered from the FP32 state
+ * with gamma rounded to FP32. */
+BS_API bs_status bs_engine_read_primitives(bs_engine *engine, double *primitives);
+
+/* Steps taken since the state was last set. */
+BS_API bs_status bs_engine_steps(bs_engine *engine, int64_t *steps);
+
+/* Iterate until the FP64 RMS density residual is at most `tolerance` times
+ * the residual of the starting state (relative = 1) or at most `tolerance`
+ * (relative = 0), checking every `check_every` steps, up to `max_steps`.
+ * method 0 = explicit (config integrator), 1 = LU-SGS at fixed `cfl` and
+ * `omega`. The convergence test runs on the GPU in FP64; the host reads one
+ * word per check. Fills `result` (drag with p = 1, q = gamma M^2 / 2 taken
+ * from the jMin-side free stream is not known here, so result->drag is 0;
+ * use bs_engine_forebody_drag). Returns BS_NOT_CONVERGED if the budget ran
+ * out first. */
+BS_API bs_status bs_engine_solve(bs_engine *engine, int32_t method, double cfl, double omega,
+                          double tolerance, int32_t relative, int32_t max_steps,
+                          int32_t check_every, bs_solve_result *result);
+
+/* ---- batches: many cases of uneven size in one set of launches ------------ */
+
+typedef struct bs_batch bs_batch;
+
+/* A batch of n independent cases (their own grids, configurations and free
+ * streams) solved together: every kernel launch covers all active cases, and
+ * a case stops when its own residual reaches the tolerance. configs[k] with
+ * nodes x[k], y[k] as in bs_engine_create. The cases share one time
+ * integrator. */
+BS_API bs_status bs_batch_create(int32_t n, const bs_config *configs, const double *const *x,
+                                 const double *const *y, int32_t precision, bs_batch **out);
+BS_API bs_status bs_batch_destroy(bs_batch *batch);
+BS_API bs_status bs_batch_size(bs_batch *batch, int32_t *n);
+
+/* As bs_engine_set_primitives, for case `c`. */
+BS_API bs_status bs_batch_set_primitives(bs_batch *batch, int32_t c, const double *primitives);
+
+/* Every case from its own jMax/iMin inflow state (the free stream). */
+BS_API bs_status bs_batch_set_free_stream(bs_batch *batch);
+
+/* As bs_engine_solve for every case at once; results[k] for case k. Returns
+ * BS_OK when the call ran; each case's outcome is in its result. */
+BS_API bs_status bs_batch_solve(bs_batch *batch, int32_t method, double cfl, double omega,
+                                double tolerance, int32_t relative, int32_t max_steps,
+                                int32_t check_every, bs_solve_result *results);
+
+/* As bs_engine_forebody_drag, for case `c`. */
+BS_API bs_status bs_batch_forebody_drag(bs_batch *batch, int32_t c, double p_inf, double q_inf,
+                                        double base_radius, double *drag);
+/* As bs_engine_read_primitives / bs_engine_density_residual_norm, for case c. */
+BS_API bs_status bs_batch_read_primitives(bs_batch *batch, int32_t c, double *primitives);
+BS_API bs_status bs_batch_density_residual_norms(bs_batch *batch, double *norms);
+
+/* Device time (CUDA events on the batch's stream) and kernel launches of the
+ * last bs_batch_solve. */
+BS_API bs_status bs_batch_last_solve_timing(bs_batch *batch, double *device_ms,
+                                            int64_t *launches);
+
+/* Times each kernel of the solve's step on the batch's current state:
+ * `iterations` steps of `method`, a CUDA event pair around every launch on
+ * the batch's stream. ms[k] is the mean duration of kernel k per launch:
+ * method 1 (LU-SGS): k = 0 residual/diagonal pass, 1 wavefront sweeps;
+ * method 0 (explicit): k = 0 the first stage, 1 a later stage.
+ * The state advances by `iterations` steps. */
+BS_API bs_status bs_batch_kernel_times(bs_batch *batch, int32_t method, double cfl,
+                                       double omega, int32_t iterations, double *ms);
+
+/* ---- grids and exact solutions (host, FP64) ------------------------------ */
+
+/* Nose shapes (NoseShape, src/geometry/nose.ts:13-34). */
+typedef enum bs_nose_kind {
+  BS_NOSE_CONICAL = 0,
+  BS_NOSE_OGIVE = 1,     /* parameter: ogive parameter, 1 = tangent ogive */
+  BS_NOSE_ELLIPSOID = 2,
+  BS_NOSE_POWER = 3,     /* parameter: exponent in (0, 1] */
+  BS_NOSE_PARABOLIC = 4, /* parameter: K in [0, 1] */
+  BS_NOSE_HAACK = 5      /* parameter: C in [0, 1/3]; 0 = Von Karman */
+} bs_nose_kind;
+
+/* Body (src/geometry/body.ts:8-13): a nose followed by a cylinder. */
+typedef struct bs_body {
+  int32_t nose_kind;
+  int32_t reserved;
+  double parameter;
+  double nose_length;
+  double base_radius;
+  double cylinder_length;
+} bs_body;
+
+/* BodyGridOptions (src/grid/body-grid.ts:27-45), plus `ni`: when > 0 the
+ * grid gets exactly ni columns (refinement must be 1), apportioned to the
+ * upstream, nose and cylinder intervals by the generator's own density. */
+typedef struct bs_body_grid_options {
+  int32_t nj;
+  int32_t refinement;
+  int32_t ni;
+  int32_t reserved;
+  double mach;
+  double gamma;
+} bs_body_grid_options;
+
+typedef struct bs_grid bs_grid;
+
+/* bodyGrid (src/grid/body-grid.ts:76-181): the H-topology grid of a sharp
+ * nose; BS_GRID_QUALITY if it fails the quality gates
+ * (src/grid/quality.ts:24-38). */
+BS_API bs_status bs_body_grid(const bs_body *body, const bs_body_grid_options *options, bs_grid **out);
+
+/* rampGrid (src/grid/shapes.ts:30-52): a channel whose lower wall turns by
+ * `angle` at x_corner. */
+BS_API bs_status bs_ramp_grid(int32_t ni, int32_t nj, double x_min, double x_corner, double x_max,
+                       double height, double angle, bs_grid **out);
+
+BS_API bs_status bs_grid_dims(const bs_grid *grid, int32_t *ni, int32_t *nj);
+/* Node coordinates, (ni + 1)(nj + 1) each. */
+BS_API bs_status bs_grid_nodes(const bs_grid *grid, double *x, double *y);
+/* BodyGrid.iTip and outerAngle (src/grid/body-grid.ts:47-54). */
+BS_API bs_status bs_grid_info(const bs_grid *grid, int32_t *i_tip, double *outer_angle);
+BS_API bs_status bs_grid_destroy(bs_grid *grid);
+
+/* GridQuality (src/grid/quality.ts:6-21, gridQuality :75-128). */
+typedef struct bs_grid_quality {
+  double min_angle, min_wall_angle, max_size_ratio, max_aspect_ratio, min_area;
+} bs_grid_quality;
+BS_API bs_status bs_grid_quality_of(int32_t ni, int32_t nj, const double *x, const double *y,
+                             bs_grid_quality *out);
+
+/* ConeFlow (src/validation/taylor-maccoll.ts:23-36). */
+typedef struct bs_cone_flow {
+  double shock_angle, post_shock_mach, post_shock_pressure_ratio, surface_mach,
+      surface_pressure_ratio, surface_pressure_coefficient;
+} bs_cone_flow;
+
+/* taylorMaccoll (src/validation/taylor-maccoll.ts:153-216); BS_INVALID_ARGUMENT
+ * if the shock detaches. */
+BS_API bs_status bs_taylor_maccoll(double mach, double cone_angle, double gamma, double tolerance,
+                            bs_cone_flow *out);
+
+/* ObliqueShock / NormalShock (src/validation/gas-dynamics.ts:29-96). */
+typedef struct bs_shock {
+  double beta, pressure_ratio, density_ratio, downstream_mach;
+} bs_shock;
+BS_API bs_status bs_oblique_shock(double mach, double theta, double gamma, bs_shock *out);
+BS_API bs_status bs_normal_shock(double mach, double gamma, bs_shock *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BOWSHOCK_B200_H */

@@ -1,0 +1,76 @@
+"""Extracts the known answers that pin the steady Euler path from the
+reference's own test files (read as text; nothing of the reference runs) into
+reference_known_answers.json. Run from the repository root with the
+reference checked out at REFERENCE (default /root/reference):
+
+    python tests/golden/extract_known_answers.py
+
+The tests read only the JSON file."""
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+from pathlib import Path
+
+REF = Path(os.environ.get("REFERENCE", "/root/reference"))
+OUT = Path(__file__).resolve().parent / "reference_known_answers.json"
+
+
+def find_line(text: str, needle: str) -> int:
+    for k, line in enumerate(text.splitlines(), 1):
+        if needle in line:
+            return k
+    raise KeyError(needle)
+
+
+def main() -> None:
+    out: dict = {}
+    # Verified drag of the CPU engine on the 20 deg cone at Mach 3 (cylinder 4,
+    # nj = 20), refinements 1 and 2.
+    f = "tests/gpu/verified-drag-gpu.test.ts"
+    t = (REF / f).read_text()
+    m = re.search(r"const cpu = \[([0-9.]+),\s*([0-9.]+)\]", t)
+    out["verified_drag_cone20_mach3"] = {
+        "source": f"{f}:{find_line(t, 'const cpu = [')}",
+        "body": {"shape": "conical", "half_angle_deg": 20, "base_radius": 0.5, "cylinder": 4},
+        "mach": 3.0, "nj": 20, "refinements": [1, 2],
+        "drag": [float(m.group(1)), float(m.group(2))],
+        "tolerance_relative": 2e-6,
+    }
+    # Taylor-Maccoll against NASA SP-3004 (cone deg, Mach, shock angle rad,
+    # surface Mach, Cp) and the NPARC 10 deg / Mach 2.35 case.
+    f = "tests/validation/taylor-maccoll.test.ts"
+    t = (REF / f).read_text()
+    rows = re.findall(r"\[\s*([0-9.]+),\s*([0-9.]+),\s*([0-9.]+),\s*([0-9.]+),\s*([0-9.]+)\s*\]", t)
+    out["taylor_maccoll_sp3004"] = {
+        "source": f"{f}:{find_line(t, 'const rows')}",
+        "columns": ["cone_deg", "mach", "shock_angle_rad", "surface_mach", "cp"],
+        "rows": [[float(v) for v in r] for r in rows],
+        "tolerance": {"shock_angle_abs": 5e-6, "surface_mach_rel": 3e-5, "cp_abs": 3e-5},
+    }
+    out["taylor_maccoll_nparc"] = {
+        "source": f"{f}:{find_line(t, 'NPARC/WIND')}",
+        "cone_deg": 10, "mach": 2.35,
+        "post_shock_mach": 2.2677, "surface_mach": 2.1469, "surface_mach_cfd": 2.1467886,
+        "surface_pressure_ratio": 1.37405,
+        "tolerance": {"post_shock_mach_abs": 5e-4, "surface_mach_abs": 5e-4,
+                      "surface_mach_cfd_abs": 2e-4, "surface_pressure_ratio_abs": 5e-4},
+    }
+    assert re.search(r"toBeCloseTo\(2\.2677", t) is not None
+    # Implicit steps reach the explicit drag (15 deg cone, Mach 2, nj 12, cylinder 1).
+    f = "tests/engine-cpu/implicit.test.ts"
+    t = (REF / f).read_text()
+    out["implicit_equals_explicit"] = {
+        "source": f"{f}:{find_line(t, 'implicit steps reach the steady state')}",
+        "body": {"shape": "conical", "half_angle_deg": 15, "base_radius": 0.5, "cylinder": 1},
+        "mach": 2.0, "nj": 12, "explicit_steps": 6000, "residual_below": 1e-12,
+        "drag_equal_within": 1e-12,
+    }
+    OUT.write_text(json.dumps(out, indent=1) + "\n")
+    print(f"wrote {OUT}")
+
+
+if __name__ == "__main__":
+    sys.exit(main())
