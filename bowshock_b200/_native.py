@@ -90,6 +90,8 @@ SIGNATURES: dict[str, list] = {
     "bs_batch_density_residual_norms": [_vp, _dp],
     "bs_batch_last_solve_timing": [_vp, _dp, C.POINTER(C.c_int64)],
     "bs_batch_kernel_times": [_vp, C.c_int32, C.c_double, C.c_double, C.c_int32, _dp],
+    "bs_lusgs_step_static": [C.POINTER(abi.Config), _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_double,
+                             C.c_double, _vp, _dp, _ip],
     "bs_body_grid": [C.POINTER(abi.Body), C.POINTER(abi.BodyGridOptions), C.POINTER(_vp)],
     "bs_ramp_grid": [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
                      C.c_double, C.POINTER(_vp)],

@@ -261,6 +261,32 @@ BS_API bs_status bs_engine_solve(bs_engine *engine, int32_t method, double cfl, 
                           double tolerance, int32_t relative, int32_t max_steps,
                           int32_t check_every, bs_solve_result *result);
 
+/* ---- an LU-SGS step that allocates nothing -------------------------------- */
+
+/* One LU-SGS step (residual and diagonal pass, forward and backward wavefront
+ * sweeps, update) of one case whose FP64 state and grid metrics the caller
+ * keeps in its own device memory; no counterpart in the reference. For
+ * callers that cannot let a library allocate device memory: applications
+ * that hand out all GPU memory from their own pool (cudaMalloc would bypass
+ * their budget, and cudaMalloc/cudaFree synchronise the device) and solver
+ * loops that must not allocate once running. All scratch lives in one static
+ * device array of the library, reserved on every GPU that loads it until the
+ * process exits: at most 65536 cells (ni nj) and 512 cells across (nj);
+ * larger grids return BS_INVALID_ARGUMENT. The first call on a device looks up
+ * the array's device address with that device current; make that first call
+ * before any stream capture. Every call shares the array, so calls that
+ * overlap on the GPU race: order them. Device inputs (layout as the engine's,
+ * device/layout.cuh): iface (ni + 1) nj float4 (nx, ny, area, 0), jface
+ * ni (nj + 1) float4, cells ni nj float2 (volume, planar area); the state as
+ * four FP64 arrays of ni nj, updated in place. `stream` is a cudaStream_t
+ * (NULL for the default stream). On return, *residual is the RMS density
+ * residual of the state the step started from and *non_physical is 1 if a
+ * cell became non-physical. */
+BS_API bs_status bs_lusgs_step_static(const bs_config *config, const float *iface,
+                                      const float *jface, const float *cells, double *rho,
+                                      double *mu, double *mv, double *e, double cfl, double omega,
+                                      void *stream, double *residual, int32_t *non_physical);
+
 /* ---- batches: many cases of uneven size in one set of launches ------------ */
 
 typedef struct bs_batch bs_batch;
