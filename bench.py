@@ -47,9 +47,11 @@ CHECK_EVERY = 20
 #   sweeps: forward  residual 16 + state copy 16 + diagonal 4 + faces 32
 #                    + dQ* 16 = 84
 #           backward dQ* 16 + state copy 16 + diagonal 4 + faces 32
-#                    + state read 32 + state write 32 = 132
+#                    + dQ 16 = 84
+#   update: state 32 + dQ 16 + state 32 = 80
 BYTES_PREPARE = 108
-BYTES_SWEEP = 216
+BYTES_SWEEP = 168
+BYTES_UPDATE = 80
 
 
 def workload_config() -> dict:
@@ -257,7 +259,7 @@ def run_gpu(args, world, rank, local) -> None:
     # Roofline of the dominant kernel, timed with CUDA events on the
     # library's stream over the same solve from the free stream.
     batch.set_free_stream()
-    prep_ms, sweep_ms = batch.kernel_times("lusgs", CFL, OMEGA, iterations=50)
+    prep_ms, sweep_ms, update_ms = batch.kernel_times("lusgs", CFL, OMEGA, iterations=50)
     cells = sum(c.config.grid.ni * c.config.grid.nj for c in cases)
     peaks = {}
     try:
@@ -269,6 +271,7 @@ def run_gpu(args, world, rank, local) -> None:
     kernels = {
         "lusgs_sweep": (sweep_ms, BYTES_SWEEP * cells),
         "lusgs_prepare": (prep_ms, BYTES_PREPARE * cells),
+        "lusgs_update": (update_ms, BYTES_UPDATE * cells),
     }
     dominant = max(kernels, key=lambda k: kernels[k][0])
     kms, kbytes = kernels[dominant]
@@ -303,7 +306,8 @@ def run_gpu(args, world, rank, local) -> None:
                          "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic,
                          "kernel_ms": {k: v[0] for k, v in kernels.items()},
-                         "bytes_per_cell": {"lusgs_sweep": BYTES_SWEEP, "lusgs_prepare": BYTES_PREPARE}},
+                         "bytes_per_cell": {"lusgs_sweep": BYTES_SWEEP, "lusgs_prepare": BYTES_PREPARE,
+                                            "lusgs_update": BYTES_UPDATE}},
             "cpu_baseline": cpu,
             "clocks": clock_info,
             "accuracy": {"converged": converged, "lusgs_steps": steps_taken,

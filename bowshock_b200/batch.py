@@ -92,8 +92,8 @@ class CudaBatch:
         return ms.value, launches.value
 
     def kernel_times(self, method: str = "lusgs", cfl: float = 5.0, omega: float = 1.5,
-                     iterations: int = 20) -> tuple[float, float]:
-        ms = np.empty(2)
+                     iterations: int = 20) -> tuple[float, float, float]:
+        ms = np.empty(3)
         self._call("bs_batch_kernel_times", 1 if method == "lusgs" else 0, cfl, omega, iterations,
                    ms.ctypes.data_as(_dp))
-        return float(ms[0]), float(ms[1])
+        return float(ms[0]), float(ms[1]), float(ms[2])

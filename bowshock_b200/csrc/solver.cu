@@ -305,9 +305,9 @@ class Solver final : public SolverBase {
 
   bs_status kernel_times(int method, double cfl, double omega, int iterations, double* ms) override {
     if (iterations < 1) return fail(BS_INVALID_ARGUMENT, "iterations must be positive");
-    cudaEvent_t ev[4];
+    cudaEvent_t ev[6];
     for (auto& e : ev) BS_CUDA(cudaEventCreate(&e));
-    double sum[2] = {0, 0};
+    double sum[3] = {0, 0, 0};
     bs_status st = BS_OK;
     if (method == kMethodImplicit) {
       st = ensure_implicit();
@@ -324,29 +324,35 @@ class Solver final : public SolverBase {
         cudaEventRecord(ev[1], stream_);
         cudaEventRecord(ev[2], stream_);
         if (st == BS_OK) st = launch_sweep();
+        cudaEventRecord(ev[3], stream_);
+        cudaEventRecord(ev[4], stream_);
+        if (st == BS_OK) st = launch_update();
       } else {
         const bsd::StateView<R> q = q_view(), s1 = s1_view(), s2 = s2_view();
         st = launch_tile<bsd::MODE_STAGE>(q, q, s1, 0.0, 1.0, true, norm_.p, nullptr, false);
         cudaEventRecord(ev[1], stream_);
         cudaEventRecord(ev[2], stream_);
         if (st == BS_OK) st = launch_tile<bsd::MODE_STAGE>(s1, q, s2, 0.75, 0.25, false, nullptr, nullptr, false);
+        cudaEventRecord(ev[3], stream_);
+        cudaEventRecord(ev[4], stream_);
       }
-      cudaEventRecord(ev[3], stream_);
-      const cudaError_t e = cudaEventSynchronize(ev[3]);
+      cudaEventRecord(ev[5], stream_);
+      const cudaError_t e = cudaEventSynchronize(ev[5]);
       if (e != cudaSuccess) {
         st = cuda_fail(e, "kernel timing");
         break;
       }
-      float a = 0, b = 0;
+      float a = 0, b = 0, u = 0;
       cudaEventElapsedTime(&a, ev[0], ev[1]);
       cudaEventElapsedTime(&b, ev[2], ev[3]);
+      cudaEventElapsedTime(&u, ev[4], ev[5]);
       sum[0] += a;
       sum[1] += b;
+      sum[2] += u;
     }
     for (auto& e : ev) cudaEventDestroy(e);
     if (st != BS_OK) return st;
-    ms[0] = sum[0] / iterations;
-    ms[1] = sum[1] / iterations;
+    for (int k = 0; k < 3; k++) ms[k] = sum[k] / iterations;
     return BS_OK;
   }
 
@@ -704,7 +710,8 @@ class Solver final : public SolverBase {
   bs_status record_implicit_step(bool norm) {
     const bsd::StateView<R> q = q_view();
     BS_TRY(launch_tile<bsd::MODE_PREPARE>(q, q, q, 0, 1, false, norm ? norm_.p : nullptr, nullptr, false));
-    return launch_sweep();
+    BS_TRY(launch_sweep());
+    return launch_update();
   }
 
   bs_status launch_sweep() {
@@ -722,10 +729,14 @@ class Solver final : public SolverBase {
     S.growth = growth_.p;
     S.omega = omega_.p;
     S.status = status_.p;
-    bsd::UpdateArgs<R> U{q_view()};
-    const int nt = ((max_nj_ + 31) / 32) * 32;
-    const size_t smem = size_t(nt) * (4 * sizeof(float4) + 2 * sizeof(float));
-    bsd::lusgs_sweep_kernel<R><<<n_, nt, smem, stream_>>>(S, U);
+    BS_CUDA(bsd::launch_sweep(S, n_, max_nj_, stream_));
+    launches_++;
+    return BS_OK;
+  }
+
+  bs_status launch_update() {
+    bsd::lusgs_update_kernel<R><<<n_tiles_, bsd::TILE_THREADS, 0, stream_>>>(
+        d_cases_.p, d_tiles_.p, d_active_.p, q_view(), dq_.p, status_.p);
     launches_++;
     BS_CUDA(cudaGetLastError());
     return BS_OK;

@@ -206,10 +206,11 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
     S.growth = &d_words->growth;
     S.omega = &d_words->omega;
     S.status = &d_words->status;
-    const bsd::UpdateArgs<double> U{q};
-    const int nt = ((nj + 31) / 32) * 32;
-    const size_t smem = size_t(nt) * (4 * sizeof(float4) + 2 * sizeof(float));
-    bsd::lusgs_sweep_kernel<double><<<1, nt, smem, st>>>(S, U);
+    err = bsd::launch_sweep(S, 1, nj, st);
+  }
+  if (err == cudaSuccess) {
+    bsd::lusgs_update_kernel<double><<<n_tiles, bsd::TILE_THREADS, 0, st>>>(
+        d_case, d_tiles, nullptr, q, d_dq, &d_words->status);
     err = cudaGetLastError();
   }
   double norm = 0;

@@ -327,10 +327,10 @@ BS_API bs_status bs_batch_last_solve_timing(bs_batch *batch, double *device_ms,
 
 /* Times each kernel of the solve's step on the batch's current state:
  * `iterations` steps of `method`, a CUDA event pair around every launch on
- * the batch's stream. ms[k] is the mean duration of kernel k per launch:
- * method 1 (LU-SGS): k = 0 residual/diagonal pass, 1 wavefront sweeps;
- * method 0 (explicit): k = 0 the first stage, 1 a later stage.
- * The state advances by `iterations` steps. */
+ * the batch's stream. ms[k] (three values) is the mean duration of kernel k
+ * per launch: method 1 (LU-SGS): k = 0 residual/diagonal pass, 1 wavefront
+ * sweeps, 2 update; method 0 (explicit): k = 0 the first stage, 1 a later
+ * stage, 2 zero. The state advances by `iterations` steps. */
 BS_API bs_status bs_batch_kernel_times(bs_batch *batch, int32_t method, double cfl,
                                        double omega, int32_t iterations, double *ms);
 
