@@ -40,17 +40,15 @@ OMEGA = 1.5
 MAX_STEPS = 20000
 CHECK_EVERY = 20
 # Algorithmic bytes per cell of each LU-SGS kernel launch: every array
-# element a pass reads or writes, counted once (FP64 state, FP32 LU-SGS
-# arrays, float4 face metrics), halo re-reads not counted.
-#   residual/diagonal pass: state 32 + i-face 16 + j-face 16 + cell 8
-#                           + residual 16 + state copy 16 + diagonal 4 = 108
-#   sweeps: forward  residual 16 + state copy 16 + diagonal 4 + faces 32
-#                    + dQ* 16 = 84
-#           backward dQ* 16 + state copy 16 + diagonal 4 + faces 32
-#                    + dQ 16 = 84
+# element a pass reads or writes, counted once (FP64 state, FP32 sweep
+# records, float4 face metrics), halo re-reads not counted.
+#   residual pass: state 32 + i-face 16 + j-face 16 + cell 8
+#                  + sweep record 80 (residual, state, u/v/p/(1/D), 2 faces) = 152
+#   sweeps: forward  record 80 + dQ* 16 = 96
+#           backward record 80 + dQ* 16 + dQ 16 = 112
 #   update: state 32 + dQ 16 + state 32 = 80
-BYTES_PREPARE = 108
-BYTES_SWEEP = 168
+BYTES_PREPARE = 152
+BYTES_SWEEP = 208
 BYTES_UPDATE = 80
 
 
@@ -320,6 +318,21 @@ def run_gpu(args, world, rank, local) -> None:
         dist.destroy_process_group()
 
 
+def run_probe(args) -> None:
+    """A few LU-SGS steps of the benchmark's batch, each kernel timed with CUDA
+    events: a short command for profilers (ncu) to capture."""
+    from bowshock_b200.batch import CudaBatch
+    from bowshock_b200.workloads import drag_sweep_cases
+
+    cases = drag_sweep_cases()
+    batch = CudaBatch([c.config for c in cases], precision=64)
+    batch.set_free_stream()
+    prep, sweep, update = batch.kernel_times("lusgs", CFL, OMEGA, iterations=args.probe)
+    print(json.dumps({"probe_iterations": args.probe, "lusgs_prepare_ms": prep,
+                      "lusgs_sweep_ms": sweep, "lusgs_update_ms": update}), flush=True)
+    batch.destroy()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -327,8 +340,13 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--probe", type=int, default=0,
+                    help="run this many LU-SGS steps of the batch with per-kernel timing and exit")
     args = ap.parse_args()
     world, rank, local = dist_env()
+    if args.probe > 0:
+        run_probe(args)
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
         return

@@ -32,9 +32,7 @@ struct SweepArgs {
   const int* case_list;   // blockIdx.x -> case
   const int* active;      // per case (may be null)
   MetricsView m;
-  const float4* r32;      // residual of each cell (pass A)
-  const float4* q32;      // state of each cell (pass A)
-  const float* diag;      // scalar diagonal (pass A)
+  const float4* rec;      // the sweep record of each cell (5 float4, pass A)
   float4* dq;             // forward result, then the final correction
   float* cfl;             // per case current CFL number (ramped after the sweep)
   const float* cfl_max;   // per case
@@ -62,56 +60,42 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// A cell's state as the neighbour term needs it: conserved (rho, mx, my, E)
-// and the derived (u, v, a, p) - all independent of dQ, so they are computed
-// off the sweep's critical path and handed to the next row with the dQ.
-struct NbrState {
-  float4 q;
-  float4 w;  // u, v, sound speed, pressure
-};
-
-__device__ __forceinline__ NbrState derive(const float4 q, float gamma, float gm1) {
-  const float inv = __frcp_rn(q.x);
-  const float u = q.y * inv, v = q.z * inv;
-  const float p = gm1 * (q.w - 0.5f * (q.y * u + q.z * v));
-  const float a = __fsqrt_rn(gamma * p * inv);
-  return {q, make_float4(u, v, a, p)};
-}
-
-// Change of the physical flux along (nx, ny) of state s for the change d,
-// times area/2, less (omega lambda A / 2) d, added to `sum` (the neighbour
-// term, src/engine-cpu/euler2d.ts:977-1005) - the exact difference
-// F(Q + dQ) - F(Q) written so that every term is proportional to dQ. d = 0
-// contributes exactly nothing, which stands for an absent neighbour.
-__device__ __forceinline__ void neighbour_change(float4& sum, const NbrState& s, const float4 d,
-                                                 float nx, float ny, float half_area,
-                                                 float damp, float gm1) {
-  const float u = s.w.x, v = s.w.y, p = s.w.w;
+// Change of the physical flux along (nx, ny) of state q (with u, v, p in
+// w) for the change d, times half_area, less damp d, added to `sum` (the
+// neighbour term, src/engine-cpu/euler2d.ts:977-1005: half_area = A / 2,
+// damp = omega lambda A / 2) - the exact difference F(Q + dQ) - F(Q) written
+// so that every term is proportional to dQ. d = 0 contributes exactly
+// nothing, which stands for an absent neighbour.
+__device__ __forceinline__ void neighbour_change(float4& sum, const float4 q, const float4 w,
+                                                 const float4 d, float nx, float ny,
+                                                 float half_area, float damp, float gm1) {
+  const float u = w.x, v = w.y, p = w.z;
   const float un = u * nx + v * ny;
-  const float inv1 = __frcp_rn(s.q.x + d.x);
+  const float inv1 = __frcp_rn(q.x + d.x);
   const float dmn = d.y * nx + d.z * ny;
   const float dun = (dmn - un * d.x) * inv1;
-  const float dk = (s.q.x * (u * d.y + v * d.z - 0.5f * (u * u + v * v) * d.x) +
+  const float dk = (q.x * (u * d.y + v * d.z - 0.5f * (u * u + v * v) * d.x) +
                     0.5f * (d.y * d.y + d.z * d.z)) * inv1;
   const float dp = gm1 * (d.w - dk);
   sum.x += half_area * dmn - damp * d.x;
-  sum.y += half_area * (d.y * un + (s.q.y + d.y) * dun + dp * nx) - damp * d.y;
-  sum.z += half_area * (d.z * un + (s.q.z + d.z) * dun + dp * ny) - damp * d.z;
-  sum.w += half_area * ((d.w + dp) * un + (s.q.w + d.w + p + dp) * dun) - damp * d.w;
+  sum.y += half_area * (d.y * un + (q.y + d.y) * dun + dp * nx) - damp * d.y;
+  sum.z += half_area * (d.z * un + (q.z + d.z) * dun + dp * ny) - damp * d.z;
+  sum.w += half_area * ((d.w + dp) * un + (q.w + d.w + p + dp) * dun) - damp * d.w;
 }
 
-__device__ __forceinline__ float spectral(const NbrState& s, float nx, float ny) {
-  return fabsf(s.w.x * nx + s.w.y * ny) + s.w.z;
-}
+// Fields of the sweep record (five float4 per cell, written by the residual
+// pass): residual; state; (u, v, p, 1/D); west face and south face as
+// (nx, ny, A/2, omega lambda A / 2).
+enum { REC_R = 0, REC_Q = 1, REC_W = 2, REC_FW = 3, REC_FS = 4, REC_SIZE = 5 };
 
 // Shared memory of the sweep kernel for `nt` threads and a prefetch ring of
-// `depth` slots: each thread stages the data of its next `depth` cells
-// (everything that does not depend on dQ) in its own ring, so global-memory
-// latency overlaps the dependent chain of diagonal steps.
+// `depth` slots: each thread stages the records of its next `depth` cells in
+// its own ring (cp.async), so memory latency overlaps the dependent chain of
+// diagonal steps.
 __host__ __device__ constexpr size_t sweep_smem_bytes(int nt, int depth) {
-  // exchange: q, w, dq (float4), double-buffered; ring: r, q, face_i,
-  // face_j (float4) and diag (float) per slot.
-  return size_t(nt) * (2 * 3 * 16 + depth * (4 * 16 + 4));
+  // exchange: state, (u, v, p, 1/D), dQ, south face (float4), double-buffered;
+  // ring: the record and dQ* (6 float4) per slot.
+  return size_t(nt) * 16 * (2 * 4 + depth * (REC_SIZE + 1));
 }
 
 // The forward and backward sweeps of every active case, one CTA per case,
@@ -126,103 +110,82 @@ __global__ void __launch_bounds__(512) lusgs_sweep_kernel(const SweepArgs A) {
   const int nt = blockDim.x;
   const int j = threadIdx.x;
   const bool row = j < nj;
-  const float gamma = float(cd.gamma);
-  const float gm1 = gamma - 1.f;
-  const float half_omega = 0.5f * A.omega[c];
+  const float gm1 = float(cd.gamma) - 1.f;
   const int ndiag = ni + nj - 1;
   const int64_t cell0 = cd.cell + int64_t(j) * ni;
-  const int64_t if0 = cd.iface + int64_t(j) * (ni + 1);
-  const int64_t jf0 = cd.jface + int64_t(j) * ni;
 
   float4* xq = reinterpret_cast<float4*>(smem_raw);  // [2][nt] exchange: state
-  float4* xw = xq + 2 * nt;                           // [2][nt] derived
-  float4* xd = xw + 2 * nt;                           // [2][nt] dQ
-  float4* ring_r = xd + 2 * nt;                       // [depth][nt]
-  float4* ring_q = ring_r + kSweepDepth * nt;
-  float4* ring_fi = ring_q + kSweepDepth * nt;
-  float4* ring_fj = ring_fi + kSweepDepth * nt;
-  float* ring_d = reinterpret_cast<float*>(ring_fj + kSweepDepth * nt);
-
+  float4* xw = xq + 2 * nt;                           // (u, v, p, 1/D)
+  float4* xd = xw + 2 * nt;                           // dQ
+  float4* xf = xd + 2 * nt;                           // south face record
+  float4* ring = xf + 2 * nt;                         // [depth][6][nt]
+  auto at = [&](int step, int field) { return ring + ((step % kSweepDepth) * (REC_SIZE + 1) + field) * nt + j; };
   const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
 
-  // One sweep: `dir` +1 forward (neighbours i - 1 and j - 1, faces (i, j)),
-  // -1 backward (neighbours i + 1 and j + 1, faces (i + 1, j) and (i, j + 1)).
   for (int pass = 0; pass < 2; pass++) {
     const bool fwd = pass == 0;
-    auto cell_at = [&](int step) { return (fwd ? step : ndiag - 1 - step) - j; };
     auto fetch = [&](int step) {
-      const int i = cell_at(step);
+      const int i = (fwd ? step : ndiag - 1 - step) - j;
       if (row && step < ndiag && i >= 0 && i < ni) {
-        const int slot = (step % kSweepDepth) * nt + j;
-        const int64_t k = cell0 + i;
-        cp_async16(&ring_r[slot], fwd ? &A.r32[k] : &A.dq[k]);
-        cp_async16(&ring_q[slot], &A.q32[k]);
-        cp_async16(&ring_fi[slot], &A.m.iface[if0 + i + (fwd ? 0 : 1)]);
-        cp_async16(&ring_fj[slot], &A.m.jface[jf0 + i + (fwd ? 0 : ni)]);
-        cp_async4(&ring_d[slot], &A.diag[k]);
+        const float4* src = A.rec + REC_SIZE * (cell0 + i);
+#pragma unroll
+        for (int f = 0; f < REC_SIZE; f++) cp_async16(at(step, f), src + f);
+        if (!fwd) cp_async16(at(step, REC_SIZE), &A.dq[cell0 + i]);
       }
       cp_async_commit();
     };
     for (int s = 0; s < kSweepDepth; s++) fetch(s);
-    // The neighbour along the row: the cell this thread finished last step.
-    NbrState prev{make_float4(1.f, 0.f, 0.f, 1.f), make_float4(0.f, 0.f, 1.f, 1.f)};
-    float4 prev_dq = zero;
+    // The cell this thread finished last step (its neighbour along the row).
+    float4 pq = make_float4(1.f, 0.f, 0.f, 1.f), pw = make_float4(0.f, 0.f, 1.f, 1.f);
+    float4 pd = zero, pfw = zero;
     for (int step = 0; step < ndiag; step++) {
       cp_async_wait<kSweepDepth - 1>();
       const int d = fwd ? step : ndiag - 1 - step;
       const int i = d - j;
-      const bool live = row && i >= 0 && i < ni;
-      NbrState self{};
-      float4 r = zero, fi = zero, fj = zero;
-      float inv_d = 0.f;
-      if (live) {
-        // Everything here is independent of dQ.
-        const int slot = (step % kSweepDepth) * nt + j;
-        r = ring_r[slot];
-        fi = ring_fi[slot];
-        fj = ring_fj[slot];
-        inv_d = __frcp_rn(ring_d[slot]);
-        self = derive(ring_q[slot], gamma, gm1);
-      }
-      const float sx = fwd ? -1.f : 1.f;  // the flux leaves the cell being solved
-      const float rad_i = live ? spectral(self, fi.x, fi.y) : 0.f;
-      const float rad_j = live ? spectral(self, fj.x, fj.y) : 0.f;
-      // Neighbour across the j-face: thread j -+ 1's cell of the last step.
-      const int nb = fwd ? j - 1 : j + 1;
-      const bool has_j = live && (fwd ? j > 0 : j < nj - 1);
-      const bool has_i = live && (fwd ? i > 0 : i < ni - 1);
-      NbrState other = self;
-      float4 other_dq = zero;
-      if (has_j) {
-        const int b = ((step - 1) & 1) * nt + nb;
-        other.q = xq[b];
-        other.w = xw[b];
-        other_dq = xd[b];
-      }
-      if (live) {
-        const float4 dq_i = has_i ? prev_dq : zero;
-        const NbrState& si = has_i ? prev : self;
-        const float lam_i = fmaxf(spectral(si, fi.x, fi.y), rad_i) * fi.z;
-        const float lam_j = fmaxf(spectral(other, fj.x, fj.y), rad_j) * fj.z;
+      if (row && i >= 0 && i < ni) {
+        const float4 q = *at(step, REC_Q), w = *at(step, REC_W);
+        const float4 fw = *at(step, REC_FW), fs = *at(step, REC_FS);
+        const float4 base = *at(step, fwd ? REC_R : REC_SIZE);
+        const bool has_i = fwd ? i > 0 : i < ni - 1;
+        const bool has_j = fwd ? j > 0 : j < nj - 1;
+        // Across the j-face: the cell thread j -+ 1 finished last step.
+        float4 oq = q, ow = w, od = zero, of = fs;
+        if (has_j) {
+          const int b = ((step - 1) & 1) * nt + (fwd ? j - 1 : j + 1);
+          oq = xq[b];
+          ow = xw[b];
+          od = xd[b];
+          if (!fwd) of = xf[b];
+        }
+        // Forward: the faces are this cell's west and south faces, the flux
+        // leaving through -n; backward: the east neighbour's west face and
+        // the north neighbour's south face, through +n.
+        const float s = fwd ? -1.f : 1.f;
+        const float4 face_i = fwd ? fw : pfw;
+        const float4 face_j = fwd ? fs : of;
         float4 sum = zero;
-        neighbour_change(sum, si, dq_i, sx * fi.x, sx * fi.y, 0.5f * fi.z, half_omega * lam_i, gm1);
-        neighbour_change(sum, other, other_dq, sx * fj.x, sx * fj.y, 0.5f * fj.z,
-                         half_omega * lam_j, gm1);
+        neighbour_change(sum, has_i ? pq : q, has_i ? pw : w, has_i ? pd : zero, s * face_i.x,
+                         s * face_i.y, face_i.z, face_i.w, gm1);
+        neighbour_change(sum, oq, ow, od, s * face_j.x, s * face_j.y, face_j.z, face_j.w, gm1);
+        const float inv_d = w.w;
         float4 dq;
         if (fwd) {
-          dq = make_float4((r.x - sum.x) * inv_d, (r.y - sum.y) * inv_d, (r.z - sum.z) * inv_d,
-                           (r.w - sum.w) * inv_d);
+          dq = make_float4((base.x - sum.x) * inv_d, (base.y - sum.y) * inv_d,
+                           (base.z - sum.z) * inv_d, (base.w - sum.w) * inv_d);
         } else {
-          dq = make_float4(r.x - sum.x * inv_d, r.y - sum.y * inv_d, r.z - sum.z * inv_d,
-                           r.w - sum.w * inv_d);
+          dq = make_float4(base.x - sum.x * inv_d, base.y - sum.y * inv_d,
+                           base.z - sum.z * inv_d, base.w - sum.w * inv_d);
         }
         const int b = (step & 1) * nt + j;
-        xq[b] = self.q;
-        xw[b] = self.w;
+        xq[b] = q;
+        xw[b] = w;
         xd[b] = dq;
+        xf[b] = fs;
         A.dq[cell0 + i] = dq;
-        prev = self;
-        prev_dq = dq;
+        pq = q;
+        pw = w;
+        pd = dq;
+        pfw = fw;
       }
       __syncthreads();
       fetch(step + kSweepDepth);
@@ -274,24 +237,23 @@ __global__ void __launch_bounds__(TILE_THREADS) lusgs_update_kernel(const CaseDe
 }
 
 // Launches the sweep kernel with the deepest prefetch ring that fits the
-// shared memory of one CTA (8 slots for up to 384 rows, 4 beyond).
+// shared memory of one CTA.
+template <int kDepth>
+inline cudaError_t launch_sweep_depth(const SweepArgs& A, int n_cases, int nt, cudaStream_t stream) {
+  const size_t bytes = sweep_smem_bytes(nt, kDepth);
+  const cudaError_t e = cudaFuncSetAttribute(lusgs_sweep_kernel<kDepth>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+  if (e != cudaSuccess) return e;
+  lusgs_sweep_kernel<kDepth><<<n_cases, nt, bytes, stream>>>(A);
+  return cudaGetLastError();
+}
+
 inline cudaError_t launch_sweep(const SweepArgs& A, int n_cases, int max_nj, cudaStream_t stream) {
   const int nt = ((max_nj + 31) / 32) * 32;
   constexpr size_t kLimit = 227 * 1024;
-  const size_t deep = sweep_smem_bytes(nt, 8);
-  if (deep <= kLimit) {
-    cudaError_t e = cudaFuncSetAttribute(lusgs_sweep_kernel<8>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(deep));
-    if (e != cudaSuccess) return e;
-    lusgs_sweep_kernel<8><<<n_cases, nt, deep, stream>>>(A);
-    return cudaGetLastError();
-  }
-  const size_t shallow = sweep_smem_bytes(nt, 4);
-  cudaError_t e = cudaFuncSetAttribute(lusgs_sweep_kernel<4>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(shallow));
-  if (e != cudaSuccess) return e;
-  lusgs_sweep_kernel<4><<<n_cases, nt, shallow, stream>>>(A);
-  return cudaGetLastError();
+  if (sweep_smem_bytes(nt, 8) <= kLimit) return launch_sweep_depth<8>(A, n_cases, nt, stream);
+  if (sweep_smem_bytes(nt, 6) <= kLimit) return launch_sweep_depth<6>(A, n_cases, nt, stream);
+  return launch_sweep_depth<3>(A, n_cases, nt, stream);
 }
 
 }  // namespace bsd

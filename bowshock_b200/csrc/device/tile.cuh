@@ -35,9 +35,7 @@ struct TileArgs {
   unsigned* status;       // per case status bits
   double a, b;            // STAGE coefficients
   int first_stage;        // STAGE: compute the time step from src (== u0)
-  float4* r32;            // PREPARE outputs
-  float4* q32;
-  float* diag;
+  float4* rec;            // PREPARE output: the sweep record of each cell (5 float4)
   const float* cfl;       // PREPARE: per case current implicit CFL number
   const float* omega;     // PREPARE: per case omega
   double* res_out;        // RESIDUAL: 4 values per cell, arena like the state
@@ -200,8 +198,10 @@ __global__ void __launch_bounds__(TILE_THREADS) tile_kernel(const TileArgs<R> A)
       A.out.store(k, o);
       if (!is_physical(o, gamma)) atomicOr(&A.status[c], STATUS_NON_PHYSICAL);
     } else if (MODE == MODE_PREPARE) {
-      A.r32[k] = make_float4(float(res[0]), float(res[1]), float(res[2]), float(res[3]));
-      A.q32[k] = make_float4(float(qs.rho), float(qs.mu), float(qs.mv), float(qs.e));
+      // The sweep record (see lusgs_sweep_kernel): residual, state, (u, v,
+      // p, 1/D), and the west and south faces with their half areas and
+      // damping omega lambda A / 2 - everything the sweeps need that does
+      // not depend on dQ, computed here where every cell is independent.
       const float g = float(gamma);
       const float4 fw = A.m.iface[cd.iface + i + int64_t(j) * (ni + 1)];
       const float4 fe = A.m.iface[cd.iface + i + 1 + int64_t(j) * (ni + 1)];
@@ -215,8 +215,15 @@ __global__ void __launch_bounds__(TILE_THREADS) tile_kernel(const TileArgs<R> A)
       const float le = fmaxf(rad(sj, si, fe.x, fe.y), i + 1 < ni ? rad(sj, si + 1, fe.x, fe.y) : 0.f) * fe.z;
       const float ls = fmaxf(j > 0 ? rad(sj - 1, si, fs.x, fs.y) : 0.f, rad(sj, si, fs.x, fs.y)) * fs.z;
       const float ln = fmaxf(rad(sj, si, fn.x, fn.y), j + 1 < nj ? rad(sj + 1, si, fn.x, fn.y) : 0.f) * fn.z;
-      const float scale = 0.5f * (A.omega[c] + 1.f / A.cfl[c]);
-      A.diag[k] = scale * (lw + le + ls + ln) + (cd.axisym ? cm.y * rad(sj, si, 0.f, 1.f) : 0.f);
+      const float omega = A.omega[c];
+      const float scale = 0.5f * (omega + 1.f / A.cfl[c]);
+      const float diag = scale * (lw + le + ls + ln) + (cd.axisym ? cm.y * rad(sj, si, 0.f, 1.f) : 0.f);
+      float4* rec = A.rec + 5 * k;
+      rec[0] = make_float4(float(res[0]), float(res[1]), float(res[2]), float(res[3]));
+      rec[1] = make_float4(float(qs.rho), float(qs.mu), float(qs.mv), float(qs.e));
+      rec[2] = make_float4(float(W[1][sj][si]), float(W[2][sj][si]), float(W[3][sj][si]), 1.f / diag);
+      rec[3] = make_float4(fw.x, fw.y, 0.5f * fw.z, 0.5f * omega * lw);
+      rec[4] = make_float4(fs.x, fs.y, 0.5f * fs.z, 0.5f * omega * ls);
     } else if (A.res_out != nullptr) {
       double* o = A.res_out + 4 * k;
       o[0] = double(res[0]);

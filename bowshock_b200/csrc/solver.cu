@@ -605,11 +605,9 @@ class Solver final : public SolverBase {
   }
 
   bs_status ensure_implicit() {
-    if (r32_.p != nullptr) return BS_OK;
-    BS_CUDA(r32_.alloc(total_cells_));
-    BS_CUDA(q32_.alloc(total_cells_));
+    if (rec_.p != nullptr) return BS_OK;
+    BS_CUDA(rec_.alloc(5 * size_t(total_cells_)));
     BS_CUDA(dq_.alloc(total_cells_));
-    BS_CUDA(diag_.alloc(total_cells_));
     return BS_OK;
   }
 
@@ -659,9 +657,7 @@ class Solver final : public SolverBase {
     A.a = a;
     A.b = b;
     A.first_stage = first ? 1 : 0;
-    A.r32 = r32_.p;
-    A.q32 = q32_.p;
-    A.diag = diag_.p;
+    A.rec = rec_.p;
     A.cfl = cfl_.p;
     A.omega = omega_.p;
     A.res_out = res_out;
@@ -720,9 +716,7 @@ class Solver final : public SolverBase {
     S.case_list = d_case_list_.p;
     S.active = d_active_.p;
     S.m = metrics();
-    S.r32 = r32_.p;
-    S.q32 = q32_.p;
-    S.diag = diag_.p;
+    S.rec = rec_.p;
     S.dq = dq_.p;
     S.cfl = cfl_.p;
     S.cfl_max = cflmax_.p;
@@ -842,8 +836,8 @@ class Solver final : public SolverBase {
   DevBuf<int2> d_tiles_;
   DevBuf<int> d_case_list_, d_active_;
   DevBuf<R> q_[4], s1_[4], s2_[4];
-  DevBuf<float> dt_, diag_, cfl_, cflmax_, growth_, omega_;
-  DevBuf<float4> iface_, jface_, r32_, q32_, dq_;
+  DevBuf<float> dt_, cfl_, cflmax_, growth_, omega_;
+  DevBuf<float4> iface_, jface_, rec_, dq_;
   DevBuf<float2> cellm_;
   DevBuf<double> norm_, bgeom_, bflux_, force_, res_out_;
   DevBuf<unsigned> status_, dtmin_;

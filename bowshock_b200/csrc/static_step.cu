@@ -40,13 +40,11 @@ constexpr size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign;
 constexpr size_t kOffCase = 0;
 constexpr size_t kOffTiles = kOffCase + align_up(sizeof(bsd::CaseDev));
 constexpr size_t kOffWords = kOffTiles + align_up(sizeof(int2) * kStaticMaxTiles);
-constexpr size_t kOffR32 = kOffWords + kAlign;
-constexpr size_t kOffQ32 = kOffR32 + align_up(sizeof(float4) * kStaticMaxCells);
-constexpr size_t kOffDq = kOffQ32 + align_up(sizeof(float4) * kStaticMaxCells);
-constexpr size_t kOffDiag = kOffDq + align_up(sizeof(float4) * kStaticMaxCells);
-constexpr size_t kStaticBytes = kOffDiag + align_up(sizeof(float) * kStaticMaxCells);
+constexpr size_t kOffRec = kOffWords + kAlign;
+constexpr size_t kOffDq = kOffRec + align_up(5 * sizeof(float4) * kStaticMaxCells);
+constexpr size_t kStaticBytes = kOffDq + align_up(sizeof(float4) * kStaticMaxCells);
 
-// The scratch: about 3.4 MB on every device that loads the library.
+// The scratch: about 6.3 MB on every device that loads the library.
 static __device__ __align__(256) unsigned char g_step_scratch[kStaticBytes];
 
 // The per-case words inside the kOffWords region.
@@ -158,10 +156,8 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
   auto* d_case = reinterpret_cast<bsd::CaseDev*>(base + kOffCase);
   auto* d_tiles = reinterpret_cast<int2*>(base + kOffTiles);
   auto* d_words = reinterpret_cast<Words*>(base + kOffWords);
-  auto* d_r32 = reinterpret_cast<float4*>(base + kOffR32);
-  auto* d_q32 = reinterpret_cast<float4*>(base + kOffQ32);
+  auto* d_rec = reinterpret_cast<float4*>(base + kOffRec);
   auto* d_dq = reinterpret_cast<float4*>(base + kOffDq);
-  auto* d_diag = reinterpret_cast<float*>(base + kOffDiag);
 
   cudaError_t err = cudaMemcpyAsync(d_case, &cd, sizeof(cd), cudaMemcpyHostToDevice, st);
   if (err == cudaSuccess) {
@@ -184,9 +180,7 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
     A.status = &d_words->status;
     A.a = 0;
     A.b = 1;
-    A.r32 = d_r32;
-    A.q32 = d_q32;
-    A.diag = d_diag;
+    A.rec = d_rec;
     A.cfl = &d_words->cfl;
     A.omega = &d_words->omega;
     bsd::tile_kernel<double, bsd::MODE_PREPARE><<<n_tiles, bsd::TILE_THREADS, 0, st>>>(A);
@@ -197,9 +191,7 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
     S.cases = d_case;
     S.case_list = &d_words->case_list;
     S.m = m;
-    S.r32 = d_r32;
-    S.q32 = d_q32;
-    S.diag = d_diag;
+    S.rec = d_rec;
     S.dq = d_dq;
     S.cfl = &d_words->cfl;
     S.cfl_max = &d_words->cfl_max;
