@@ -5,7 +5,9 @@
 //              ni nj cells of the case at `cell`, cell (i, j) at i + j ni;
 //   i-faces    float4 (nx, ny, area, 0), (ni + 1) nj at `iface`;
 //   j-faces    float4 (nx, ny, area, 0), ni (nj + 1) at `jface`;
-//   cells      float2 (volume, planar area) at `cell`.
+//   cells      float2 (volume, planar area) at `cell`;
+//   LU-SGS     per-cell sweep records and corrections in diagonal-major
+//              order, (ni + nj - 1) nj slots at `skew` (skew_slot).
 // Metrics are computed in FP64 on the host and stored as FP32. The state is
 // stored in the solve's arithmetic type R: double for the steady solves
 // (the residual that decides convergence is evaluated in FP64), float for
@@ -26,12 +28,22 @@ constexpr int TILE_THREADS = TI * TJ;
 
 // Per-case status bits.
 constexpr unsigned STATUS_NON_PHYSICAL = 1u;
+// A kernel gave up waiting for an asynchronous copy (bounded wait).
+constexpr unsigned STATUS_TIMEOUT = 2u;
+
+// Slot of cell (i, j) in a case's diagonal-major ("skewed") LU-SGS arrays:
+// anti-diagonal d = i + j, then j, so the cells of consecutive diagonals are
+// one contiguous range.
+__host__ __device__ __forceinline__ int64_t skew_slot(int i, int j, int nj) {
+  return int64_t(i + j) * nj + j;
+}
 
 struct CaseDev {
   int32_t ni, nj;
   int64_t cell;   // offset of the case's cell arrays
   int64_t iface;  // offset of its i-face arrays
   int64_t jface;  // offset of its j-face arrays
+  int64_t skew;   // offset of its diagonal-major LU-SGS arrays, (ni + nj - 1) nj slots
   int32_t bc[4];  // bs_bc_kind per side
   int32_t flux, limiter, recon, axisym;
   int32_t integrator, local_dt;

@@ -35,7 +35,7 @@ struct TileArgs {
   unsigned* status;       // per case status bits
   double a, b;            // STAGE coefficients
   int first_stage;        // STAGE: compute the time step from src (== u0)
-  float4* rec;            // PREPARE output: the sweep record of each cell (5 float4)
+  float4* rec;            // PREPARE output: each cell's sweep record (5 float4, skewed)
   const float* cfl;       // PREPARE: per case current implicit CFL number
   const float* omega;     // PREPARE: per case omega
   double* res_out;        // RESIDUAL: 4 values per cell, arena like the state
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(TILE_THREADS) tile_kernel(const TileArgs<R> A)
       const float omega = A.omega[c];
       const float scale = 0.5f * (omega + 1.f / A.cfl[c]);
       const float diag = scale * (lw + le + ls + ln) + (cd.axisym ? cm.y * rad(sj, si, 0.f, 1.f) : 0.f);
-      float4* rec = A.rec + 5 * k;
+      float4* rec = A.rec + 5 * (cd.skew + skew_slot(i, j, nj));
       rec[0] = make_float4(float(res[0]), float(res[1]), float(res[2]), float(res[3]));
       rec[1] = make_float4(float(qs.rho), float(qs.mu), float(qs.mv), float(qs.e));
       rec[2] = make_float4(float(W[1][sj][si]), float(W[2][sj][si]), float(W[3][sj][si]), 1.f / diag);

@@ -121,7 +121,7 @@ class Solver final : public SolverBase {
     BS_CUDA(cudaEventCreate(&ev1_));
     std::vector<bsd::CaseDev> hc(n_);
     std::vector<int2> tiles;
-    int64_t cell = 0, ifc = 0, jfc = 0, bfc = 0;
+    int64_t cell = 0, ifc = 0, jfc = 0, bfc = 0, skw = 0;
     boundary_off_.resize(n_);
     cell_off_.resize(n_);
     for (int c = 0; c < n_; c++) {
@@ -134,6 +134,8 @@ class Solver final : public SolverBase {
       d.cell = cell;
       d.iface = ifc;
       d.jface = jfc;
+      d.skew = skw;
+      skw += int64_t(cfg.ni + cfg.nj - 1) * cfg.nj;
       for (int s = 0; s < 4; s++) d.bc[s] = cfg.boundaries[s].kind;
       d.flux = cfg.flux;
       d.limiter = cfg.limiter;
@@ -167,6 +169,7 @@ class Solver final : public SolverBase {
       max_along_ = std::max(max_along_, std::max(cfg.ni, cfg.nj));
     }
     total_cells_ = cell;
+    total_skew_ = skw;
     n_tiles_ = int(tiles.size());
     steps_.assign(n_, 0);
     active_h_.assign(n_, 1);
@@ -606,8 +609,8 @@ class Solver final : public SolverBase {
 
   bs_status ensure_implicit() {
     if (rec_.p != nullptr) return BS_OK;
-    BS_CUDA(rec_.alloc(5 * size_t(total_cells_)));
-    BS_CUDA(dq_.alloc(total_cells_));
+    BS_CUDA(rec_.alloc(5 * size_t(total_skew_)));
+    BS_CUDA(dq_.alloc(total_skew_));
     return BS_OK;
   }
 
@@ -826,6 +829,7 @@ class Solver final : public SolverBase {
   std::vector<HostCase> cases_;
   int n_ = 0;
   int64_t total_cells_ = 0;
+  int64_t total_skew_ = 0;
   int n_tiles_ = 0;
   int max_nj_ = 0, max_along_ = 0;
   bool any_global_dt_ = false;

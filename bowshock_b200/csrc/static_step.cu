@@ -11,8 +11,8 @@
 // kernels) lives in one file-scope static device array of fixed size that the
 // library reserves on every GPU that loads it, for as long as the process runs.
 //
-// Limits and sharing: at most kStaticMaxCells cells (ni nj) and at most 512
-// cells across (nj). Every call uses the same array, which keeps the last
+// Limits and sharing: at most kStaticMaxCells cells (ni nj), kStaticMaxSlots
+// diagonal slots ((ni + nj - 1) nj) and 512 cells across (nj). Every call uses the same array, which keeps the last
 // call's contents; the per-call words that must start at zero are cleared by
 // each call. Calls whose work overlaps on the GPU (from several threads, or on
 // several streams of one device) race on the array; the caller must order them.
@@ -31,6 +31,8 @@
 namespace {
 
 constexpr int64_t kStaticMaxCells = 65536;
+// Diagonal-major slots, (ni + nj - 1) nj, of the LU-SGS records.
+constexpr int64_t kStaticMaxSlots = 98304;
 constexpr int kStaticMaxTiles = 4096;
 constexpr int kMaxDevices = 64;
 
@@ -41,10 +43,10 @@ constexpr size_t kOffCase = 0;
 constexpr size_t kOffTiles = kOffCase + align_up(sizeof(bsd::CaseDev));
 constexpr size_t kOffWords = kOffTiles + align_up(sizeof(int2) * kStaticMaxTiles);
 constexpr size_t kOffRec = kOffWords + kAlign;
-constexpr size_t kOffDq = kOffRec + align_up(5 * sizeof(float4) * kStaticMaxCells);
-constexpr size_t kStaticBytes = kOffDq + align_up(sizeof(float4) * kStaticMaxCells);
+constexpr size_t kOffDq = kOffRec + align_up(5 * sizeof(float4) * kStaticMaxSlots);
+constexpr size_t kStaticBytes = kOffDq + align_up(sizeof(float4) * kStaticMaxSlots);
 
-// The scratch: about 6.3 MB on every device that loads the library.
+// The scratch: about 9.5 MB on every device that loads the library.
 static __device__ __align__(256) unsigned char g_step_scratch[kStaticBytes];
 
 // The per-case words inside the kOffWords region.
@@ -114,6 +116,12 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
                     "the grid has " + std::to_string(n_cells) +
                         " cells; the allocation-free step takes at most " +
                         std::to_string(kStaticMaxCells));
+  const int64_t n_slots = int64_t(ni + nj - 1) * nj;
+  if (n_slots > kStaticMaxSlots)
+    return bs::fail(BS_INVALID_ARGUMENT,
+                    "the grid needs " + std::to_string(n_slots) +
+                        " diagonal slots ((ni + nj - 1) nj); the allocation-free step takes at most " +
+                        std::to_string(kStaticMaxSlots));
   const int n_tiles = ((ni + bsd::TI - 1) / bsd::TI) * ((nj + bsd::TJ - 1) / bsd::TJ);
   if (n_tiles > kStaticMaxTiles)
     return bs::fail(BS_INVALID_ARGUMENT, "the grid needs more tiles than the static scratch holds");
@@ -133,6 +141,7 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
   cd.cell = 0;
   cd.iface = 0;
   cd.jface = 0;
+  cd.skew = 0;
   for (int k = 0; k < 4; k++) cd.bc[k] = config->boundaries[k].kind;
   cd.flux = config->flux;
   cd.limiter = config->limiter;
