@@ -93,6 +93,7 @@ SIGNATURES: dict[str, list] = {
     "bs_lusgs_step_static": [C.POINTER(abi.Config), _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_double,
                              C.c_double, _vp, _dp, _ip],
     "bs_body_grid": [C.POINTER(abi.Body), C.POINTER(abi.BodyGridOptions), C.POINTER(_vp)],
+    "bs_blunt_body_grid": [C.POINTER(abi.Body), C.POINTER(abi.BodyGridOptions), C.POINTER(_vp)],
     "bs_ramp_grid": [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
                      C.c_double, C.POINTER(_vp)],
     "bs_grid_dims": [_vp, _ip, _ip],

@@ -44,6 +44,7 @@ TIME_STEPPING = {"local": 0, "global": 1}
 BC_KIND = {"inflow": 0, "outflow": 1, "wall": 2, "farField": 3, "periodic": 4}
 SIDES = ("iMin", "iMax", "jMin", "jMax")
 SIDE = {name: k for k, name in enumerate(SIDES)}
+GRID_UNGATED = 1
 NOSE_KIND = {"conical": 0, "ogive": 1, "ellipsoid": 2, "power": 3, "parabolic": 4, "haack": 5}
 
 
@@ -108,7 +109,7 @@ class BodyGridOptions(C.Structure):
         ("nj", C.c_int32),
         ("refinement", C.c_int32),
         ("ni", C.c_int32),
-        ("reserved", C.c_int32),
+        ("flags", C.c_int32),
         ("mach", C.c_double),
         ("gamma", C.c_double),
     ]

@@ -49,6 +49,28 @@ bs_status bs_body_grid(const bs_body* body, const bs_body_grid_options* options,
   return bs::ok();
 }
 
+bs_status bs_blunt_body_grid(const bs_body* body, const bs_body_grid_options* options,
+                             bs_grid** out) {
+  if (body == nullptr || options == nullptr || out == nullptr)
+    return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  bs::BluntGridOptions o;
+  o.nj = options->nj;
+  o.refinement = options->refinement <= 0 ? 1 : options->refinement;
+  o.ni = options->ni;
+  o.mach = options->mach;
+  o.gated = (options->flags & BS_GRID_UNGATED) == 0;
+  auto* g = new (std::nothrow) bs_grid;
+  if (g == nullptr) return bs::fail(BS_MEMORY_LIMIT, "out of host memory");
+  bool quality = false;
+  const std::string e = bs::blunt_body_grid(to_body(*body), o, &g->g, &quality);
+  if (!e.empty()) {
+    delete g;
+    return bs::fail(quality ? BS_GRID_QUALITY : BS_INVALID_ARGUMENT, e);
+  }
+  *out = g;
+  return bs::ok();
+}
+
 bs_status bs_ramp_grid(int32_t ni, int32_t nj, double x_min, double x_corner, double x_max,
                        double height, double angle, bs_grid** out) {
   if (out == nullptr || ni < 1 || nj < 1) return bs::fail(BS_INVALID_ARGUMENT, "invalid argument");

@@ -79,11 +79,13 @@ std::vector<std::string> quality_failures(const GridQuality& q, const QualityLim
 
 std::vector<double> column_positions(const std::vector<double>& bp,
                                      const std::function<double(double)>& density, int refinement,
-                                     int total) {
+                                     int total, double max_spacing_slope) {
   struct Table {
     double a, b;
     int samples;
+    std::vector<double> values;
     std::vector<double> cumulative;
+    double at(int n) const { return a + ((b - a) * n) / samples; }
   };
   std::vector<Table> tables;
   for (size_t k = 1; k < bp.size(); k++) {
@@ -93,14 +95,36 @@ std::vector<double> column_positions(const std::vector<double>& bp,
     // At least 64 samples per base-grid node, estimated from the ends.
     const double baseNodes = (((density(t.a) + density(t.b)) / 2) * (t.b - t.a)) / refinement;
     t.samples = std::max(2048, 64 * int(std::ceil(baseNodes)));
-    std::vector<double> values(t.samples + 1);
-    auto at = [&](int n) { return t.a + ((t.b - t.a) * n) / t.samples; };
-    for (int n = 0; n <= t.samples; n++) values[n] = density(at(n));
+    t.values.resize(t.samples + 1);
+    for (int n = 0; n <= t.samples; n++) t.values[n] = density(t.at(n));
+    tables.push_back(std::move(t));
+  }
+  if (max_spacing_slope > 0) {
+    // limitSpacingSlope (src/grid/spacing.ts:84-113): the largest spacing
+    // below the given one whose slope is at most the limit, by a forward and
+    // a backward pass over all samples in order along the line, on the base
+    // grid's spacing (the density divided by the refinement).
+    std::vector<double> xs, spacing;
+    for (const Table& t : tables)
+      for (int n = 0; n <= t.samples; n++) {
+        xs.push_back(t.at(n));
+        spacing.push_back(refinement / t.values[n]);
+      }
+    std::vector<double> limited = spacing;
+    for (size_t k = 1; k < limited.size(); k++)
+      limited[k] = std::min(limited[k], limited[k - 1] + max_spacing_slope * (xs[k] - xs[k - 1]));
+    for (size_t k = limited.size() - 1; k-- > 0;)
+      limited[k] = std::min(limited[k], limited[k + 1] + max_spacing_slope * (xs[k + 1] - xs[k]));
+    size_t k = 0;
+    for (Table& t : tables)
+      for (int n = 0; n <= t.samples; n++, k++)
+        if (limited[k] < spacing[k]) t.values[n] = refinement / limited[k];
+  }
+  for (Table& t : tables) {
     t.cumulative.assign(t.samples + 1, 0.0);
     for (int n = 1; n <= t.samples; n++)
       t.cumulative[n] =
-          t.cumulative[n - 1] + 0.5 * (values[n - 1] + values[n]) * (at(n) - at(n - 1));
-    tables.push_back(std::move(t));
+          t.cumulative[n - 1] + 0.5 * (t.values[n - 1] + t.values[n]) * (t.at(n) - t.at(n - 1));
   }
   // Intervals per breakpoint interval.
   std::vector<int> counts(tables.size());
@@ -145,7 +169,7 @@ std::vector<double> column_positions(const std::vector<double>& bp,
   std::vector<double> xs{bp[0]};
   for (size_t k = 0; k < tables.size(); k++) {
     const Table& t = tables[k];
-    auto at = [&](int n) { return t.a + ((t.b - t.a) * n) / t.samples; };
+    auto at = [&](int n) { return t.at(n); };
     const double integral = t.cumulative[t.samples];
     const int count = counts[k];
     int n = 0;
@@ -256,6 +280,278 @@ std::string body_grid(const Body& body, const BodyGridOptions& o, Grid* out, boo
       out->x[k] = xs[i];
       out->y[k] = a.wall + (a.h * std::expm1((a.b * j) / nj)) / std::expm1(a.b);
     }
+  const std::vector<std::string> failures =
+      quality_failures(grid_quality(ni, nj, out->x.data(), out->y.data()), limits);
+  if (!failures.empty()) {
+    *quality_error = true;
+    std::string msg = "the generated grid fails its quality checks: ";
+    for (size_t k = 0; k < failures.size(); k++) msg += (k ? "; " : "") + failures[k];
+    return msg;
+  }
+  return "";
+}
+
+namespace {
+
+// Stretching towards the body along a line of height h (lineStrength,
+// src/grid/blunt-grid.ts:547-549): b = ln(1 + h / R), capped by the
+// aspect-ratio limit.
+double line_strength(double h, double radius, const QualityLimits& q) {
+  return std::min(std::log1p(h / radius), 2 * std::log(q.max_aspect_ratio));
+}
+
+double stretched_fraction(double b, int j, int nj) {
+  return std::expm1((b * j) / nj) / std::expm1(b);
+}
+
+}  // namespace
+
+std::string blunt_body_grid(const Body& body, const BluntGridOptions& o, Grid* out,
+                            bool* quality_error) {
+  *quality_error = false;
+  std::string e = validate_body(body);
+  if (!e.empty()) return e;
+  const int refinement = o.refinement;
+  if (!(o.nj >= 4)) return "a body grid needs at least 4 cells across";
+  if (!(refinement >= 1 && (refinement & (refinement - 1)) == 0))
+    return "the refinement must be 1, 2, 4, 8, ...";
+  if (o.ni > 0 && refinement != 1) return "an exact column count needs refinement 1";
+  if (!(o.mach > 1)) return "blunt-body grids are for supersonic free streams";
+  const QualityLimits limits;
+  // Placement constants (DEFAULT_TUNING, blunt-grid.ts:130-137).
+  const double kStandoffFactor = 2, kArcRadiusFactor = 2, kTipScaleFactor = 2;
+  const double kSmoothing = 0.25, kFanRatio = 1.25, kMaxWidthSlope = 0.5;
+  const double kMaxNoseRadius = 10, kMaxShoulderAngle = 15 * M_PI / 180;
+  const int kWidthSamples = 4096, kUniformWidthSamples = 1024, kSpacingSamples = 8192;
+  const int kWindowSamples = 64, kProfileSamples = 20000;
+
+  const Nose& nose = body.nose;
+  const bool sharp = std::isfinite(nose_tip_slope(nose));
+  const bool ellipsoid = nose.kind == NOSE_ELLIPSOID;
+  const double L = nose.length, R = nose.base_radius;
+
+  // The profile by arc length, sampled in u with x = L u^2 (clustered at the tip).
+  auto profile_x = [&](double u) { return L * u * u; };
+  auto profile_r = [&](double u) { return nose_radius(nose, profile_x(u)); };
+  std::vector<double> u_of(kProfileSamples + 1, 0.0), s_of(kProfileSamples + 1, 0.0);
+  for (int k = 1; k <= kProfileSamples; k++) {
+    const double u0 = double(k - 1) / kProfileSamples, u1 = double(k) / kProfileSamples;
+    u_of[k] = u1;
+    s_of[k] = s_of[k - 1] + std::hypot(profile_x(u1) - profile_x(u0), profile_r(u1) - profile_r(u0));
+  }
+  const double s_nose = s_of[kProfileSamples];
+  const double s_end = s_nose + body.cylinder_length;
+  auto u_at = [&](double s) {
+    int low = 0, high = kProfileSamples;
+    while (high - low > 1) {
+      const int mid = (low + high) >> 1;
+      if (s_of[mid] <= s) low = mid;
+      else high = mid;
+    }
+    const double f = (s - s_of[low]) / (s_of[high] - s_of[low]);
+    return u_of[low] + std::min(std::max(f, 0.0), 1.0) / kProfileSamples;
+  };
+  struct SurfacePoint {
+    double x, y, nx, ny;
+  };
+  // The body point at arc length s and its outward normal.
+  auto surface = [&](double s) -> SurfacePoint {
+    if (s >= s_nose) return {L + (s - s_nose), R, 0, 1};
+    const double u = u_at(s);
+    const double x = profile_x(u), y = profile_r(u);
+    if (u == 0) return {x, y, -1, 0};
+    const double eps = 1e-7;
+    const double ua = std::max(u - eps, 0.0), ub = std::min(u + eps, 1.0);
+    const double tx = profile_x(ub) - profile_x(ua), ty = profile_r(ub) - profile_r(ua);
+    const double t = std::hypot(tx, ty);
+    return {x, y, -ty / t, tx / t};
+  };
+  const SurfacePoint shoulder = surface(s_nose * (1 - 1e-9));
+  const double shoulder_angle = std::atan2(-shoulder.nx, shoulder.ny);
+  if (!(shoulder_angle <= kMaxShoulderAngle))
+    return "blunt noses meeting the body at more than 15 deg are not supported";
+
+  // Length scales: the tip's radius of curvature, and the tip scale (the x
+  // at which the profile crosses r = x).
+  const double x_small = 1e-6 * L;
+  const double r_small = nose_radius(nose, x_small);
+  const double tip_radius = r_small * r_small / (2 * x_small);
+  if (!(tip_radius <= kMaxNoseRadius * R)) return "noses that are nearly flat at the tip are not supported";
+  double tip_scale = 0;
+  if (!sharp) {
+    if (nose_radius(nose, L) > L) {
+      tip_scale = L;
+    } else {
+      double low = 0, high = L;
+      for (int k = 0; k < 200; k++) {
+        const double mid = 0.5 * (low + high);
+        if (nose_radius(nose, mid) > mid) low = mid;
+        else high = mid;
+      }
+      tip_scale = 0.5 * (low + high);
+    }
+  }
+  const double scale = ellipsoid ? std::max(tip_radius, R)
+                                 : sharp ? R
+                                         : std::max(tip_radius, std::min(R, kTipScaleFactor * tip_scale));
+
+  // Outer boundary: an arc ahead of the tip (standoff from Billig's
+  // correlation, billigStandoff, blunt-grid.ts:99-101), then a straight line.
+  const double outer_angle = (M_PI / 2 + std::asin(1 / o.mach)) / 2;
+  const double arc_radius = kArcRadiusFactor * scale;
+  const double standoff = kStandoffFactor * 0.143 * std::exp(3.24 / (o.mach * o.mach)) * scale;
+  const double centre = arc_radius - standoff;
+  const double y_join = arc_radius * std::cos(outer_angle);
+  const double x_join = centre - arc_radius * std::sin(outer_angle);
+  auto outer_x = [&](double y) {
+    return y <= y_join ? centre - std::sqrt(arc_radius * arc_radius - y * y)
+                       : x_join + (y - y_join) / std::tan(outer_angle);
+  };
+  bool reaches = false;
+  // Distance from the body point at s to the outer boundary along (dx, dy).
+  auto length_along = [&](double s, double dx, double dy) {
+    const SurfacePoint p = surface(s);
+    auto outside = [&](double d) { return p.x + d * dx - outer_x(p.y + d * dy) <= 0; };
+    if (outside(0)) {
+      reaches = true;
+      return R;
+    }
+    double high = R;
+    while (!outside(high)) high *= 2;
+    double low = 0;
+    for (int k = 0; k < 60; k++) {
+      const double mid = (low + high) / 2;
+      if (outside(mid)) high = mid;
+      else low = mid;
+    }
+    return high;
+  };
+  auto width_at = [&](double s) {
+    const SurfacePoint p = surface(s);
+    return std::min(kSmoothing * length_along(s, p.nx, p.ny), s_end - s);
+  };
+  // The smoothing window's half-width along the body, tabulated and limited
+  // to change by at most kMaxWidthSlope per unit length.
+  std::vector<double> width_s, widths;
+  const bool uniform = ellipsoid;
+  const int nw = uniform ? kUniformWidthSamples : kWidthSamples;
+  width_s.resize(nw + 1);
+  widths.resize(nw + 1);
+  for (int k = 0; k <= nw; k++) {
+    width_s[k] = uniform ? k * (s_end / nw) : (s_end * double(k) * k) / (double(nw) * nw);
+    widths[k] = width_at(width_s[k]);
+  }
+  if (reaches) return "the body reaches the outer boundary; the nose is not supported";
+  for (int k = 1; k <= nw; k++)
+    widths[k] = std::min(widths[k], widths[k - 1] + kMaxWidthSlope * (width_s[k] - width_s[k - 1]));
+  for (int k = nw - 1; k >= 0; k--)
+    widths[k] = std::min(widths[k], widths[k + 1] + kMaxWidthSlope * (width_s[k + 1] - width_s[k]));
+  auto half_width = [&](double s) {
+    if (uniform) {
+      const double step = s_end / nw;
+      const double t = std::min(std::max(s / step, 0.0), double(nw));
+      const int k = std::min(int(std::floor(t)), nw - 1);
+      return widths[k] + (t - k) * (widths[k + 1] - widths[k]);
+    }
+    const double t = std::min(std::max(std::sqrt(std::max(s, 0.0) / s_end) * nw, 0.0), double(nw));
+    const int k = std::min(int(std::floor(t)), nw - 1);
+    const double f = (std::min(std::max(s, 0.0), s_end) - width_s[k]) / (width_s[k + 1] - width_s[k]);
+    return widths[k] + std::min(std::max(f, 0.0), 1.0) * (widths[k + 1] - widths[k]);
+  };
+  // Angle of the body normal to the upstream axis, odd about the tip.
+  std::function<double(double)> normal_angle = [&](double s) -> double {
+    if (s < 0) return -normal_angle(-s);
+    if (s >= s_nose) return M_PI / 2;
+    const SurfacePoint p = surface(s);
+    return std::atan2(p.ny, -p.nx);
+  };
+  // A sharp tip's jump in the normal, fanned out geometrically.
+  const double tip_jump = sharp ? normal_angle(s_nose * 1e-9) : 0;
+  double fan_scale = std::numeric_limits<double>::infinity();
+  if (sharp) {
+    const double h = length_along(0, -1, 0);
+    const double c = 1 / std::log(kFanRatio) / o.nj;
+    fan_scale = (h * (-tip_jump + std::sqrt(tip_jump * tip_jump + 4 * c * c))) / 2;
+  }
+  auto fan = [&](double s) { return tip_jump * -std::expm1(-s / fan_scale); };
+  std::function<double(double)> line_angle = [&](double s) -> double {
+    if (s == 0) return 0;
+    if (s < 0) return -line_angle(-s);
+    if (s >= s_end) return M_PI / 2;
+    const double w = half_width(s);
+    double sum = 0;
+    for (int k = 0; k < kWindowSamples; k++) {
+      const double t = s - w + (2 * w * (k + 0.5)) / kWindowSamples;
+      const double sign = t > 0 ? 1.0 : t < 0 ? -1.0 : 0.0;
+      sum += normal_angle(t) - sign * tip_jump;
+    }
+    return sum / kWindowSamples + fan(s);
+  };
+  auto turn_rate = [&](double s) {
+    const double ew = std::max(std::min(half_width(s) / 4, std::max(fan_scale / 4, s / 8)),
+                               s_end / kProfileSamples);
+    return (line_angle(s + ew) - line_angle(s - ew)) / (2 * ew);
+  };
+  struct Line {
+    double dx, dy, h;
+  };
+  auto line = [&](double s) -> Line {
+    const double angle = line_angle(s);
+    const double dx = -std::cos(angle), dy = std::sin(angle);
+    return {dx, dy, length_along(s, dx, dy)};
+  };
+  const int nj = o.nj * refinement;
+  // Spacing along the body: wall cells as long as the geometric mean of
+  // their height and the outer cells' height, allowing for the lines'
+  // spreading.
+  auto spacing = [&](double s) {
+    const Line l = line(s);
+    const double b = line_strength(l.h, R, limits);
+    const double wall_height = (l.h * b) / (std::expm1(b) * nj);
+    return (wall_height * std::exp(b / 2)) / std::sqrt(1 + turn_rate(s) * l.h);
+  };
+  std::vector<double> bps = body.cylinder_length > 0 ? std::vector<double>{0, s_nose, s_end}
+                                                     : std::vector<double>{0, s_nose};
+  std::vector<double> ss;
+  if (ellipsoid) {
+    ss = column_positions(bps, [&](double s) { return 1 / spacing(s); }, refinement, o.ni, 0.15);
+  } else {
+    std::vector<double> dens_s(kSpacingSamples + 1), dens(kSpacingSamples + 1);
+    for (int k = 0; k <= kSpacingSamples; k++) {
+      dens_s[k] = (s_end * double(k) * k) / (double(kSpacingSamples) * kSpacingSamples);
+      dens[k] = 1 / spacing(dens_s[k]);
+    }
+    auto tabulated = [&](double s) {
+      const double t = std::min(
+          std::max(std::sqrt(std::max(s, 0.0) / s_end) * kSpacingSamples, 0.0), double(kSpacingSamples));
+      const int k = std::min(int(std::floor(t)), kSpacingSamples - 1);
+      const double f = (std::min(std::max(s, 0.0), s_end) - dens_s[k]) / (dens_s[k + 1] - dens_s[k]);
+      return dens[k] + std::min(std::max(f, 0.0), 1.0) * (dens[k + 1] - dens[k]);
+    };
+    ss = column_positions(bps, tabulated, refinement, o.ni);
+  }
+  if (reaches) return "the body reaches the outer boundary; the nose is not supported";
+  const int ni = int(ss.size()) - 1;
+  out->ni = ni;
+  out->nj = nj;
+  out->i_tip = 0;
+  out->outer_angle = outer_angle;
+  out->x.assign(size_t(ni + 1) * (nj + 1), 0);
+  out->y.assign(size_t(ni + 1) * (nj + 1), 0);
+  for (int i = 0; i <= ni; i++) {
+    const SurfacePoint p = surface(ss[i]);
+    const Line l = line(ss[i]);
+    const double b = line_strength(l.h, R, limits);
+    for (int j = 0; j <= nj; j++) {
+      const double d = l.h * stretched_fraction(b, j, nj);
+      const size_t k = i + size_t(j) * (ni + 1);
+      out->x[k] = p.x + d * l.dx;
+      out->y[k] = p.y + d * l.dy;
+    }
+  }
+  // The first line lies on the axis ahead of the tip.
+  for (int j = 0; j <= nj; j++) out->y[size_t(j) * (ni + 1)] = 0;
+  if (!o.gated) return "";
   const std::vector<std::string> failures =
       quality_failures(grid_quality(ni, nj, out->x.data(), out->y.data()), limits);
   if (!failures.empty()) {

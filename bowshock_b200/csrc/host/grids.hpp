@@ -41,7 +41,7 @@ std::vector<std::string> quality_failures(const GridQuality& q, const QualityLim
 // interval's own count: the batched configurations name ni exactly.
 std::vector<double> column_positions(const std::vector<double>& breakpoints,
                                      const std::function<double(double)>& density, int refinement,
-                                     int total);
+                                     int total, double max_spacing_slope = 0);
 
 struct BodyGridOptions {
   int nj = 20;          // least cells across on the base grid
@@ -55,6 +55,23 @@ struct BodyGridOptions {
 // failing the quality gates sets *quality_error.
 std::string body_grid(const Body& body, const BodyGridOptions& options, Grid* out,
                       bool* quality_error);
+
+// bluntBodyGrid (src/grid/blunt-grid.ts:159-540): the C-topology grid of a
+// blunt nose (or of a sharp one whose bow shock detaches): straight lines
+// from the body, close to its smoothed normals, to an outer boundary made of
+// an arc ahead of the tip and a straight line at the angle halfway between
+// the normal shock and the Mach angle. iMin is the axis ahead of the tip,
+// jMin the body, jMax the outer boundary, iMax the outflow plane. `ni` > 0
+// asks for exactly that many columns (refinement 1).
+struct BluntGridOptions {
+  int nj = 20;
+  int refinement = 1;
+  int ni = 0;
+  double mach = 2;
+  bool gated = true;
+};
+std::string blunt_body_grid(const Body& body, const BluntGridOptions& options, Grid* out,
+                            bool* quality_error);
 
 // rampGrid (src/grid/shapes.ts:30-52).
 std::string ramp_grid(int ni, int nj, double x_min, double x_corner, double x_max, double height,

@@ -1,5 +1,6 @@
 """Grids and exact solutions from the native host code: `bodyGrid`
-(src/grid/body-grid.ts:76-181), `rampGrid` (src/grid/shapes.ts:30-52),
+(src/grid/body-grid.ts:76-181), `bluntBodyGrid` (src/grid/blunt-grid.ts:159-540),
+`rampGrid` (src/grid/shapes.ts:30-52),
 `gridQuality` (src/grid/quality.ts:75-128), `taylorMaccoll`
 (src/validation/taylor-maccoll.ts:153-216), `obliqueShock` / `normalShock`
 (src/validation/gas-dynamics.ts:40-96)."""
@@ -83,6 +84,26 @@ def body_grid(body: Body, nj: int, mach: float, gamma: float = 1.4, refinement: 
     b = body.to_abi()
     h = C.c_void_p()
     _native.check(L.bs_body_grid(C.byref(b), C.byref(o), C.byref(h)), L)
+    grid, tip, angle = _take(h, L)
+    return BodyGrid(grid, tip, angle)
+
+
+def blunt_body_grid(body: Body, nj: int, mach: float, refinement: int = 1, ni: int = 0,
+                    gated: bool = True, lib=None) -> BodyGrid:
+    """bluntBodyGrid: the C-topology grid of a blunt nose (or of a sharp one
+    whose shock detaches); iMin is the axis ahead of the tip. `gated=False`
+    skips the quality gates, as for the reference's two-scale (Haack) noses."""
+    L = lib or _native.load()
+    o = abi.BodyGridOptions()
+    o.nj = nj
+    o.refinement = refinement
+    o.ni = ni
+    o.flags = 0 if gated else abi.GRID_UNGATED
+    o.mach = mach
+    o.gamma = 1.4
+    b = body.to_abi()
+    h = C.c_void_p()
+    _native.check(L.bs_blunt_body_grid(C.byref(b), C.byref(o), C.byref(h)), L)
     grid, tip, angle = _take(h, L)
     return BodyGrid(grid, tip, angle)
 

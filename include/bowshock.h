@@ -363,10 +363,15 @@ typedef struct bs_body_grid_options {
   int32_t nj;
   int32_t refinement;
   int32_t ni;
-  int32_t reserved;
+  int32_t flags;  /* BS_GRID_UNGATED: skip the quality gates (blunt grids only) */
   double mach;
   double gamma;
 } bs_body_grid_options;
+
+/* Skip the quality gates of a C-topology grid, as the reference does for the
+ * captured solution of a two-scale (Haack) nose, whose grids fail them
+ * (src/grid/blunt-grid.ts:47-51, tests/grid/blunt-grid.test.ts:133-137). */
+#define BS_GRID_UNGATED 1
 
 typedef struct bs_grid bs_grid;
 
@@ -374,6 +379,14 @@ typedef struct bs_grid bs_grid;
  * nose; BS_GRID_QUALITY if it fails the quality gates
  * (src/grid/quality.ts:24-38). */
 BS_API bs_status bs_body_grid(const bs_body *body, const bs_body_grid_options *options, bs_grid **out);
+
+/* bluntBodyGrid (src/grid/blunt-grid.ts:159-540): the C-topology grid of a
+ * blunt nose (ellipsoid, Haack / Von Karman, power series) or of a sharp one
+ * whose bow shock detaches. iMin is the axis ahead of the tip (a symmetry
+ * line: give it a wall condition), jMin the body, jMax the outer boundary,
+ * iMax the outflow plane. options->ni > 0 asks for exactly ni columns. */
+BS_API bs_status bs_blunt_body_grid(const bs_body *body, const bs_body_grid_options *options,
+                                    bs_grid **out);
 
 /* rampGrid (src/grid/shapes.ts:30-52): a channel whose lower wall turns by
  * `angle` at x_corner. */

@@ -39,7 +39,7 @@ def test_struct_layouts_match_the_header():
     assert C.sizeof(abi.FaceFlux) == 72
     assert C.sizeof(abi.SolveResult) == 32
     assert C.sizeof(abi.Body) == 40
-    assert C.sizeof(abi.BodyGridOptions) == 32
+    assert C.sizeof(abi.BodyGridOptions) == 32  # nj, refinement, ni, flags, mach, gamma
 
 
 def test_version_and_device_count_without_a_gpu():
