@@ -1,6 +1,6 @@
 // LU-SGS forward and backward sweeps as anti-diagonal wavefronts
-// (implicitCorrection's sweeps, src/engine-cpu/euler2d.ts:1058-1102, and
-// applyImplicitUpdate, :816-847, fused into the backward sweep).
+// (implicitCorrection's sweeps, src/engine-cpu/euler2d.ts:1058-1102), and
+// the update that applies the correction (applyImplicitUpdate, :816-847).
 //
 // The forward sweep solves (D + L) dQ* = R cell by cell in the order j, then
 // i; cell (i, j) needs only (i - 1, j) and (i, j - 1), both on the previous
@@ -10,11 +10,14 @@
 //   - its west (forward) / east (backward) neighbour is the cell it finished
 //     on the previous step, held in registers;
 //   - its south / north neighbour is the cell thread j -+ 1 finished on the
-//     previous step, exchanged through double-buffered shared memory;
-//   - everything that does not depend on dQ (residual, diagonal, state, face
-//     metrics) is prefetched one step ahead, so a step's critical path is the
-//     exchange, the two neighbour terms and one division.
-// One __syncthreads per diagonal orders the exchange.
+//     previous step: its dQ by warp shuffle (shared memory across a warp
+//     edge), its state and face through double-buffered shared memory;
+//   - its own operands (residual or dQ*, state, (u, v, p, 1/D), faces) come
+//     from the per-cell records that the residual pass wrote diagonal-major,
+//     staged into shared memory by TMA bulk copies a chunk of diagonals at a
+//     time, two chunks in flight.
+// One barrier per diagonal orders the exchange. A step has no branch: every
+// thread computes, and only cells on the grid store.
 //
 // The operator runs in FP32. The neighbour term is the change of the
 // physical flux, F(Q + dQ) - F(Q), exactly as the reference forms it, but
@@ -22,6 +25,8 @@
 // (no difference of two O(|F|) numbers), so FP32 rounding is relative to the
 // term itself and vanishes with dQ.
 #pragma once
+
+#include <algorithm>
 
 #include "layout.cuh"
 
@@ -42,29 +47,6 @@ struct SweepArgs {
   int chunk;              // diagonals per bulk copy
   int wait_limit;         // mbarrier polls before a wait gives up
 };
-
-// Change of the physical flux along (nx, ny) of state q (with u, v, p in
-// w) for the change d, times half_area, less damp d, added to `sum` (the
-// neighbour term, src/engine-cpu/euler2d.ts:977-1005: half_area = A / 2,
-// damp = omega lambda A / 2) - the exact difference F(Q + dQ) - F(Q) written
-// so that every term is proportional to dQ. d = 0 contributes exactly
-// nothing, which stands for an absent neighbour.
-__device__ __forceinline__ void neighbour_change(float4& sum, const float4 q, const float4 w,
-                                                 const float4 d, float nx, float ny,
-                                                 float half_area, float damp, float gm1) {
-  const float u = w.x, v = w.y, p = w.z;
-  const float un = u * nx + v * ny;
-  const float inv1 = __frcp_rn(q.x + d.x);
-  const float dmn = d.y * nx + d.z * ny;
-  const float dun = (dmn - un * d.x) * inv1;
-  const float dk = (q.x * (u * d.y + v * d.z - 0.5f * (u * u + v * v) * d.x) +
-                    0.5f * (d.y * d.y + d.z * d.z)) * inv1;
-  const float dp = gm1 * (d.w - dk);
-  sum.x += half_area * dmn - damp * d.x;
-  sum.y += half_area * (d.y * un + (q.y + d.y) * dun + dp * nx) - damp * d.y;
-  sum.z += half_area * (d.z * un + (q.z + d.z) * dun + dp * ny) - damp * d.z;
-  sum.w += half_area * ((d.w + dp) * un + (q.w + d.w + p + dp) * dun) - damp * d.w;
-}
 
 // Fields of the sweep record (five float4 per cell, written by the residual
 // pass): residual; state; (u, v, p, 1/D); west face and south face as
@@ -112,11 +94,64 @@ __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async;\n" ::: "memory");
 }
 
-// Shared memory of the sweep kernel for `nt` threads, `nj` rows and chunks
-// of `chunk` diagonals: two mbarriers; the exchange (state, u/v/p/(1/D), dQ,
-// south face; double-buffered); two chunk buffers of records and of dQ*.
+// 1/x by the hardware approximation (rcp.approx.ftz.f32, within about one
+// ulp): the LU-SGS operator runs in FP32 and only shapes the path to the
+// steady state, whose residual is FP64.
+__device__ __forceinline__ float approx_rcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Shared memory of the sweep for `nt` threads, `nj` rows and chunks of
+// `chunk` diagonals: a 128-byte header (two mbarriers), the double-buffered
+// exchange (state, (u, v, p, 1/D), dQ, south face) and two chunk buffers of
+// records and of dQ*.
 __host__ __device__ constexpr size_t sweep_smem_bytes(int nt, int nj, int chunk) {
   return 128 + size_t(nt) * 16 * 8 + 2 * size_t(chunk) * nj * 16 * (REC_SIZE + 1);
+}
+
+// The d-independent part of a neighbour's term: its state, the face normal
+// (signed for the direction the flux leaves), A/2, omega lambda A/2, its
+// normal velocity and the momentum and kinetic-energy weights of dK.
+struct NeighbourTerm {
+  float4 q;
+  float nx, ny, half_area, damp, un, ku, kv, kk, p;
+};
+
+__device__ __forceinline__ NeighbourTerm neighbour_term(const float4 q, const float4 w, const float4 f,
+                                                        float sgn) {
+  NeighbourTerm t;
+  t.q = q;
+  t.nx = sgn * f.x;
+  t.ny = sgn * f.y;
+  t.half_area = f.z;
+  t.damp = f.w;
+  t.un = w.x * t.nx + w.y * t.ny;
+  t.ku = q.x * w.x;
+  t.kv = q.x * w.y;
+  t.kk = q.x * (0.5f * (w.x * w.x + w.y * w.y));
+  t.p = w.z;
+  return t;
+}
+
+// The neighbour term of src/engine-cpu/euler2d.ts:977-1005 - the change of
+// the physical flux across the face, F(Q + d) - F(Q), times A/2, less
+// omega lambda A/2 d - added to `sum`. The exact difference is written so
+// that every term is proportional to d (no difference of two O(|F|)
+// numbers), so FP32 rounding is relative to the term and d = 0 adds exactly
+// nothing, which stands for an absent neighbour.
+__device__ __forceinline__ void add_neighbour(float4& sum, const NeighbourTerm& t, const float4 d,
+                                              float gm1) {
+  const float inv1 = approx_rcp(t.q.x + d.x);
+  const float dmn = d.y * t.nx + d.z * t.ny;
+  const float dun = (dmn - t.un * d.x) * inv1;
+  const float dk = (t.ku * d.y + t.kv * d.z - t.kk * d.x + 0.5f * (d.y * d.y + d.z * d.z)) * inv1;
+  const float dp = gm1 * (d.w - dk);
+  sum.x += t.half_area * dmn - t.damp * d.x;
+  sum.y += t.half_area * (d.y * t.un + (t.q.y + d.y) * dun + dp * t.nx) - t.damp * d.y;
+  sum.z += t.half_area * (d.z * t.un + (t.q.z + d.z) * dun + dp * t.ny) - t.damp * d.z;
+  sum.w += t.half_area * ((d.w + dp) * t.un + (t.q.w + d.w + t.p + dp) * dun) - t.damp * d.w;
 }
 
 // The forward and backward sweeps of every active case, one CTA per case,
@@ -147,8 +182,7 @@ static __global__ void __launch_bounds__(512) lusgs_sweep_kernel(const SweepArgs
   const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
 
   if (j == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    for (int b = 0; b < 2; b++) mbar_init(&bars[b], 1);
     mbar_fence_init();
   }
   // Benign exchange contents: a slot read for an absent neighbour is
@@ -161,8 +195,8 @@ static __global__ void __launch_bounds__(512) lusgs_sweep_kernel(const SweepArgs
   }
   __syncthreads();
 
-  unsigned uses[2] = {0u, 0u};    // completed phases of each buffer's mbarrier
-  unsigned issued[2] = {0u, 0u};  // copies issued into each buffer
+  unsigned uses[2] = {};    // completed phases of each buffer's mbarrier
+  unsigned issued[2] = {};  // copies issued into each buffer
   bool failed = false;
   for (int pass = 0; pass < 2 && !failed; pass++) {
     const bool fwd = pass == 0;
@@ -174,7 +208,7 @@ static __global__ void __launch_bounds__(512) lusgs_sweep_kernel(const SweepArgs
     auto issue = [&](int cc) {  // one thread
       int dlo, n;
       chunk_range(cc, dlo, n);
-      const int buf = cc & 1;
+      const int buf = cc % 2;
       const unsigned rec_bytes = unsigned(n) * nj * 16u * REC_SIZE;
       const unsigned dq_bytes = fwd ? 0u : unsigned(n) * nj * 16u;
       mbar_arrive_expect_tx(&bars[buf], rec_bytes + dq_bytes);
@@ -182,23 +216,16 @@ static __global__ void __launch_bounds__(512) lusgs_sweep_kernel(const SweepArgs
                 rec_bytes, &bars[buf]);
       if (!fwd) bulk_load(ring_dq + size_t(buf) * K * nj, dq_case + size_t(dlo) * nj, dq_bytes, &bars[buf]);
     };
-    if (j == 0) {
-      fence_proxy_async();
-      issue(0);
-      issued[0]++;
-      if (nchunks > 1) {
-        issue(1);
-        issued[1]++;
-      }
-    } else {
-      issued[0]++;
-      if (nchunks > 1) issued[1]++;
+    if (j == 0) fence_proxy_async();
+    for (int k = 0; k < 2 && k < nchunks; k++) {
+      if (j == 0) issue(k);
+      issued[k]++;
     }
     // The cell this thread finished last step (its neighbour along the row).
     float4 pq = make_float4(1.f, 0.f, 0.f, 1.f), pw = make_float4(0.f, 0.f, 1.f, 1.f);
     float4 pd = zero, pfw = zero;
     for (int cc = 0; cc < nchunks; cc++) {
-      const int buf = cc & 1;
+      const int buf = cc % 2;
       const bool ok = mbar_wait(&bars[buf], uses[buf] & 1u, A.wait_limit);
       if (ok) uses[buf]++;
       if (__syncthreads_or(!ok)) {
@@ -213,8 +240,18 @@ static __global__ void __launch_bounds__(512) lusgs_sweep_kernel(const SweepArgs
         const int step = cc * K + t;
         const int d = fwd ? step : ndiag - 1 - step;
         const int i = d - j;
-        if (row && i >= 0 && i < ni) {
-          const int local = (d - dlo) * nj + j;
+        // The dQ row j -+ 1 finished on the previous step, inside the warp.
+        float4 sh;
+        sh.x = fwd ? __shfl_up_sync(0xffffffffu, pd.x, 1) : __shfl_down_sync(0xffffffffu, pd.x, 1);
+        sh.y = fwd ? __shfl_up_sync(0xffffffffu, pd.y, 1) : __shfl_down_sync(0xffffffffu, pd.y, 1);
+        sh.z = fwd ? __shfl_up_sync(0xffffffffu, pd.z, 1) : __shfl_down_sync(0xffffffffu, pd.z, 1);
+        sh.w = fwd ? __shfl_up_sync(0xffffffffu, pd.w, 1) : __shfl_down_sync(0xffffffffu, pd.w, 1);
+        const bool lane_edge = (j & 31) == (fwd ? 0 : 31);
+        // Only cells on the grid store; the others compute on records of
+        // their chunk (possibly padding) and discard the result.
+        const bool active = row && i >= 0 && i < ni;
+        {
+          const int local = (d - dlo) * nj + min(j, nj - 1);
           const float4* r5 = rb + size_t(REC_SIZE) * local;
           const float4 q = r5[REC_Q], w = r5[REC_W], fw = r5[REC_FW], fs = r5[REC_FS];
           const float4 base = fwd ? r5[REC_R] : db[local];
@@ -223,7 +260,8 @@ static __global__ void __launch_bounds__(512) lusgs_sweep_kernel(const SweepArgs
           const int b = ((step - 1) & 1) * nt + (fwd ? j - 1 : j + 1);
           const int bb = has_j ? b : (step & 1) * nt + j;  // an in-range slot either way
           const float4 oq = xq[bb], ow = xw[bb], of = xf[bb];
-          const float4 od = has_j ? xd[bb] : zero;
+          float4 od = zero;
+          if (has_j) od = lane_edge ? xd[bb] : sh;
           // Forward: this cell's west and south faces, the flux leaving
           // through -n; backward: the east neighbour's west face and the
           // north neighbour's south face, through +n.
@@ -231,9 +269,10 @@ static __global__ void __launch_bounds__(512) lusgs_sweep_kernel(const SweepArgs
           const float4 face_i = fwd ? fw : pfw;
           const float4 face_j = fwd ? fs : of;
           float4 sum = zero;
-          neighbour_change(sum, pq, pw, has_i ? pd : zero, sgn * face_i.x, sgn * face_i.y, face_i.z,
-                           face_i.w, gm1);
-          neighbour_change(sum, oq, ow, od, sgn * face_j.x, sgn * face_j.y, face_j.z, face_j.w, gm1);
+          const NeighbourTerm ti = neighbour_term(pq, pw, face_i, sgn);
+          const NeighbourTerm tj = neighbour_term(oq, ow, face_j, sgn);
+          add_neighbour(sum, ti, has_i ? pd : zero, gm1);
+          add_neighbour(sum, tj, od, gm1);
           const float inv_d = w.w;
           float4 dq;
           if (fwd) {
@@ -244,23 +283,21 @@ static __global__ void __launch_bounds__(512) lusgs_sweep_kernel(const SweepArgs
                              base.z - sum.z * inv_d, base.w - sum.w * inv_d);
           }
           const int o = (step & 1) * nt + j;
-          xq[o] = q;
-          xw[o] = w;
-          xd[o] = dq;
-          xf[o] = fs;
-          dq_case[size_t(d) * nj + j] = dq;
-          pq = q;
-          pw = w;
-          pd = dq;
-          pfw = fw;
+          if (active) {
+            xq[o] = q;
+            xw[o] = w;
+            xd[o] = dq;
+            xf[o] = fs;
+            dq_case[size_t(d) * nj + j] = dq;
+          }
+          pq = active ? q : pq;
+          pw = active ? w : pw;
+          pd = active ? dq : pd;
+          pfw = active ? fw : pfw;
         }
         __syncthreads();
       }
       if (cc + 2 < nchunks) {
-        // The buffer is free: order this CTA's reads of it before the next
-        // asynchronous write into it.
-        fence_proxy_async();
-        __syncthreads();
         if (j == 0) issue(cc + 2);
         issued[buf]++;
       }
@@ -319,19 +356,25 @@ __global__ void __launch_bounds__(TILE_THREADS) lusgs_update_kernel(const CaseDe
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&status[c], STATUS_NON_PHYSICAL);
 }
 
-// Diagonals per bulk copy for a case of `nj` rows: the largest of 8, 6, 4,
-// 3, 2, 1 whose shared memory fits one CTA.
-inline int sweep_chunk(int nt, int nj) {
-  constexpr size_t kLimit = 200 * 1024;
-  for (int k : {8, 6, 4, 3, 2, 1})
-    if (sweep_smem_bytes(nt, nj, k) <= kLimit) return k;
+// Diagonals per bulk copy for cases of up to `nj` rows (`nt` threads) when
+// `cases_in_flight` cases sweep at once: the largest (up to 8) that lets
+// the resident cases (up to 8 per SM) share an SM's shared memory, else the
+// largest that fits one CTA; 0 if not even one diagonal does.
+inline int sweep_chunk(int nt, int nj, int cases_in_flight) {
+  const int per_sm = std::min(8, std::max(1, (cases_in_flight + 147) / 148));
+  for (size_t budget : {size_t(200 * 1024) / per_sm, size_t(200 * 1024)})
+    for (int k = 8; k >= 1; k--)
+      if (sweep_smem_bytes(nt, nj, k) <= budget) return k;
   return 0;
 }
 
-inline cudaError_t launch_sweep(SweepArgs A, int n_cases, int max_nj, cudaStream_t stream) {
+// `cases_in_flight`: cases of the whole batch sweeping at the same time
+// (other lanes included), which sets the shared memory each CTA may take.
+inline cudaError_t launch_sweep(SweepArgs A, int n_cases, int max_nj, int cases_in_flight,
+                                cudaStream_t stream) {
   const int nt = ((max_nj + 31) / 32) * 32;
-  A.chunk = sweep_chunk(nt, max_nj);
-  if (A.chunk == 0) return cudaErrorInvalidConfiguration;
+  A.chunk = sweep_chunk(nt, max_nj, cases_in_flight);
+  if (A.chunk == 0 || nt > 512) return cudaErrorInvalidConfiguration;
   A.wait_limit = 1 << 22;
   const size_t bytes = sweep_smem_bytes(nt, max_nj, A.chunk);
   const cudaError_t e = cudaFuncSetAttribute(lusgs_sweep_kernel,

@@ -102,6 +102,21 @@ struct GraphKey {
 constexpr int kMethodExplicit = 0;
 constexpr int kMethodImplicit = 1;
 
+// The launch geometry of a group of cases: its tile list, case list, widest
+// case and stream. The whole batch is one lane; a batch of several cases is
+// also split into lanes whose step chains run concurrently (a lane's residual
+// pass fills the SMs that the other lanes' sweeps leave idle).
+struct LaneView {
+  const int2* tiles;
+  int n_tiles;
+  const int* case_list;
+  int n_cases;
+  int max_nj;
+  cudaStream_t stream;
+};
+
+constexpr int kMaxLanes = 16;
+
 template <class R>
 class Solver final : public SolverBase {
  public:
@@ -109,6 +124,10 @@ class Solver final : public SolverBase {
 
   ~Solver() override {
     for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    for (auto& l : lanes_)
+      if (l->stream != nullptr) cudaStreamDestroy(l->stream);
+    for (auto e : ev_join_) cudaEventDestroy(e);
+    if (ev_fork_ != nullptr) cudaEventDestroy(ev_fork_);
     if (ev0_ != nullptr) cudaEventDestroy(ev0_);
     if (ev1_ != nullptr) cudaEventDestroy(ev1_);
     if (stream_ != nullptr) cudaStreamDestroy(stream_);
@@ -245,6 +264,49 @@ class Solver final : public SolverBase {
       }
     }
     BS_CUDA(cudaMemcpy(bgeom_.p, bg.data(), bg.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return init_lanes(hc);
+  }
+
+  // Splits the cases into lanes of about equal cell counts (largest first,
+  // each to the lightest lane).
+  bs_status init_lanes(const std::vector<bsd::CaseDev>& hc) {
+    const int L = std::min(n_, kMaxLanes);
+    if (L < 2) return BS_OK;
+    std::vector<int> order(n_);
+    for (int c = 0; c < n_; c++) order[c] = c;
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+      return int64_t(hc[a].ni) * hc[a].nj > int64_t(hc[b].ni) * hc[b].nj;
+    });
+    std::vector<std::vector<int>> members(L);
+    std::vector<int64_t> load(L, 0);
+    for (int c : order) {
+      const int l = int(std::min_element(load.begin(), load.end()) - load.begin());
+      members[l].push_back(c);
+      load[l] += int64_t(hc[c].ni) * hc[c].nj;
+    }
+    BS_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+    for (int l = 0; l < L; l++) {
+      auto lane = std::make_unique<Lane>();
+      std::sort(members[l].begin(), members[l].end());
+      std::vector<int2> tiles;
+      for (int c : members[l]) {
+        const int ti = (hc[c].ni + bsd::TI - 1) / bsd::TI, tj = (hc[c].nj + bsd::TJ - 1) / bsd::TJ;
+        for (int t = 0; t < ti * tj; t++) tiles.push_back(make_int2(c, t));
+        lane->max_nj = std::max(lane->max_nj, hc[c].nj);
+      }
+      lane->n_cases = int(members[l].size());
+      lane->n_tiles = int(tiles.size());
+      BS_CUDA(lane->tiles.alloc(tiles.size()));
+      BS_CUDA(cudaMemcpy(lane->tiles.p, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice));
+      BS_CUDA(lane->case_list.alloc(members[l].size()));
+      BS_CUDA(cudaMemcpy(lane->case_list.p, members[l].data(), members[l].size() * sizeof(int),
+                         cudaMemcpyHostToDevice));
+      BS_CUDA(cudaStreamCreateWithFlags(&lane->stream, cudaStreamNonBlocking));
+      cudaEvent_t ev;
+      BS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      ev_join_.push_back(ev);
+      lanes_.push_back(std::move(lane));
+    }
     return BS_OK;
   }
 
@@ -641,13 +703,24 @@ class Solver final : public SolverBase {
     return BS_OK;
   }
 
+  LaneView whole() const {
+    return {d_tiles_.p, n_tiles_, d_case_list_.p, n_, max_nj_, stream_};
+  }
+
   template <int MODE>
   bs_status launch_tile(bsd::StateView<R> src, bsd::StateView<R> u0, bsd::StateView<R> out,
                         double a, double b, bool first, double* norm, double* res_out,
                         bool all_cases) {
+    return launch_tile_on<MODE>(whole(), src, u0, out, a, b, first, norm, res_out, all_cases);
+  }
+
+  template <int MODE>
+  bs_status launch_tile_on(const LaneView& lane, bsd::StateView<R> src, bsd::StateView<R> u0,
+                           bsd::StateView<R> out, double a, double b, bool first, double* norm,
+                           double* res_out, bool all_cases) {
     bsd::TileArgs<R> A{};
     A.cases = d_cases_.p;
-    A.tiles = d_tiles_.p;
+    A.tiles = lane.tiles;
     A.active = all_cases ? nullptr : d_active_.p;
     A.src = src;
     A.u0 = u0;
@@ -664,7 +737,7 @@ class Solver final : public SolverBase {
     A.cfl = cfl_.p;
     A.omega = omega_.p;
     A.res_out = res_out;
-    bsd::tile_kernel<R, MODE><<<n_tiles_, bsd::TILE_THREADS, 0, stream_>>>(A);
+    bsd::tile_kernel<R, MODE><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
     launches_++;
     BS_CUDA(cudaGetLastError());
     return BS_OK;
@@ -672,7 +745,9 @@ class Solver final : public SolverBase {
 
   // One explicit step of every active case; `norm` adds the density
   // residual of the step's starting state to the per-case slots.
-  bs_status record_explicit_step(bool norm) {
+  bs_status record_explicit_step(bool norm) { return record_explicit_step_on(whole(), norm); }
+
+  bs_status record_explicit_step_on(const LaneView& lane, bool norm) {
     double a[3], b[3];
     int n = 3;
     const int integrator = cases_[0].cfg.integrator;
@@ -684,39 +759,47 @@ class Solver final : public SolverBase {
       a[0] = 0; b[0] = 1; a[1] = 3.0 / 4.0; b[1] = 1.0 / 4.0; a[2] = 1.0 / 3.0; b[2] = 2.0 / 3.0;
     }
     if (any_global_dt_) {
-      BS_CUDA(cudaMemsetAsync(dtmin_.p, 0x7f, n_ * sizeof(unsigned), stream_));
-      bsd::dt_kernel<R><<<n_tiles_, bsd::TILE_THREADS, 0, stream_>>>(
-          d_cases_.p, d_tiles_.p, d_active_.p, q_view(), metrics(), dt_.p, dtmin_.p);
+      BS_CUDA(cudaMemsetAsync(dtmin_.p, 0x7f, n_ * sizeof(unsigned), lane.stream));
+      bsd::dt_kernel<R><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(
+          d_cases_.p, lane.tiles, d_active_.p, q_view(), metrics(), dt_.p, dtmin_.p);
       launches_++;
       BS_CUDA(cudaGetLastError());
     }
     const bsd::StateView<R> q = q_view(), s1 = s1_view(), s2 = s2_view();
     if (n == 1) {
-      BS_TRY(launch_tile<bsd::MODE_STAGE>(q, q, s1, a[0], b[0], true, norm ? norm_.p : nullptr, nullptr, false));
+      BS_TRY(launch_tile_on<bsd::MODE_STAGE>(lane, q, q, s1, a[0], b[0], true, norm ? norm_.p : nullptr,
+                                             nullptr, false));
       for (int v = 0; v < 4; v++)
-        BS_CUDA(cudaMemcpyAsync(q_[v].p, s1_[v].p, total_cells_ * sizeof(R), cudaMemcpyDeviceToDevice, stream_));
+        BS_CUDA(cudaMemcpyAsync(q_[v].p, s1_[v].p, total_cells_ * sizeof(R), cudaMemcpyDeviceToDevice,
+                                lane.stream));
       return BS_OK;
     }
     for (int s = 0; s < n; s++) {
       const bsd::StateView<R> src = s == 0 ? q : (s == 1 ? s1 : s2);
       const bsd::StateView<R> out = s == n - 1 ? q : (s == 0 ? s1 : s2);
-      BS_TRY(launch_tile<bsd::MODE_STAGE>(src, q, out, a[s], b[s], s == 0,
-                                          (norm && s == 0) ? norm_.p : nullptr, nullptr, false));
+      BS_TRY(launch_tile_on<bsd::MODE_STAGE>(lane, src, q, out, a[s], b[s], s == 0,
+                                             (norm && s == 0) ? norm_.p : nullptr, nullptr, false));
     }
     return BS_OK;
   }
 
-  bs_status record_implicit_step(bool norm) {
+  bs_status record_implicit_step(bool norm) { return record_implicit_step_on(whole(), norm); }
+
+  bs_status record_implicit_step_on(const LaneView& lane, bool norm) {
     const bsd::StateView<R> q = q_view();
-    BS_TRY(launch_tile<bsd::MODE_PREPARE>(q, q, q, 0, 1, false, norm ? norm_.p : nullptr, nullptr, false));
-    BS_TRY(launch_sweep());
-    return launch_update();
+    BS_TRY(launch_tile_on<bsd::MODE_PREPARE>(lane, q, q, q, 0, 1, false, norm ? norm_.p : nullptr,
+                                             nullptr, false));
+    BS_TRY(launch_sweep_on(lane));
+    return launch_update_on(lane);
   }
 
-  bs_status launch_sweep() {
+  bs_status launch_sweep() { return launch_sweep_on(whole()); }
+  bs_status launch_update() { return launch_update_on(whole()); }
+
+  bs_status launch_sweep_on(const LaneView& lane) {
     bsd::SweepArgs S{};
     S.cases = d_cases_.p;
-    S.case_list = d_case_list_.p;
+    S.case_list = lane.case_list;
     S.active = d_active_.p;
     S.m = metrics();
     S.rec = rec_.p;
@@ -726,26 +809,54 @@ class Solver final : public SolverBase {
     S.growth = growth_.p;
     S.omega = omega_.p;
     S.status = status_.p;
-    BS_CUDA(bsd::launch_sweep(S, n_, max_nj_, stream_));
+    BS_CUDA(bsd::launch_sweep(S, lane.n_cases, lane.max_nj, n_, lane.stream));
     launches_++;
     return BS_OK;
   }
 
-  bs_status launch_update() {
-    bsd::lusgs_update_kernel<R><<<n_tiles_, bsd::TILE_THREADS, 0, stream_>>>(
-        d_cases_.p, d_tiles_.p, d_active_.p, q_view(), dq_.p, status_.p);
+  bs_status launch_update_on(const LaneView& lane) {
+    bsd::lusgs_update_kernel<R><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(
+        d_cases_.p, lane.tiles, d_active_.p, q_view(), dq_.p, status_.p);
     launches_++;
     BS_CUDA(cudaGetLastError());
     return BS_OK;
   }
 
+  bool lanes_apply(int method) const {
+    if (lanes_.size() < 2) return false;
+    // Forward Euler copies whole arenas and global stepping reduces over the
+    // batch: those run as one lane.
+    return method == kMethodImplicit ||
+           (!any_global_dt_ && cases_[0].cfg.integrator != BS_FORWARD_EULER);
+  }
+
   bs_status record_steps(int method, int count, bool norm_last) {
-    for (int s = 0; s < count; s++) {
-      const bool norm = norm_last && s == count - 1;
-      if (method == kMethodExplicit)
-        BS_TRY(record_explicit_step(norm));
-      else
-        BS_TRY(record_implicit_step(norm));
+    if (!lanes_apply(method)) {
+      for (int s = 0; s < count; s++) {
+        const bool norm = norm_last && s == count - 1;
+        if (method == kMethodExplicit)
+          BS_TRY(record_explicit_step(norm));
+        else
+          BS_TRY(record_implicit_step(norm));
+      }
+      return BS_OK;
+    }
+    // Fork one chain of `count` steps per lane off the batch stream, join them back.
+    BS_CUDA(cudaEventRecord(ev_fork_, stream_));
+    for (auto& l : lanes_) BS_CUDA(cudaStreamWaitEvent(l->stream, ev_fork_, 0));
+    for (auto& l : lanes_) {
+      const LaneView lane{l->tiles.p, l->n_tiles, l->case_list.p, l->n_cases, l->max_nj, l->stream};
+      for (int s = 0; s < count; s++) {
+        const bool norm = norm_last && s == count - 1;
+        if (method == kMethodExplicit)
+          BS_TRY(record_explicit_step_on(lane, norm));
+        else
+          BS_TRY(record_implicit_step_on(lane, norm));
+      }
+    }
+    for (size_t k = 0; k < lanes_.size(); k++) {
+      BS_CUDA(cudaEventRecord(ev_join_[k], lanes_[k]->stream));
+      BS_CUDA(cudaStreamWaitEvent(stream_, ev_join_[k], 0));
     }
     return BS_OK;
   }
@@ -847,6 +958,15 @@ class Solver final : public SolverBase {
   DevBuf<unsigned> status_, dtmin_;
   cudaStream_t stream_ = nullptr;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  struct Lane {
+    DevBuf<int2> tiles;
+    DevBuf<int> case_list;
+    int n_tiles = 0, n_cases = 0, max_nj = 0;
+    cudaStream_t stream = nullptr;
+  };
+  std::vector<std::unique_ptr<Lane>> lanes_;
+  cudaEvent_t ev_fork_ = nullptr;
+  std::vector<cudaEvent_t> ev_join_;
   std::map<GraphKey, cudaGraphExec_t> graphs_;
   std::map<GraphKey, int64_t> graph_launches_;
   int64_t launches_ = 0;

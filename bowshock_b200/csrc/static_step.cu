@@ -207,7 +207,7 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
     S.growth = &d_words->growth;
     S.omega = &d_words->omega;
     S.status = &d_words->status;
-    err = bsd::launch_sweep(S, 1, nj, st);
+    err = bsd::launch_sweep(S, 1, nj, 1, st);
   }
   if (err == cudaSuccess) {
     bsd::lusgs_update_kernel<double><<<n_tiles, bsd::TILE_THREADS, 0, st>>>(

@@ -271,8 +271,9 @@ BS_API bs_status bs_engine_solve(bs_engine *engine, int32_t method, double cfl, 
  * their budget, and cudaMalloc/cudaFree synchronise the device) and solver
  * loops that must not allocate once running. All scratch lives in one static
  * device array of the library, reserved on every GPU that loads it until the
- * process exits: at most 65536 cells (ni nj) and 512 cells across (nj);
- * larger grids return BS_INVALID_ARGUMENT. The first call on a device looks up
+ * process exits: at most 65536 cells (ni nj), 512 cells across (nj) and
+ * 98304 diagonal-major record slots ((ni + nj - 1) nj); larger grids return
+ * BS_INVALID_ARGUMENT. The first call on a device looks up
  * the array's device address with that device current; make that first call
  * before any stream capture. Every call shares the array, so calls that
  * overlap on the GPU race: order them. Device inputs (layout as the engine's,
