@@ -267,23 +267,45 @@ class Solver final : public SolverBase {
     return init_lanes(hc);
   }
 
-  // Splits the cases into lanes of about equal cell counts (largest first,
-  // each to the lightest lane).
+  // Splits the cases into lanes of about equal cell counts. A few cases per
+  // lane: largest first, each to the lightest lane. Many: contiguous runs of
+  // the cases sorted by width, so that a lane's sweep CTAs share one size
+  // class (a sweep launch sizes its shared memory for its widest case).
   bs_status init_lanes(const std::vector<bsd::CaseDev>& hc) {
     const int L = std::min(n_, kMaxLanes);
     if (L < 2) return BS_OK;
+    auto cells = [&](int c) { return int64_t(hc[c].ni) * hc[c].nj; };
     std::vector<int> order(n_);
     for (int c = 0; c < n_; c++) order[c] = c;
-    std::sort(order.begin(), order.end(), [&](int a, int b) {
-      return int64_t(hc[a].ni) * hc[a].nj > int64_t(hc[b].ni) * hc[b].nj;
-    });
     std::vector<std::vector<int>> members(L);
-    std::vector<int64_t> load(L, 0);
-    for (int c : order) {
-      const int l = int(std::min_element(load.begin(), load.end()) - load.begin());
-      members[l].push_back(c);
-      load[l] += int64_t(hc[c].ni) * hc[c].nj;
+    if (n_ < 4 * L) {
+      std::sort(order.begin(), order.end(), [&](int a, int b) { return cells(a) > cells(b); });
+      std::vector<int64_t> load(L, 0);
+      for (int c : order) {
+        const int l = int(std::min_element(load.begin(), load.end()) - load.begin());
+        members[l].push_back(c);
+        load[l] += cells(c);
+      }
+    } else {
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return hc[a].nj != hc[b].nj ? hc[a].nj > hc[b].nj : cells(a) > cells(b);
+      });
+      int64_t total = 0;
+      for (int c = 0; c < n_; c++) total += cells(c);
+      int64_t acc = 0;
+      int l = 0;
+      for (int k = 0; k < n_; k++) {
+        // Move to the next lane once this one has its share, or when the
+        // cases left are just enough to give every later lane one.
+        const int after = L - 1 - l;
+        const bool share = acc >= total * (l + 1) / L;
+        if (after > 0 && !members[l].empty() && (share || n_ - k <= after)) l++;
+        members[l].push_back(order[k]);
+        acc += cells(order[k]);
+      }
     }
+    for (auto& m : members)
+      if (m.empty()) return fail(BS_EXECUTION, "internal error: an empty lane");
     BS_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
     for (int l = 0; l < L; l++) {
       auto lane = std::make_unique<Lane>();
