@@ -426,6 +426,17 @@ typedef struct bs_shock {
 BS_API bs_status bs_oblique_shock(double mach, double theta, double gamma, bs_shock *out);
 BS_API bs_status bs_normal_shock(double mach, double gamma, bs_shock *out);
 
+/* ---- learned warm start (no counterpart in the reference) -----------------
+ *
+ * The tensor-core GEMM under the warm-start network, exposed for testing:
+ * C (m x n, FP32, row-major) = A (m x k) . B (n x k)^T with A and B bf16,
+ * row-major, on the device; n a multiple of 64, k a multiple of 64, 16-byte
+ * aligned pointers. With `accumulate`, C += A B^T with K split over `splits`
+ * CTAs per tile (FP32 atomics); otherwise splits must be 1. `stream` is a
+ * cudaStream_t (NULL: default stream); the call returns after the GEMM. */
+BS_API bs_status bs_gemm_bf16(const void *a, const void *b, float *c, int32_t m, int32_t n, int32_t k,
+                              int32_t splits, int32_t accumulate, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
