@@ -106,6 +106,15 @@ SIGNATURES: dict[str, list] = {
     "bs_oblique_shock": [C.c_double, C.c_double, C.c_double, C.POINTER(abi.Shock)],
     "bs_normal_shock": [C.c_double, C.c_double, C.POINTER(abi.Shock)],
     "bs_gemm_bf16": [_vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _vp],
+    "bs_mlp_create": [C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(_vp)],
+    "bs_mlp_destroy": [_vp],
+    "bs_mlp_param_count": [_vp, C.POINTER(C.c_int64)],
+    "bs_mlp_get_params": [_vp, _vp],
+    "bs_mlp_set_params": [_vp, _vp],
+    "bs_mlp_set_data": [_vp, C.c_int64, _vp, _vp],
+    "bs_mlp_train": [_vp, C.c_int32, C.c_float, C.c_uint64, _vp],
+    "bs_mlp_loss_grad": [_vp, C.c_int32, _vp, _vp, _vp, _vp],
+    "bs_mlp_predict": [_vp, C.c_int64, _vp, _vp],
 }
 
 

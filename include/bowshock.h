@@ -437,6 +437,46 @@ BS_API bs_status bs_normal_shock(double mach, double gamma, bs_shock *out);
 BS_API bs_status bs_gemm_bf16(const void *a, const void *b, float *c, int32_t m, int32_t n, int32_t k,
                               int32_t splits, int32_t accumulate, void *stream);
 
+/* The warm-start network: a GELU MLP from one grid cell's sample to its
+ * steady primitive state, trained with Adam on solved cases, all on the GPU
+ * (BF16 weights and activations, FP32 accumulation and master weights).
+ *
+ * A sample is 10 floats: the cell centroid (x, r) in body diameters and 8
+ * case values (nose family one-hot over conical, ogive, parabolic, ellipsoid,
+ * haack; fineness / 5; body length / 8; Mach / 5). A target or prediction is
+ * 4 floats: log(rho / rho_inf), u / u_inf, v / u_inf, log(p / p_inf).
+ * Inside, the sample becomes 74 features (x / 8, r / 4, the case values, and
+ * sin and cos of pi 2^(7k/15) x / 8 and r / 4, k = 0..15), padded to 128.
+ *
+ * Parameters, flat, layer by layer: W (out x in, row-major) then b (out);
+ * in = 128 for the first layer, out = 128 for the last (only its first 4
+ * outputs are used; the other rows stay zero). One call at a time per network
+ * (BS_BUSY otherwise). */
+typedef struct bs_mlp bs_mlp;
+
+/* hidden_layers of width 256 (width must be 256); `batch` (a multiple of
+ * 128) samples per training step and per inference pass; weights drawn from
+ * `seed`. */
+BS_API bs_status bs_mlp_create(int32_t hidden_layers, int32_t width, int32_t batch, uint64_t seed,
+                               bs_mlp **out);
+BS_API bs_status bs_mlp_destroy(bs_mlp *net);
+BS_API bs_status bs_mlp_param_count(const bs_mlp *net, int64_t *out);
+BS_API bs_status bs_mlp_get_params(bs_mlp *net, float *out);
+BS_API bs_status bs_mlp_set_params(bs_mlp *net, const float *params);
+/* The training set: n samples (n x 10) and targets (n x 4), copied to the
+ * device. */
+BS_API bs_status bs_mlp_set_data(bs_mlp *net, int64_t n, const float *samples, const float *targets);
+/* `steps` Adam steps (learning rate lr) on random batches of the training
+ * set drawn from `seed`; losses[s] (if not NULL) is step s's mean squared
+ * error over the batch's 4 outputs. */
+BS_API bs_status bs_mlp_train(bs_mlp *net, int32_t steps, float lr, uint64_t seed, float *losses);
+/* Loss and parameter gradients (flat, as the parameters) over n <= batch
+ * given samples, without changing the network. */
+BS_API bs_status bs_mlp_loss_grad(bs_mlp *net, int32_t n, const float *samples, const float *targets,
+                                  float *loss, float *grads);
+/* Predictions (n x 4) for n samples (n x 10). */
+BS_API bs_status bs_mlp_predict(bs_mlp *net, int64_t n, const float *samples, float *out);
+
 #ifdef __cplusplus
 }
 #endif
