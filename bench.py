@@ -410,6 +410,77 @@ def run_seeded(args) -> None:
     batch.destroy()
 
 
+def run_warmstart(args) -> None:
+    """The learned warm start: `--train-cases` seeded 160x80 cases are solved
+    cold in one batch and their fields train the network (5 x 256 GELU, Adam,
+    tcgen05 GEMMs); `--eval-cases` held-out seeds are then solved in one batch
+    from the free stream and from the network's fields. One JSON line: the
+    warm-started batch's solves/s, its LU-SGS steps against the cold batch's,
+    the drag difference, and the plain cold single-case solve rate."""
+    import torch
+
+    from bowshock_b200.mlp import WarmStartNet
+    from bowshock_b200.warmstart import solve_cases, training_set, warm_solve
+    from bowshock_b200.workloads import seeded_cases
+
+    torch.cuda.set_device(0)
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    train, _ = seeded_cases(args.train_cases, first_seed=1, threads=threads, levels=(2,))
+    held, _ = seeded_cases(args.eval_cases, first_seed=1_000_001, threads=threads, levels=(2,))
+    grid_s = time.perf_counter() - t0
+
+    solved = solve_cases(train, max_steps=args.max_steps, keep_fields=True)
+    ok = [k for k, s in enumerate(solved.status) if s == 0]
+    samples, targets = training_set([train[k] for k in ok], [solved.fields[k] for k in ok],
+                                    args.cells_per_case)
+    solved.fields = None
+    net = WarmStartNet(hidden_layers=5, batch=16384, seed=1)
+    net.set_data(samples, targets)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = []
+    # Learning rate: 1e-3, then 3e-4, then 1e-4 over the three thirds.
+    third = max(1, args.train_steps // 3)
+    for phase, lr in enumerate((1e-3, 3e-4, 1e-4)):
+        losses.extend(net.train(third, lr, seed=101 + phase).tolist())
+    train_s = time.perf_counter() - t0
+
+    cold = solve_cases(held, max_steps=args.max_steps)
+    good = [k for k, s in enumerate(cold.status) if s == 0]
+    t0 = time.perf_counter()
+    warm, fell_back = warm_solve(net, held, max_steps=args.max_steps)
+    warm_wall_s = time.perf_counter() - t0
+    single = solve_cases(held[good[0]:good[0] + 1], max_steps=args.max_steps)
+    cd_diff = max(abs(warm.drags[k] - cold.drags[k]) / abs(cold.drags[k]) for k in good)
+    n = len(held)
+    print(json.dumps({
+        "metric": "warm-started steady solves/s to RMS density residual 1e-6 (seeded 160x80 batch, LU-SGS CFL 5)",
+        "value": sum(1 for s in warm.status if s == 0) / (warm.device_ms / 1000), "unit": UNIT,
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f64 solve, bf16/fp32 network", "data": "synthetic",
+        "config": {"workload": f"train on {len(ok)} converged of {len(train)} seeded 160x80 cases "
+                               f"({args.cells_per_case} random cells each, {len(samples)} samples), "
+                               f"evaluate on {n} held-out seeds", "network": "5 x 256 GELU, Fourier features",
+                   "train_steps": 3 * third, "batch": 16384, "grid_build_s": grid_s},
+        "train": {"solve_device_ms": solved.device_ms, "seconds": train_s,
+                  "loss_first": float(np.mean(losses[:10])), "loss_last": float(np.mean(losses[-10:]))},
+        "cold": {"solves_per_s": len(good) / (cold.device_ms / 1000), "device_ms": cold.device_ms,
+                 "steps_median": int(statistics.median([cold.steps[k] for k in good])),
+                 "steps_total": int(sum(cold.steps[k] for k in good)),
+                 "initial_residual_median": float(statistics.median([cold.initial_residual[k] for k in good]))},
+        "warm": {"device_ms": warm.device_ms, "wall_s_with_prediction": warm_wall_s,
+                 "steps_median": int(statistics.median([warm.steps[k] for k in good])),
+                 "steps_total": int(sum(warm.steps[k] for k in good)), "fell_back": len(fell_back),
+                 "initial_residual_median": float(statistics.median([warm.initial_residual[k] for k in good]))},
+        "step_ratio_cold_over_warm": sum(cold.steps[k] for k in good) / max(1, sum(warm.steps[k] for k in good)),
+        "cd_max_rel_diff_warm_vs_cold": cd_diff,
+        "single_case_cold_solves_per_s": 1000.0 / single.device_ms,
+        "warm_batch_over_single_cold": (sum(1 for s in warm.status if s == 0) / (warm.device_ms / 1000))
+                                       / (1000.0 / single.device_ms),
+    }), flush=True)
+    net.destroy()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -419,7 +490,11 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--probe", type=int, default=0,
                     help="run this many LU-SGS steps of the batch with per-kernel timing and exit")
-    ap.add_argument("--workload", choices=["drag-curve", "seeded"], default="drag-curve")
+    ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart"], default="drag-curve")
+    ap.add_argument("--train-cases", type=int, default=4096, help="warm start: training seeds")
+    ap.add_argument("--eval-cases", type=int, default=512, help="warm start: held-out seeds")
+    ap.add_argument("--train-steps", type=int, default=3000, help="warm start: Adam steps")
+    ap.add_argument("--cells-per-case", type=int, default=4096, help="warm start: cells sampled per case")
     ap.add_argument("--cases", type=int, default=2048, help="seeded workload: cases drawn")
     ap.add_argument("--max-steps", type=int, default=5000, help="seeded workload: steps per case")
     ap.add_argument("--check", type=int, default=16,
@@ -434,6 +509,9 @@ def main() -> None:
         return
     if args.workload == "seeded":
         run_seeded(args)
+        return
+    if args.workload == "warmstart":
+        run_warmstart(args)
         return
     run_gpu(args, world, rank, local)
 
