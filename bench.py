@@ -481,6 +481,33 @@ def run_warmstart(args) -> None:
     net.destroy()
 
 
+def run_gemm(args) -> None:
+    """Throughput of the warm-start network's tensor-core GEMM (tcgen05, bf16
+    in, FP32 accumulate) on the network's layer shapes at large batches."""
+    import ctypes as C
+
+    import torch
+
+    from bowshock_b200 import _native
+
+    lib = _native.load()
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("bf16_tflops", 1590.0)
+    rows = []
+    for m, n, k in [(16384, 256, 256), (65536, 256, 256), (131072, 256, 256), (16384, 256, 4096),
+                    (8192, 8192, 8192)]:
+        a = torch.randn(m, k, device="cuda").to(torch.bfloat16)
+        b = torch.randn(n, k, device="cuda").to(torch.bfloat16)
+        c = torch.empty(m, n, device="cuda")
+        ms = C.c_float()
+        _native.check(lib.bs_gemm_bf16_time(a.data_ptr(), b.data_ptr(), c.data_ptr(), m, n, k, 20, C.byref(ms)), lib)
+        tf = 2.0 * m * n * k / (ms.value / 1000) / 1e12
+        rows.append({"m": m, "n": n, "k": k, "ms": ms.value, "tflops": tf, "frac_of_measured_peak": tf / peak})
+        del a, b, c
+    print(json.dumps({"gemm": rows, "peak_tflops": peak, "peak_source": "measured" if peaks else "fallback"}),
+          flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -490,7 +517,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--probe", type=int, default=0,
                     help="run this many LU-SGS steps of the batch with per-kernel timing and exit")
-    ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart"], default="drag-curve")
+    ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart", "gemm"], default="drag-curve")
     ap.add_argument("--train-cases", type=int, default=4096, help="warm start: training seeds")
     ap.add_argument("--eval-cases", type=int, default=512, help="warm start: held-out seeds")
     ap.add_argument("--train-steps", type=int, default=3000, help="warm start: Adam steps")
@@ -512,6 +539,9 @@ def main() -> None:
         return
     if args.workload == "warmstart":
         run_warmstart(args)
+        return
+    if args.workload == "gemm":
+        run_gemm(args)
         return
     run_gpu(args, world, rank, local)
 

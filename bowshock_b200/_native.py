@@ -106,6 +106,7 @@ SIGNATURES: dict[str, list] = {
     "bs_oblique_shock": [C.c_double, C.c_double, C.c_double, C.POINTER(abi.Shock)],
     "bs_normal_shock": [C.c_double, C.c_double, C.POINTER(abi.Shock)],
     "bs_gemm_bf16": [_vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _vp],
+    "bs_gemm_bf16_time": [_vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_float)],
     "bs_mlp_create": [C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(_vp)],
     "bs_mlp_destroy": [_vp],
     "bs_mlp_param_count": [_vp, C.POINTER(C.c_int64)],

@@ -539,6 +539,45 @@ bs_status bs_gemm_bf16(const void* a, const void* b, float* c, int32_t m, int32_
   return BS_OK;
 }
 
+bs_status bs_gemm_bf16_time(const void* a, const void* b, float* c, int32_t m, int32_t n, int32_t k,
+                            int32_t iterations, float* ms) {
+  if (a == nullptr || b == nullptr || c == nullptr || ms == nullptr || iterations < 1)
+    return bs::fail(BS_INVALID_ARGUMENT, "null pointer or no iterations");
+  const int bn = n % 256 == 0 ? 256 : n % 128 == 0 ? 128 : n % 64 == 0 ? 64 : 0;
+  if (bn == 0) return bs::fail(BS_INVALID_ARGUMENT, "GEMM n must be a multiple of 64");
+  CUtensorMap ma, mb;
+  BS_TRY_ST(bsm::make_map(&ma, a, m, k, bsm::kBM));
+  BS_TRY_ST(bsm::make_map(&mb, b, n, k, bn));
+  bsm::Buf<int> err;
+  MLP_CUDA(err.alloc(1));
+  const bsd::umma::EpiStoreF32 epi{c, n};
+  auto run = [&]() -> bs_status {
+    if (bn == 256) return bsm::gemm<256>(ma, mb, m, n, k, 1, epi, err.p, nullptr);
+    if (bn == 128) return bsm::gemm<128>(ma, mb, m, n, k, 1, epi, err.p, nullptr);
+    return bsm::gemm<64>(ma, mb, m, n, k, 1, epi, err.p, nullptr);
+  };
+  BS_TRY_ST(run());  // warm-up
+  cudaEvent_t e0, e1;
+  MLP_CUDA(cudaEventCreate(&e0));
+  MLP_CUDA(cudaEventCreate(&e1));
+  cudaEventRecord(e0, nullptr);
+  bs_status st = BS_OK;
+  for (int it = 0; it < iterations && st == BS_OK; it++) st = run();
+  cudaEventRecord(e1, nullptr);
+  const cudaError_t e = cudaEventSynchronize(e1);
+  float total = 0.f;
+  cudaEventElapsedTime(&total, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != BS_OK) return st;
+  if (e != cudaSuccess) return bs::fail(BS_EXECUTION, std::string("GEMM timing: ") + cudaGetErrorString(e));
+  int h = 0;
+  MLP_CUDA(cudaMemcpy(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h != 0) return bs::fail(BS_EXECUTION, "GEMM: a pipeline wait timed out");
+  *ms = total / float(iterations);
+  return BS_OK;
+}
+
 bs_status bs_mlp_create(int32_t hidden_layers, int32_t width, int32_t batch, uint64_t seed, bs_mlp** out) {
   if (out == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null output");
   *out = nullptr;

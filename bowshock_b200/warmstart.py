@@ -76,11 +76,14 @@ def predicted_starts(net: WarmStartNet, cases) -> list[np.ndarray]:
     return starts
 
 
-def warm_solve(net: WarmStartNet, cases, max_steps: int = 5000) -> tuple[BatchSolve, list[int]]:
-    """Warm-started batch; cases whose warm start fails are solved again from
-    the free stream (their steps and time are added). Returns the combined
-    result and the indices that fell back."""
-    warm = solve_cases(cases, predicted_starts(net, cases), max_steps=max_steps)
+def warm_solve(net: WarmStartNet, cases, max_steps: int = 5000,
+               warm_steps: int = 2500) -> tuple[BatchSolve, list[int]]:
+    """Warm-started batch; cases whose warm start fails (non-physical, or not
+    converged within `warm_steps`, about three times a typical cold solve
+    here) are solved again from the free stream within `max_steps` (their
+    steps and time are added). Returns the combined result and the indices
+    that fell back."""
+    warm = solve_cases(cases, predicted_starts(net, cases), max_steps=min(warm_steps, max_steps))
     failed = [k for k, s in enumerate(warm.status) if s != 0]
     if failed:
         cold = solve_cases([cases[k] for k in failed], max_steps=max_steps)

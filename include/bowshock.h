@@ -436,6 +436,11 @@ BS_API bs_status bs_normal_shock(double mach, double gamma, bs_shock *out);
  * cudaStream_t (NULL: default stream); the call returns after the GEMM. */
 BS_API bs_status bs_gemm_bf16(const void *a, const void *b, float *c, int32_t m, int32_t n, int32_t k,
                               int32_t splits, int32_t accumulate, void *stream);
+/* The same GEMM (no split, C stored) launched `iterations` times back to back
+ * on the default stream after one warm-up; *ms = CUDA-event milliseconds per
+ * launch. */
+BS_API bs_status bs_gemm_bf16_time(const void *a, const void *b, float *c, int32_t m, int32_t n, int32_t k,
+                                   int32_t iterations, float *ms);
 
 /* The warm-start network: a GELU MLP from one grid cell's sample to its
  * steady primitive state, trained with Adam on solved cases, all on the GPU
