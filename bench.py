@@ -72,6 +72,24 @@ def dist_env() -> tuple[int, int, int]:
     return world, rank, local
 
 
+def max_over_ranks(value: float, world: int, device: str) -> float:
+    """The largest `value` over the ranks of the job; every rank calls it at
+    the same point (the job's time is its slowest rank's)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_solves_per_s(world: int, cases_per_rank: int, steps: int, job_ms: float) -> float:
+    """Whole-job throughput: every rank solves its own cases (weak scaling)."""
+    return world * cases_per_rank * steps / (job_ms / 1000)
+
+
 class Clocks:
     """nvidia-smi clock and throttle samples during the timed region."""
 
@@ -220,12 +238,8 @@ def run_gpu(args, world, rank, local) -> None:
     torch.cuda.synchronize()
     barrier()
     clock_info = clocks.stop()
-    total_ms = sum(device_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * n * args.steps / (total_ms / 1000)
+    total_ms = max_over_ranks(sum(device_ms), world, f"cuda:{local}")
+    value = job_solves_per_s(world, n, args.steps, total_ms)
     converged = all(r.status == 0 for r in results)
     steps_taken = [r.steps for r in results]
 
@@ -247,12 +261,8 @@ def run_gpu(args, world, rank, local) -> None:
                     check_every=CHECK_EVERY, cfl=CFL, omega=OMEGA)
         drags = [batch.forebody_drag(k, c.free, c.body.nose.base_radius) for k, c in enumerate(cases)]
         e2e_times.append(time.perf_counter() - t0)
-    e2e_total = sum(e2e_times)
-    if world > 1:
-        t = torch.tensor([e2e_total], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * n * args.steps / e2e_total
+    e2e_total = max_over_ranks(sum(e2e_times), world, f"cuda:{local}")
+    e2e_value = job_solves_per_s(world, n, args.steps, 1000 * e2e_total)
 
     # Roofline of the dominant kernel, timed with CUDA events on the
     # library's stream over the same solve from the free stream.
@@ -508,6 +518,36 @@ def run_gemm(args) -> None:
           flush=True)
 
 
+def run_stencil(args) -> None:
+    """HBM throughput of the stencil kernels on a batch larger than L2:
+    `--cases` copies of a 640x320 case (a 15 deg cone, explicit SSP-RK3 stages;
+    the fineness-3 ogive, LU-SGS passes), each kernel timed with CUDA events
+    over 20 launches; algorithmic bytes per cell as in DESIGN.md."""
+    from bowshock_b200.batch import CudaBatch
+    from bowshock_b200.workloads import cone_case, ogive_case
+
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    n = args.stencil_cases
+    out = {"cases": n, "grid": "640x320", "peak_gbs": peak, "peak_source": "measured" if peaks else "fallback"}
+    cone = cone_case(640, 320)
+    ogive = ogive_case(2.0, 640, 320)
+    cells = 640 * 320 * n
+    for name, case, method, kinds in (
+            ("explicit", cone, "explicit", (("ssprk3_stage1", 108), ("ssprk3_stage2", 140))),
+            ("lusgs", ogive, "lusgs", (("lusgs_prepare", BYTES_PREPARE), ("lusgs_sweep", BYTES_SWEEP),
+                                       ("lusgs_update", BYTES_UPDATE)))):
+        batch = CudaBatch([case.config] * n, precision=64)
+        batch.set_free_stream()
+        batch.kernel_times(method, CFL, OMEGA, iterations=3)
+        ms = batch.kernel_times(method, CFL, OMEGA, iterations=20)
+        for (kind, bytes_per_cell), t in zip(kinds, ms):
+            gbs = bytes_per_cell * cells / (t / 1000) / 1e9
+            out[kind] = {"ms": t, "bytes_per_cell": bytes_per_cell, "gbs": gbs, "frac_of_peak": gbs / peak}
+        batch.destroy()
+    print(json.dumps(out), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -517,12 +557,13 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--probe", type=int, default=0,
                     help="run this many LU-SGS steps of the batch with per-kernel timing and exit")
-    ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart", "gemm"], default="drag-curve")
+    ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart", "gemm", "stencil"], default="drag-curve")
     ap.add_argument("--train-cases", type=int, default=4096, help="warm start: training seeds")
     ap.add_argument("--eval-cases", type=int, default=512, help="warm start: held-out seeds")
     ap.add_argument("--train-steps", type=int, default=3000, help="warm start: Adam steps")
     ap.add_argument("--cells-per-case", type=int, default=4096, help="warm start: cells sampled per case")
     ap.add_argument("--cases", type=int, default=2048, help="seeded workload: cases drawn")
+    ap.add_argument("--stencil-cases", type=int, default=32, help="stencil workload: 640x320 cases")
     ap.add_argument("--max-steps", type=int, default=5000, help="seeded workload: steps per case")
     ap.add_argument("--check", type=int, default=16,
                     help="seeded workload: smallest converged cases checked against the FP64 oracle")
@@ -542,6 +583,9 @@ def main() -> None:
         return
     if args.workload == "gemm":
         run_gemm(args)
+        return
+    if args.workload == "stencil":
+        run_stencil(args)
         return
     run_gpu(args, world, rank, local)
 

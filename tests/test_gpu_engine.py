@@ -232,3 +232,31 @@ def test_non_physical_initial_state_is_rejected():
         w = uniform_primitives(cfg, Primitive2D(1.0, 0.0, 0.0, -1.0))
         with pytest.raises(NonPhysicalStateError):
             e.set_primitives(w)
+
+
+def test_overlapping_calls_on_one_engine_return_busy():
+    """One operation at a time per engine (ExclusiveRunner,
+    src/engine-gpu/gpu-common.ts:122-140): a call made while another thread's
+    call runs gets BS_BUSY, and the engine works again afterwards."""
+    import threading
+    import time
+
+    from bowshock_b200._native import BusyError
+
+    cfg, free, _ = config1()
+    with CudaEuler2D(cfg, 64) as e:
+        e.set_uniform(free.state)
+        worker = threading.Thread(target=e.iterate, args=(6000,))
+        worker.start()
+        seen = False
+        for _ in range(4000):
+            try:
+                e.density_residual_norm()
+            except BusyError:
+                seen = True
+                break
+            time.sleep(0.0002)
+        worker.join()
+        assert seen
+        assert e.steps() == 6000
+        assert math.isfinite(e.density_residual_norm())
