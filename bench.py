@@ -207,6 +207,9 @@ def run_gpu(args, world, rank, local) -> None:
     cases = drag_sweep_cases()
     n = len(cases)
     batch = CudaBatch([c.config for c in cases], precision=64)
+    # Setup, untimed: the autotuner picks the number of lanes.
+    batch.set_free_stream()
+    lanes, _ = batch.autotune("lusgs", 40, CFL, OMEGA)
     flush = torch.empty(512 * 2**20 // 4, dtype=torch.int32, device=f"cuda:{local}")
     start_fields = [np.tile(np.array([c.free.state.rho, c.free.state.u, c.free.state.v,
                                       c.free.state.p]), c.config.grid.ni * c.config.grid.nj)
@@ -306,7 +309,7 @@ def run_gpu(args, world, rank, local) -> None:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": workload_config(),
+            "data": "synthetic", "config": dict(workload_config(), lanes=lanes),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
@@ -365,6 +368,8 @@ def run_seeded(args) -> None:
     n = len(cases)
     cells = [c.config.grid.ni * c.config.grid.nj for c in cases]
     batch = CudaBatch([c.config for c in cases], precision=64)
+    batch.set_free_stream()
+    lanes, _ = batch.autotune("lusgs", 40, CFL, OMEGA)
     flush = torch.empty(512 * 2**20 // 4, dtype=torch.int32, device="cuda:0")
 
     def one_step():
@@ -407,7 +412,7 @@ def run_seeded(args) -> None:
                                "the grid generator): nose conical/tangent ogive/parabolic/ellipsoid/"
                                "Von Karman, fineness U[1,5], body length U[2,8], Mach U[1.5,5], "
                                f"ni = 40*2^k (k in 0..3), nj = ni/2, at most {args.max_steps} steps each",
-                   "cells_total": sum(cells), "grid_build_s": grid_s,
+                   "cells_total": sum(cells), "grid_build_s": grid_s, "lanes": lanes,
                    "l2": "flushed between timed steps (512 MiB device write)"},
         "gpu_launches": launches,
         "converged": len(converged),

@@ -91,6 +91,16 @@ class CudaBatch:
         self._call("bs_batch_last_solve_timing", C.byref(ms), C.byref(launches))
         return ms.value, launches.value
 
+    def autotune(self, method: str = "lusgs", steps: int = 40, cfl: float = 5.0,
+                 omega: float = 1.5) -> tuple[int, float]:
+        """Chooses the number of lanes by timing `steps` steps with each
+        candidate (the state is unchanged); returns (lanes, ms per step)."""
+        lanes = C.c_int32()
+        ms = C.c_double()
+        self._call("bs_batch_autotune", 1 if method == "lusgs" else 0, steps, cfl, omega,
+                   C.byref(lanes), C.byref(ms))
+        return lanes.value, ms.value
+
     def kernel_times(self, method: str = "lusgs", cfl: float = 5.0, omega: float = 1.5,
                      iterations: int = 20) -> tuple[float, float, float]:
         ms = np.empty(3)

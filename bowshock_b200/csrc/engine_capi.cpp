@@ -403,4 +403,19 @@ bs_status bs_batch_kernel_times(bs_batch* batch, int32_t method, double cfl, dou
   });
 }
 
+bs_status bs_batch_autotune(bs_batch* batch, int32_t method, int32_t steps, double cfl, double omega,
+                            int32_t* lanes, double* ms_per_step) {
+  BS_BATCH_CALL(batch, {
+    if (lanes == nullptr || ms_per_step == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+    int l = 0;
+    double ms = 0;
+    const bs_status st = batch->solver->autotune(method, steps, cfl, omega, &l, &ms);
+    if (st == BS_OK) {
+      *lanes = l;
+      *ms_per_step = ms;
+    }
+    return st;
+  });
+}
+
 }  // extern "C"

@@ -115,7 +115,8 @@ struct LaneView {
   cudaStream_t stream;
 };
 
-constexpr int kMaxLanes = 16;
+constexpr int kMaxLanes = 64;
+constexpr int kDefaultLanes = 16;
 
 template <class R>
 class Solver final : public SolverBase {
@@ -264,15 +265,32 @@ class Solver final : public SolverBase {
       }
     }
     BS_CUDA(cudaMemcpy(bgeom_.p, bg.data(), bg.size() * sizeof(double), cudaMemcpyHostToDevice));
-    return init_lanes(hc);
+    hc_ = hc;
+    return init_lanes(hc, std::min(n_, kDefaultLanes));
+  }
+
+  // Frees the lanes, their streams and events, and every captured graph
+  // (whose launches reference the lanes).
+  void release_lanes() {
+    cudaStreamSynchronize(stream_);
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+    graph_launches_.clear();
+    for (auto& l : lanes_)
+      if (l->stream != nullptr) cudaStreamDestroy(l->stream);
+    lanes_.clear();
+    for (auto e : ev_join_) cudaEventDestroy(e);
+    ev_join_.clear();
+    if (ev_fork_ != nullptr) cudaEventDestroy(ev_fork_);
+    ev_fork_ = nullptr;
   }
 
   // Splits the cases into lanes of about equal cell counts. A few cases per
   // lane: largest first, each to the lightest lane. Many: contiguous runs of
   // the cases sorted by width, so that a lane's sweep CTAs share one size
   // class (a sweep launch sizes its shared memory for its widest case).
-  bs_status init_lanes(const std::vector<bsd::CaseDev>& hc) {
-    const int L = std::min(n_, kMaxLanes);
+  bs_status init_lanes(const std::vector<bsd::CaseDev>& hc, int lanes) {
+    const int L = std::max(1, std::min({n_, kMaxLanes, lanes}));
     if (L < 2) return BS_OK;
     auto cells = [&](int c) { return int64_t(hc[c].ni) * hc[c].nj; };
     std::vector<int> order(n_);
@@ -389,6 +407,63 @@ class Solver final : public SolverBase {
     }
     return BS_OK;
   }
+
+  // Times `steps` steps from the current state with 1, 2, 4, ... lanes (up to
+  // 64 and the case count), each after one untimed run that captures its
+  // graphs, restoring the state before every run; keeps the fastest. The
+  // state, CFL numbers and status words are as before the call.
+  bs_status autotune(int method, int steps, double cfl, double omega, int* lanes, double* ms_per_step) override {
+    if (steps < 1) return fail(BS_INVALID_ARGUMENT, "autotune needs steps >= 1");
+    if (method == kMethodImplicit) {
+      if (!(cfl > 0 && omega >= 1)) return fail(BS_INVALID_ARGUMENT, "LU-SGS needs cfl > 0 and omega >= 1");
+      BS_TRY(ensure_implicit());
+      BS_TRY(set_implicit_params(cfl, omega, 1.0));
+    } else {
+      BS_TRY(ensure_explicit());
+    }
+    DevBuf<R> saved[4];
+    for (int v = 0; v < 4; v++) {
+      BS_CUDA(saved[v].alloc(total_cells_));
+      BS_CUDA(cudaMemcpyAsync(saved[v].p, q_[v].p, total_cells_ * sizeof(R), cudaMemcpyDeviceToDevice, stream_));
+    }
+    auto restore = [&]() -> bs_status {
+      for (int v = 0; v < 4; v++)
+        BS_CUDA(cudaMemcpyAsync(q_[v].p, saved[v].p, total_cells_ * sizeof(R), cudaMemcpyDeviceToDevice, stream_));
+      if (method == kMethodImplicit) BS_TRY(set_implicit_cfl(cfl));
+      BS_CUDA(cudaMemsetAsync(status_.p, 0, n_ * sizeof(unsigned), stream_));
+      return BS_OK;
+    };
+    std::fill(active_h_.begin(), active_h_.end(), 1);
+    BS_TRY(upload_active());
+    int best = 0;
+    double best_ms = 0;
+    for (int L = 1; L <= std::min(n_, kMaxLanes); L *= 2) {
+      release_lanes();
+      BS_TRY(init_lanes(hc_, L));
+      BS_TRY(restore());
+      BS_TRY(run_steps(method, steps, false));
+      BS_TRY(restore());
+      BS_CUDA(cudaEventRecord(ev0_, stream_));
+      BS_TRY(run_steps(method, steps, false));
+      BS_CUDA(cudaEventRecord(ev1_, stream_));
+      BS_CUDA(cudaEventSynchronize(ev1_));
+      float t = 0;
+      BS_CUDA(cudaEventElapsedTime(&t, ev0_, ev1_));
+      if (best == 0 || t < best_ms) {
+        best = L;
+        best_ms = t;
+      }
+    }
+    release_lanes();
+    BS_TRY(init_lanes(hc_, best));
+    BS_TRY(restore());
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    *lanes = best;
+    *ms_per_step = best_ms / steps;
+    return BS_OK;
+  }
+
+  int lanes() const override { return std::max<int>(1, int(lanes_.size())); }
 
   bs_status kernel_times(int method, double cfl, double omega, int iterations, double* ms) override {
     if (iterations < 1) return fail(BS_INVALID_ARGUMENT, "iterations must be positive");
@@ -987,6 +1062,7 @@ class Solver final : public SolverBase {
     cudaStream_t stream = nullptr;
   };
   std::vector<std::unique_ptr<Lane>> lanes_;
+  std::vector<bsd::CaseDev> hc_;  // the cases as uploaded (to rebuild lanes)
   cudaEvent_t ev_fork_ = nullptr;
   std::vector<cudaEvent_t> ev_join_;
   std::map<GraphKey, cudaGraphExec_t> graphs_;

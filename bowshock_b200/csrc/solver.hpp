@@ -59,6 +59,11 @@ class SolverBase {
   virtual bs_status set_free_stream() = 0;
   virtual bs_status kernel_times(int method, double cfl, double omega, int iterations,
                                  double* ms) = 0;
+  // Chooses how many lanes (concurrent groups of cases) the batch runs, by
+  // timing `steps` steps with each candidate; the state is unchanged.
+  virtual bs_status autotune(int method, int steps, double cfl, double omega, int* lanes,
+                             double* ms_per_step) = 0;
+  virtual int lanes() const = 0;
   virtual int64_t steps(int c) const = 0;
   virtual cudaStream_t stream() const = 0;
   // Device time of the last solve, milliseconds (CUDA events on the stream).

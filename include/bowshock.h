@@ -426,6 +426,14 @@ typedef struct bs_shock {
 BS_API bs_status bs_oblique_shock(double mach, double theta, double gamma, bs_shock *out);
 BS_API bs_status bs_normal_shock(double mach, double gamma, bs_shock *out);
 
+/* Autotuning of a batch (no counterpart in the reference): times `steps`
+ * steps of `method` (0 explicit, 1 LU-SGS with cfl, omega) from the current
+ * state with 1, 2, 4, ... up to 64 lanes (concurrent groups of cases, each on
+ * its own stream) and keeps the fastest for later solves; *lanes is the
+ * choice and *ms_per_step its time. The state is unchanged. */
+BS_API bs_status bs_batch_autotune(bs_batch *batch, int32_t method, int32_t steps, double cfl, double omega,
+                                   int32_t *lanes, double *ms_per_step);
+
 /* ---- learned warm start (no counterpart in the reference) -----------------
  *
  * The tensor-core GEMM under the warm-start network, exposed for testing:

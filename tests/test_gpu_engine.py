@@ -258,5 +258,29 @@ def test_overlapping_calls_on_one_engine_return_busy():
             time.sleep(0.0002)
         worker.join()
         assert seen
-        assert e.steps() == 6000
+        assert e.steps == 6000
         assert math.isfinite(e.density_residual_norm())
+
+
+def test_autotune_keeps_the_state_and_the_answer():
+    from bowshock_b200.batch import CudaBatch
+    from bowshock_b200.workloads import ogive_case
+
+    cases = [ogive_case(m, 40, 20) for m in (1.6, 2.0, 2.4, 2.8, 3.2)]
+    results = []
+    for tune in (False, True):
+        b = CudaBatch([c.config for c in cases], precision=64)
+        b.set_free_stream()
+        b.solve("lusgs", 1e-6, max_steps=60, check_every=20)  # a state away from the free stream
+        before = b.residual_norms()
+        if tune:
+            lanes, ms = b.autotune("lusgs", 10)
+            assert lanes in (1, 2, 4) and ms > 0
+            # The state comes back exactly; the norm's FP64 atomic sums may be
+            # added in another order.
+            assert np.allclose(b.residual_norms(), before, rtol=1e-12, atol=0)
+        res = b.solve("lusgs", 1e-6, max_steps=20000, check_every=20)
+        assert all(r.status == 0 for r in res)
+        results.append([b.forebody_drag(k, c.free, 0.5) for k, c in enumerate(cases)])
+        b.destroy()
+    assert np.allclose(results[0], results[1], rtol=1e-6, atol=0)
