@@ -553,6 +553,44 @@ def run_stencil(args) -> None:
     print(json.dumps(out), flush=True)
 
 
+def run_verified(args) -> None:
+    """Verified forebody drag (the reference's banded answer) for several
+    bodies and Mach numbers at once: grid families nj = 20 .. 160, each grid
+    iterated until its drag settles, one refinement level of every case per
+    GPU batch; the error band from the grid convergence index plus the
+    captured-shock floor (1e-3 of the value)."""
+    import math
+
+    import torch
+
+    from bowshock_b200.verified_drag import DRAG_FLOOR, verified_forebody_drags
+    from bowshock_b200.workloads import cone_body, ogive_body
+
+    torch.cuda.set_device(0)
+    cases = [(cone_body(20, 4.0), m) for m in (2.0, 2.5, 3.0, 3.5, 4.0)] + \
+            [(ogive_body(3.0, 4.0), m) for m in (2.0, 2.5, 3.0)]
+    names = [f"cone20-cyl4-M{m}" for m in (2.0, 2.5, 3.0, 3.5, 4.0)] + \
+            [f"ogive3-cyl4-M{m}" for m in (2.0, 2.5, 3.0)]
+    t0 = time.perf_counter()
+    out = verified_forebody_drags(cases, tolerance=args.band, max_refinement=8)
+    wall = time.perf_counter() - t0
+    rows = []
+    for name, o in zip(names, out):
+        row = {"case": name, "kind": o.kind}
+        if o.result is not None:
+            e = o.result.estimate
+            row.update({"levels": [round(v, 10) for _, v in o.result.levels], "estimate": e.kind,
+                        "value": e.value, "extrapolated": e.extrapolated, "order": e.order,
+                        "band": o.result.uncertainty, "verified": o.result.verified,
+                        "iterations": [r.iterations for r in o.reports]})
+        else:
+            row["reason"] = o.reason
+        rows.append(row)
+    print(json.dumps({"metric": "verified forebody drags (banded) per second", "value": len(cases) / wall,
+                      "unit": "cases/s", "wall_s": wall, "tolerance_abs": args.band, "floor_rel": DRAG_FLOOR,
+                      "cases": rows}), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -562,13 +600,14 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--probe", type=int, default=0,
                     help="run this many LU-SGS steps of the batch with per-kernel timing and exit")
-    ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart", "gemm", "stencil"], default="drag-curve")
+    ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart", "gemm", "stencil", "verified"], default="drag-curve")
     ap.add_argument("--train-cases", type=int, default=4096, help="warm start: training seeds")
     ap.add_argument("--eval-cases", type=int, default=512, help="warm start: held-out seeds")
     ap.add_argument("--train-steps", type=int, default=3000, help="warm start: Adam steps")
     ap.add_argument("--cells-per-case", type=int, default=4096, help="warm start: cells sampled per case")
     ap.add_argument("--cases", type=int, default=2048, help="seeded workload: cases drawn")
     ap.add_argument("--stencil-cases", type=int, default=32, help="stencil workload: 640x320 cases")
+    ap.add_argument("--band", type=float, default=2e-3, help="verified workload: largest band, absolute")
     ap.add_argument("--max-steps", type=int, default=5000, help="seeded workload: steps per case")
     ap.add_argument("--check", type=int, default=16,
                     help="seeded workload: smallest converged cases checked against the FP64 oracle")
@@ -591,6 +630,9 @@ def main() -> None:
         return
     if args.workload == "stencil":
         run_stencil(args)
+        return
+    if args.workload == "verified":
+        run_verified(args)
         return
     run_gpu(args, world, rank, local)
 

@@ -91,6 +91,16 @@ class CudaBatch:
         self._call("bs_batch_last_solve_timing", C.byref(ms), C.byref(launches))
         return ms.value, launches.value
 
+    def iterate(self, steps: int) -> None:
+        """Explicit steps of the active cases."""
+        self._call("bs_batch_iterate", steps)
+
+    def set_active(self, flags) -> None:
+        f = np.ascontiguousarray(np.asarray(flags, dtype=np.int32))
+        if f.size != self.n:
+            raise ValueError("one flag per case")
+        self._call("bs_batch_set_active", f.ctypes.data_as(C.POINTER(C.c_int32)))
+
     def autotune(self, method: str = "lusgs", steps: int = 40, cfl: float = 5.0,
                  omega: float = 1.5) -> tuple[int, float]:
         """Chooses the number of lanes by timing `steps` steps with each

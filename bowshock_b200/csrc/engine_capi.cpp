@@ -403,6 +403,17 @@ bs_status bs_batch_kernel_times(bs_batch* batch, int32_t method, double cfl, dou
   });
 }
 
+bs_status bs_batch_iterate(bs_batch* batch, int32_t steps) {
+  BS_BATCH_CALL(batch, { return batch->solver->iterate(steps); });
+}
+
+bs_status bs_batch_set_active(bs_batch* batch, const int32_t* flags) {
+  BS_BATCH_CALL(batch, {
+    if (flags == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+    return batch->solver->set_active(flags);
+  });
+}
+
 bs_status bs_batch_autotune(bs_batch* batch, int32_t method, int32_t steps, double cfl, double omega,
                             int32_t* lanes, double* ms_per_step) {
   BS_BATCH_CALL(batch, {

@@ -465,6 +465,11 @@ class Solver final : public SolverBase {
 
   int lanes() const override { return std::max<int>(1, int(lanes_.size())); }
 
+  bs_status set_active(const int* flags) override {
+    for (int c = 0; c < n_; c++) active_h_[c] = flags[c] != 0 ? 1 : 0;
+    return upload_active();
+  }
+
   bs_status kernel_times(int method, double cfl, double omega, int iterations, double* ms) override {
     if (iterations < 1) return fail(BS_INVALID_ARGUMENT, "iterations must be positive");
     cudaEvent_t ev[6];

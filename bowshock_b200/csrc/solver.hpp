@@ -64,6 +64,9 @@ class SolverBase {
   virtual bs_status autotune(int method, int steps, double cfl, double omega, int* lanes,
                              double* ms_per_step) = 0;
   virtual int lanes() const = 0;
+  // Which cases later iterate calls advance (1 active, 0 frozen); a solve
+  // sets its own.
+  virtual bs_status set_active(const int* flags) = 0;
   virtual int64_t steps(int c) const = 0;
   virtual cudaStream_t stream() const = 0;
   // Device time of the last solve, milliseconds (CUDA events on the stream).

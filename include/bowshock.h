@@ -308,6 +308,16 @@ BS_API bs_status bs_batch_set_primitives(bs_batch *batch, int32_t c, const doubl
 /* Every case from its own jMax/iMin inflow state (the free stream). */
 BS_API bs_status bs_batch_set_free_stream(bs_batch *batch);
 
+/* `steps` explicit steps (each case's own integrator, CFL and time stepping)
+ * of the batch's active cases, as bs_engine_iterate per case; the
+ * verified-drag driver (src/analysis/verified-drag.ts:258-299) iterates a
+ * family of grids this way between drag checks. */
+BS_API bs_status bs_batch_iterate(bs_batch *batch, int32_t steps);
+
+/* Which cases bs_batch_iterate advances: flags[c] != 0 active, 0 frozen
+ * (a case whose drag has settled). bs_batch_solve sets its own. */
+BS_API bs_status bs_batch_set_active(bs_batch *batch, const int32_t *flags);
+
 /* As bs_engine_solve for every case at once; results[k] for case k. Returns
  * BS_OK when the call ran; each case's outcome is in its result. */
 BS_API bs_status bs_batch_solve(bs_batch *batch, int32_t method, double cfl, double omega,

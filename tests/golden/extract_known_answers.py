@@ -50,6 +50,19 @@ def main() -> None:
         "rows": [[float(v) for v in r] for r in rows],
         "tolerance": {"shock_angle_abs": 5e-6, "surface_mach_rel": 3e-5, "cp_abs": 3e-5},
     }
+    # Grid-convergence families measured on cone-cylinders (mean cone
+    # surface pressure over the free stream's on nj = 20, 40, 80, 160) with
+    # their Taylor-Maccoll values, and the options the reference checks
+    # their bands with.
+    fg = "tests/verification/grid-convergence.test.ts"
+    tg = (REF / fg).read_text()
+    fams = re.findall(r"\['([^']+)',\s*([0-9.]+),\s*\[([0-9.,\s]+)\]\]", tg)
+    out["grid_convergence_cone_families"] = {
+        "source": f"{fg}:{find_line(tg, 'const families')}",
+        "options": {"order_tolerance": 0.5, "noise": 1e-12, "floor": 2e-4, "max_refinement": 8},
+        "families": [{"name": name, "exact": float(exact), "values": [float(v) for v in vals.split(",")]}
+                     for name, exact, vals in fams],
+    }
     out["taylor_maccoll_nparc"] = {
         "source": f"{f}:{find_line(t, 'NPARC/WIND')}",
         "cone_deg": 10, "mach": 2.35,
