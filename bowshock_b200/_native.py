@@ -106,6 +106,7 @@ SIGNATURES: dict[str, list] = {
     "bs_oblique_shock": [C.c_double, C.c_double, C.c_double, C.POINTER(abi.Shock)],
     "bs_normal_shock": [C.c_double, C.c_double, C.POINTER(abi.Shock)],
     "bs_batch_iterate": [_vp, C.c_int32],
+    "bs_batch_flow_field": [_vp, C.c_int32, C.c_int32, C.POINTER(abi.Primitive), C.c_double, _dp],
     "bs_batch_set_active": [_vp, _ip],
     "bs_batch_autotune": [_vp, C.c_int32, C.c_int32, C.c_double, C.c_double, _ip, _dp],
     "bs_gemm_bf16": [_vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _vp],

@@ -91,6 +91,18 @@ class CudaBatch:
         self._call("bs_batch_last_solve_timing", C.byref(ms), C.byref(launches))
         return ms.value, launches.value
 
+    FIELDS = {"schlieren": 0, "mach": 1, "cp": 2, "density": 3}
+
+    def flow_field(self, c: int, field: str, free: FreeStream, length: float = 0.5) -> np.ndarray:
+        """Case c's display field per cell (i fastest), computed on the GPU:
+        'schlieren' (|grad rho| x length / rho_inf), 'mach', 'cp', 'density'."""
+        g = self.configs[c].grid
+        out = np.empty(g.ni * g.nj)
+        st = free.state
+        w = abi.Primitive(st.rho, st.u, st.v, st.p)
+        self._call("bs_batch_flow_field", c, self.FIELDS[field], C.byref(w), float(length), out.ctypes.data_as(_dp))
+        return out
+
     def iterate(self, steps: int) -> None:
         """Explicit steps of the active cases."""
         self._call("bs_batch_iterate", steps)

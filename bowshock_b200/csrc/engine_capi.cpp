@@ -403,6 +403,16 @@ bs_status bs_batch_kernel_times(bs_batch* batch, int32_t method, double cfl, dou
   });
 }
 
+bs_status bs_batch_flow_field(bs_batch* batch, int32_t c, int32_t field, const bs_primitive* free, double length,
+                              double* out) {
+  BS_BATCH_CALL(batch, {
+    if (free == nullptr || out == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+    const bs_status s = check_case(batch, c);
+    if (s != BS_OK) return s;
+    return batch->solver->flow_field(c, field, *free, length, out);
+  });
+}
+
 bs_status bs_batch_iterate(bs_batch* batch, int32_t steps) {
   BS_BATCH_CALL(batch, { return batch->solver->iterate(steps); });
 }

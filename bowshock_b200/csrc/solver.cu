@@ -8,6 +8,7 @@
 #include <cstring>
 
 #include "common.hpp"
+#include "device/fields.cuh"
 #include "device/sweep.cuh"
 #include "device/tile.cuh"
 #include "device/wall.cuh"
@@ -464,6 +465,39 @@ class Solver final : public SolverBase {
   }
 
   int lanes() const override { return std::max<int>(1, int(lanes_.size())); }
+
+  bs_status flow_field(int c, int field, const bs_primitive& free, double length, double* out) override {
+    if (field < bsd::FIELD_SCHLIEREN || field > bsd::FIELD_DENSITY)
+      return fail(BS_INVALID_ARGUMENT, "field: 0 schlieren, 1 mach, 2 cp, 3 density");
+    if (!(free.rho > 0 && free.p > 0)) return fail(BS_INVALID_ARGUMENT, "free stream density and pressure must be positive");
+    if (nodes_x_.p == nullptr) {
+      // The grids' nodes, uploaded on first use (the solve needs only metrics).
+      node_off_.assign(n_, 0);
+      int64_t total = 0;
+      for (int k = 0; k < n_; k++) {
+        node_off_[k] = total;
+        total += int64_t(cases_[k].x.size());
+      }
+      BS_CUDA(nodes_x_.alloc(total));
+      BS_CUDA(nodes_y_.alloc(total));
+      for (int k = 0; k < n_; k++) {
+        BS_CUDA(cudaMemcpy(nodes_x_.p + node_off_[k], cases_[k].x.data(), cases_[k].x.size() * sizeof(double),
+                           cudaMemcpyHostToDevice));
+        BS_CUDA(cudaMemcpy(nodes_y_.p + node_off_[k], cases_[k].y.data(), cases_[k].y.size() * sizeof(double),
+                           cudaMemcpyHostToDevice));
+      }
+    }
+    const int64_t cells = int64_t(cases_[c].cfg.ni) * cases_[c].cfg.nj;
+    DevBuf<double> d_out;
+    BS_CUDA(d_out.alloc(cells));
+    bsd::flow_field_kernel<R><<<unsigned((cells + 255) / 256), 256, 0, stream_>>>(
+        d_cases_.p, c, q_view(), nodes_x_.p + node_off_[c], nodes_y_.p + node_off_[c], field, length, free.rho,
+        free.u, free.v, free.p, d_out.p);
+    BS_CUDA(cudaGetLastError());
+    BS_CUDA(cudaMemcpyAsync(out, d_out.p, cells * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    return BS_OK;
+  }
 
   bs_status set_active(const int* flags) override {
     for (int c = 0; c < n_; c++) active_h_[c] = flags[c] != 0 ? 1 : 0;
@@ -1068,6 +1102,8 @@ class Solver final : public SolverBase {
   };
   std::vector<std::unique_ptr<Lane>> lanes_;
   std::vector<bsd::CaseDev> hc_;  // the cases as uploaded (to rebuild lanes)
+  DevBuf<double> nodes_x_, nodes_y_;  // grid nodes (display fields only)
+  std::vector<int64_t> node_off_;
   cudaEvent_t ev_fork_ = nullptr;
   std::vector<cudaEvent_t> ev_join_;
   std::map<GraphKey, cudaGraphExec_t> graphs_;

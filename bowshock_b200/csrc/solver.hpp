@@ -67,6 +67,9 @@ class SolverBase {
   // Which cases later iterate calls advance (1 active, 0 frozen); a solve
   // sets its own.
   virtual bs_status set_active(const int* flags) = 0;
+  // Case c's display field (0 schlieren, 1 Mach, 2 Cp, 3 density ratio) per
+  // cell, computed on the GPU (free: the free stream's primitives).
+  virtual bs_status flow_field(int c, int field, const bs_primitive& free, double length, double* out) = 0;
   virtual int64_t steps(int c) const = 0;
   virtual cudaStream_t stream() const = 0;
   // Device time of the last solve, milliseconds (CUDA events on the stream).

@@ -318,6 +318,15 @@ BS_API bs_status bs_batch_iterate(bs_batch *batch, int32_t steps);
  * (a case whose drag has settled). bs_batch_solve sets its own. */
 BS_API bs_status bs_batch_set_active(bs_batch *batch, const int32_t *flags);
 
+/* Case c's display field per cell into out (ni nj doubles, cell (i, j) at
+ * i + j ni), computed on the GPU from the current state: the compute half of
+ * the reference's flow view (src/render/flow-fields.ts:36-117; drawing it is
+ * graphics, not done here). field: 0 schlieren (|grad rho| by Green-Gauss in
+ * the plane, times `length` over the free stream's density), 1 Mach number,
+ * 2 pressure coefficient against `free`, 3 density over the free stream's. */
+BS_API bs_status bs_batch_flow_field(bs_batch *batch, int32_t c, int32_t field, const bs_primitive *free,
+                                     double length, double *out);
+
 /* As bs_engine_solve for every case at once; results[k] for case k. Returns
  * BS_OK when the call ran; each case's outcome is in its result. */
 BS_API bs_status bs_batch_solve(bs_batch *batch, int32_t method, double cfl, double omega,
