@@ -49,8 +49,12 @@ __device__ __forceinline__ float radius32(R rho, R u, R v, R p, float gamma, flo
   return fabsf(fu * nx + fv * ny) + __fsqrt_rn((gamma * fp) / fr);
 }
 
-template <class R, int MODE>
-__global__ void __launch_bounds__(TILE_THREADS) tile_kernel(const TileArgs<R> A) {
+// kMinBlocks 4 asks for four resident CTAs per SM (at some spilling): on
+// launches of several waves the fourth CTA's warps fill the issue slots that
+// the others leave while they wait at a barrier for their slowest face; on
+// one wave the default is faster.
+template <class R, int MODE, int kMinBlocks = 1>
+__global__ void __launch_bounds__(TILE_THREADS, kMinBlocks) tile_kernel(const TileArgs<R> A) {
   __shared__ R W[4][TJ + 4][TI + 4];
   __shared__ R Fi[4][TJ][TI + 1];
   __shared__ R Fj[4][TJ + 1][TI];

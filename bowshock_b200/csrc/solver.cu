@@ -140,6 +140,11 @@ class Solver final : public SolverBase {
     BS_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     BS_CUDA(cudaEventCreate(&ev0_));
     BS_CUDA(cudaEventCreate(&ev1_));
+    {
+      int dev = 0;
+      BS_CUDA(cudaGetDevice(&dev));
+      BS_CUDA(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev));
+    }
     std::vector<bsd::CaseDev> hc(n_);
     std::vector<int2> tiles;
     int64_t cell = 0, ifc = 0, jfc = 0, bfc = 0, skw = 0;
@@ -873,7 +878,10 @@ class Solver final : public SolverBase {
     A.cfl = cfl_.p;
     A.omega = omega_.p;
     A.res_out = res_out;
-    bsd::tile_kernel<R, MODE><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
+    if (lane.n_tiles >= 4 * sm_count_)
+      bsd::tile_kernel<R, MODE, 4><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
+    else
+      bsd::tile_kernel<R, MODE><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
     launches_++;
     BS_CUDA(cudaGetLastError());
     return BS_OK;
@@ -1102,6 +1110,7 @@ class Solver final : public SolverBase {
   };
   std::vector<std::unique_ptr<Lane>> lanes_;
   std::vector<bsd::CaseDev> hc_;  // the cases as uploaded (to rebuild lanes)
+  int sm_count_ = 148;
   DevBuf<double> nodes_x_, nodes_y_;  // grid nodes (display fields only)
   std::vector<int64_t> node_off_;
   cudaEvent_t ev_fork_ = nullptr;
