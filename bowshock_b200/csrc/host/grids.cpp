@@ -341,8 +341,34 @@ std::string blunt_body_grid(const Body& body, const BluntGridOptions& o, Grid* o
   }
   const double s_nose = s_of[kProfileSamples];
   const double s_end = s_nose + body.cylinder_length;
+  // Bisection brackets by bucket of s: bracket_lo[b] is the last sample at or
+  // below the bucket's start and bracket_hi[b] the first above its end, so a
+  // search started from them ends on the same sample as one over the whole
+  // table (the arc length grows strictly with u). An s the bucket arithmetic
+  // misplaces fails the bracket test and searches the whole table.
+  const int kBuckets = 2048;
+  const double bucket_scale = kBuckets / s_nose;
+  std::vector<int> bracket_lo(kBuckets), bracket_hi(kBuckets);
+  {
+    int k = 0;
+    for (int b = 0; b < kBuckets; b++) {
+      const double start = b / bucket_scale, end = (b + 1) / bucket_scale;
+      while (k + 1 < kProfileSamples && s_of[k + 1] <= start) k++;
+      bracket_lo[b] = k;
+      int h = k + 1;
+      while (h < kProfileSamples && s_of[h] <= end) h++;
+      bracket_hi[b] = h;
+    }
+  }
   auto u_at = [&](double s) {
     int low = 0, high = kProfileSamples;
+    if (s >= 0 && s < s_nose) {
+      const int b = std::min(int(s * bucket_scale), kBuckets - 1);
+      if (s_of[bracket_lo[b]] <= s && s < s_of[bracket_hi[b]]) {
+        low = bracket_lo[b];
+        high = bracket_hi[b];
+      }
+    }
     while (high - low > 1) {
       const int mid = (low + high) >> 1;
       if (s_of[mid] <= s) low = mid;
@@ -355,16 +381,26 @@ std::string blunt_body_grid(const Body& body, const BluntGridOptions& o, Grid* o
     double x, y, nx, ny;
   };
   // The body point at arc length s and its outward normal.
-  auto surface = [&](double s) -> SurfacePoint {
-    if (s >= s_nose) return {L + (s - s_nose), R, 0, 1};
-    const double u = u_at(s);
-    const double x = profile_x(u), y = profile_r(u);
-    if (u == 0) return {x, y, -1, 0};
+  // The nose's outward normal at profile parameter u (central difference).
+  auto nose_normal = [&](double u, double* nx, double* ny) {
+    if (u == 0) {
+      *nx = -1;
+      *ny = 0;
+      return;
+    }
     const double eps = 1e-7;
     const double ua = std::max(u - eps, 0.0), ub = std::min(u + eps, 1.0);
     const double tx = profile_x(ub) - profile_x(ua), ty = profile_r(ub) - profile_r(ua);
     const double t = std::hypot(tx, ty);
-    return {x, y, -ty / t, tx / t};
+    *nx = -ty / t;
+    *ny = tx / t;
+  };
+  auto surface = [&](double s) -> SurfacePoint {
+    if (s >= s_nose) return {L + (s - s_nose), R, 0, 1};
+    const double u = u_at(s);
+    SurfacePoint p{profile_x(u), profile_r(u), 0, 0};
+    nose_normal(u, &p.nx, &p.ny);
+    return p;
   };
   const SurfacePoint shoulder = surface(s_nose * (1 - 1e-9));
   const double shoulder_angle = std::atan2(-shoulder.nx, shoulder.ny);
@@ -459,11 +495,22 @@ std::string blunt_body_grid(const Body& body, const BluntGridOptions& o, Grid* o
     return widths[k] + std::min(std::max(f, 0.0), 1.0) * (widths[k + 1] - widths[k]);
   };
   // Angle of the body normal to the upstream axis, odd about the tip.
-  std::function<double(double)> normal_angle = [&](double s) -> double {
-    if (s < 0) return -normal_angle(-s);
-    if (s >= s_nose) return M_PI / 2;
-    const SurfacePoint p = surface(s);
-    return std::atan2(p.ny, -p.nx);
+  auto normal_angle = [&](double s) -> double {
+    const double a = s < 0 ? -s : s;
+    double angle = M_PI / 2;
+    if (a < s_nose) {
+      // The normal (-ty, tx) / |t| makes the angle atan2(tx, ty) with the
+      // upstream axis; atan2 needs no normalised tangent.
+      const double u = u_at(a);
+      if (u == 0) {
+        angle = 0;
+      } else {
+        const double eps = 1e-7;
+        const double ua = std::max(u - eps, 0.0), ub = std::min(u + eps, 1.0);
+        angle = std::atan2(profile_x(ub) - profile_x(ua), profile_r(ub) - profile_r(ua));
+      }
+    }
+    return s < 0 ? -angle : angle;
   };
   // A sharp tip's jump in the normal, fanned out geometrically.
   const double tip_jump = sharp ? normal_angle(s_nose * 1e-9) : 0;
