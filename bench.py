@@ -434,8 +434,7 @@ def run_warmstart(args) -> None:
     the drag difference, and the plain cold single-case solve rate."""
     import torch
 
-    from bowshock_b200.mlp import WarmStartNet
-    from bowshock_b200.warmstart import solve_cases, training_set, warm_solve
+    from bowshock_b200.warmstart import solve_cases, train_on_solves, warm_solve
     from bowshock_b200.workloads import seeded_cases
 
     torch.cuda.set_device(0)
@@ -445,21 +444,8 @@ def run_warmstart(args) -> None:
     held, _ = seeded_cases(args.eval_cases, first_seed=1_000_001, threads=threads, levels=(2,))
     grid_s = time.perf_counter() - t0
 
-    solved = solve_cases(train, max_steps=args.max_steps, keep_fields=True)
-    ok = [k for k, s in enumerate(solved.status) if s == 0]
-    samples, targets = training_set([train[k] for k in ok], [solved.fields[k] for k in ok],
-                                    args.cells_per_case)
-    solved.fields = None
-    net = WarmStartNet(hidden_layers=5, batch=16384, seed=1)
-    net.set_data(samples, targets)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    losses = []
-    # Learning rate: 1e-3, then 3e-4, then 1e-4 over the three thirds.
-    third = max(1, args.train_steps // 3)
-    for phase, lr in enumerate((1e-3, 3e-4, 1e-4)):
-        losses.extend(net.train(third, lr, seed=101 + phase).tolist())
-    train_s = time.perf_counter() - t0
+    tr = train_on_solves(train, args.cells_per_case, args.train_steps, args.max_steps)
+    net = tr.net
 
     cold = solve_cases(held, max_steps=args.max_steps)
     good = [k for k, s in enumerate(cold.status) if s == 0]
@@ -473,12 +459,12 @@ def run_warmstart(args) -> None:
         "metric": "warm-started steady solves/s to RMS density residual 1e-6 (seeded 160x80 batch, LU-SGS CFL 5)",
         "value": sum(1 for s in warm.status if s == 0) / (warm.device_ms / 1000), "unit": UNIT,
         "n_gpus": 1, "higher_is_better": True, "dtype": "f64 solve, bf16/fp32 network", "data": "synthetic",
-        "config": {"workload": f"train on {len(ok)} converged of {len(train)} seeded 160x80 cases "
-                               f"({args.cells_per_case} random cells each, {len(samples)} samples), "
+        "config": {"workload": f"train on {tr.solved} converged of {len(train)} seeded 160x80 cases "
+                               f"({args.cells_per_case} random cells each, {tr.samples} samples), "
                                f"evaluate on {n} held-out seeds", "network": "5 x 256 GELU, Fourier features",
-                   "train_steps": 3 * third, "batch": 16384, "grid_build_s": grid_s},
-        "train": {"solve_device_ms": solved.device_ms, "seconds": train_s,
-                  "loss_first": float(np.mean(losses[:10])), "loss_last": float(np.mean(losses[-10:]))},
+                   "train_steps": tr.steps, "batch": 16384, "grid_build_s": grid_s},
+        "train": {"solve_device_ms": tr.solve_device_ms, "seconds": tr.seconds,
+                  "loss_first": tr.loss_first, "loss_last": tr.loss_last},
         "cold": {"solves_per_s": len(good) / (cold.device_ms / 1000), "device_ms": cold.device_ms,
                  "steps_median": int(statistics.median([cold.steps[k] for k in good])),
                  "steps_total": int(sum(cold.steps[k] for k in good)),
@@ -494,6 +480,125 @@ def run_warmstart(args) -> None:
                                        / (1000.0 / single.device_ms),
     }), flush=True)
     net.destroy()
+
+
+def run_stream(args) -> None:
+    """The combined warm-started stream: the network is trained as in the
+    warm-start workload (`--train-cases` seeded 160x80 solves), then
+    `--geometries` held-out seeded geometries, each at Mach 1.5, 2, 3 and 4
+    on grids ni = 80 2^k (80x40 to 640x320, k drawn per geometry), are
+    solved wave by wave within `--wave-gb` of device memory, each wave
+    warm-started by the network, its grids made on the host while the wave
+    before it solves. `value` counts converged solves per second of solve
+    device time plus prediction wall time; beside it the fraction of warm
+    starts that fell back, the algorithmic HBM rate, the drag error against
+    the FP64 oracle on the `--check` smallest converged cases, and the plain
+    cold single-case solve of one case per grid level."""
+    import torch
+
+    from bowshock_b200.stream import by_grid_size, plan_waves, run_stream as stream
+    from bowshock_b200.warmstart import solve_cases, train_on_solves
+    from bowshock_b200.workloads import seeded_cases, stream_specs
+
+    torch.cuda.set_device(0)
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    train, _ = seeded_cases(args.train_cases, first_seed=1, threads=threads, levels=(2,))
+    train_grid_s = time.perf_counter() - t0
+    tr = train_on_solves(train, args.cells_per_case, args.train_steps, args.max_steps)
+    del train
+
+    specs = stream_specs(args.geometries, first_seed=2_000_001)
+    free_bytes, _ = torch.cuda.mem_get_info()
+    budget = int(min(args.wave_gb * 2**30, 0.6 * free_bytes))
+    levels = sorted({s.ni for s in specs})
+    keep: set[int] = set()
+    per_level: dict[int, int] = {}
+    smallest = 0
+    for k, s in enumerate(specs):
+        if per_level.get(s.ni, 0) < 4:
+            per_level[s.ni] = per_level.get(s.ni, 0) + 1
+            keep.add(k)
+        if s.ni == levels[0] and smallest < 4 * args.check:
+            smallest += 1
+            keep.add(k)
+    clocks = Clocks(0)
+    clocks.start()
+    res = stream(tr.net, specs, budget, threads, args.stream_steps, args.warm_steps, 80, keep)
+    clock_info = clocks.stop()
+    tr.net.destroy()
+
+    made = [k for k, st in enumerate(res.status) if st is not None]
+    converged = [k for k in made if res.status[k] == 0]
+    device_s = sum(w.device_ms for w in res.waves) / 1000
+    predict_s = sum(w.predict_s for w in res.waves)
+    cell_steps = sum(w.cell_steps for w in res.waves)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    hbm = cell_steps * (BYTES_PREPARE + BYTES_SWEEP + BYTES_UPDATE) / device_s / 1e9
+
+    def q(v: list[float], f: float) -> float:
+        return float(np.quantile(np.asarray(v), f)) if v else float("nan")
+
+    by_level = {}
+    for ni in levels:
+        ks = [k for k in made if specs[k].ni == ni]
+        ok = [res.steps[k] for k in ks if res.status[k] == 0]
+        by_level[f"{ni}x{ni // 2}"] = {
+            "cases": len(ks), "converged": len(ok), "fell_back": sum(1 for k in res.fell_back if specs[k].ni == ni),
+            "steps_median": int(statistics.median(ok)) if ok else None, "steps_max": max(ok) if ok else None}
+
+    check = None
+    pick = [k for k in sorted(res.kept) if specs[k].ni == levels[0] and res.status[k] == 0][: args.check]
+    if pick:
+        sec, cpu_drags, _ = cpu_solve([res.kept[k] for k in pick], threads)
+        errs = [abs(res.drags[k] - d) / max(abs(d), 1e-12) for k, d in zip(pick, cpu_drags)]
+        check = {"cases": len(pick), "grid": f"{levels[0]}x{levels[0] // 2}", "median": q(errs, 0.5),
+                 "p90": q(errs, 0.9), "max": max(errs), "oracle_seconds": sec, "oracle_threads": threads}
+
+    single = {}
+    for ni in levels:
+        ks = [k for k in sorted(res.kept) if specs[k].ni == ni and res.status[k] == 0]
+        if ks:
+            one = solve_cases([res.kept[ks[0]]], max_steps=int(args.stream_steps * ni / 80))
+            single[f"{ni}x{ni // 2}"] = {"device_ms": one.device_ms, "steps": one.steps[0],
+                                         "converged": one.status[0] == 0}
+    single_rate = (len(single) / (sum(v["device_ms"] for v in single.values()) / 1000)) if single else None
+    value = len(converged) / (device_s + predict_s)
+    print(json.dumps({
+        "metric": "combined warm-started stream: steady solves/s to RMS density residual 1e-6 "
+                  "(seeded geometries x Mach 1.5/2/3/4, 80x40..640x320, LU-SGS CFL 5)",
+        "value": value, "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+        "dtype": "f64 solve, bf16/fp32 network", "data": "synthetic",
+        "config": {"workload": f"{len(specs)} cases: {args.geometries} seeded geometries (seeds from 2000001) "
+                               "x Mach 1.5, 2, 3, 4; nose conical/tangent ogive/parabolic/ellipsoid/Von Karman, "
+                               "fineness U[1,5], body length U[2,8], ni = 80*2^k (k in 0..3 per geometry), "
+                               f"nj = ni/2; waves smallest grids first; step budgets {args.warm_steps} "
+                               f"(warm start) and {args.stream_steps} (from the free stream) at 80x40, "
+                               "scaled with ni",
+                   "cells_total": sum(s.ni * s.nj for s in specs), "waves": len(plan_waves(specs, budget, by_grid_size(specs))),
+                   "wave_budget_gb": budget / 2**30,
+                   "training": {"cases": args.train_cases, "converged": tr.solved, "samples": tr.samples,
+                                "adam_steps": tr.steps, "seconds": tr.seconds, "loss_last": tr.loss_last,
+                                "grid_build_s": train_grid_s, "solve_device_ms": tr.solve_device_ms}},
+        "gpu_launches": sum(w.launches for w in res.waves),
+        "converged": len(converged), "not_converged": len(made) - len(converged),
+        "refused_by_grid_generator": len(specs) - len(made),
+        "fell_back_fraction": len(res.fell_back) / max(1, len(made)),
+        "solve_device_s": device_s, "predict_wall_s": predict_s,
+        "solves_per_s_solve_only": len(converged) / device_s,
+        "cell_steps": cell_steps,
+        "hbm": {"achieved_gbs": hbm, "peak_gbs": hbm_peak, "frac": hbm / hbm_peak,
+                "bytes_per_cell_step": BYTES_PREPARE + BYTES_SWEEP + BYTES_UPDATE,
+                "peak_source": "measured" if peaks else "fallback"},
+        "by_level": by_level,
+        "cd_rel_err_vs_fp64_oracle": check,
+        "single_case_cold": {"per_level": single, "solves_per_s": single_rate},
+        "stream_over_single_cold": value / single_rate if single_rate else None,
+        "wall_s": res.wall_s, "first_wave_grid_build_s": res.first_build_s,
+        "waves": [w.__dict__ for w in res.waves],
+        "clocks": clock_info,
+    }), flush=True)
 
 
 def run_gemm(args) -> None:
@@ -600,7 +705,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--probe", type=int, default=0,
                     help="run this many LU-SGS steps of the batch with per-kernel timing and exit")
-    ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart", "gemm", "stencil", "verified"], default="drag-curve")
+    ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart", "stream", "gemm", "stencil", "verified"], default="drag-curve")
     ap.add_argument("--train-cases", type=int, default=4096, help="warm start: training seeds")
     ap.add_argument("--eval-cases", type=int, default=512, help="warm start: held-out seeds")
     ap.add_argument("--train-steps", type=int, default=3000, help="warm start: Adam steps")
@@ -609,6 +714,12 @@ def main() -> None:
     ap.add_argument("--stencil-cases", type=int, default=32, help="stencil workload: 640x320 cases")
     ap.add_argument("--band", type=float, default=2e-3, help="verified workload: largest band, absolute")
     ap.add_argument("--max-steps", type=int, default=5000, help="seeded workload: steps per case")
+    ap.add_argument("--geometries", type=int, default=2000, help="stream: seeded geometries (4 Mach numbers each)")
+    ap.add_argument("--wave-gb", type=float, default=48.0, help="stream: device memory per wave")
+    ap.add_argument("--warm-steps", type=int, default=1250,
+                    help="stream: steps before a warm start falls back, at 80x40 (scaled with ni)")
+    ap.add_argument("--stream-steps", type=int, default=2500,
+                    help="stream: steps from the free stream, at 80x40 (scaled with ni)")
     ap.add_argument("--check", type=int, default=16,
                     help="seeded workload: smallest converged cases checked against the FP64 oracle")
     args = ap.parse_args()
@@ -624,6 +735,9 @@ def main() -> None:
         return
     if args.workload == "warmstart":
         run_warmstart(args)
+        return
+    if args.workload == "stream":
+        run_stream(args)
         return
     if args.workload == "gemm":
         run_gemm(args)

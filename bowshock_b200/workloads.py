@@ -171,18 +171,14 @@ def case_from(nc: NoseCase) -> Case:
     return Case(name, cfg, free, body, nc.mach)
 
 
-def seeded_cases(count: int, first_seed: int = 1, threads: int | None = None,
-                 **draw) -> tuple[list[Case], list[NoseCase]]:
-    """`count` consecutive seeds drawn as draw_nose_case, their grids made on
+def make_cases(specs: list[NoseCase], threads: int | None = None) -> list[Case | None]:
+    """The grid and configuration of every spec (case_from), made on
     `threads` host threads (the generator is native code that runs outside
-    the interpreter lock); cases whose grid cannot be made are left out and
-    returned second."""
+    the interpreter lock); None where no grid can be made."""
     import os
     from concurrent.futures import ThreadPoolExecutor
 
     from . import _native
-
-    specs = [draw_nose_case(s, **draw) for s in range(first_seed, first_seed + count)]
 
     def make(nc: NoseCase):
         try:
@@ -191,7 +187,34 @@ def seeded_cases(count: int, first_seed: int = 1, threads: int | None = None,
             return None
 
     with ThreadPoolExecutor(max_workers=threads or os.cpu_count() or 1) as pool:
-        results = list(pool.map(make, specs))
+        return list(pool.map(make, specs))
+
+
+def seeded_cases(count: int, first_seed: int = 1, threads: int | None = None,
+                 **draw) -> tuple[list[Case], list[NoseCase]]:
+    """`count` consecutive seeds drawn as draw_nose_case, their grids made by
+    make_cases; cases whose grid cannot be made are left out and returned
+    second."""
+    specs = [draw_nose_case(s, **draw) for s in range(first_seed, first_seed + count)]
+    results = make_cases(specs, threads)
     made = [c for c in results if c is not None]
     refused = [nc for nc, c in zip(specs, results) if c is None]
     return made, refused
+
+
+STREAM_MACHS = (1.5, 2.0, 3.0, 4.0)
+
+
+def stream_specs(geometries: int, first_seed: int = 1, machs: tuple[float, ...] = STREAM_MACHS,
+                 levels: tuple[int, ...] = (0, 1, 2, 3), base_ni: int = 80) -> list[NoseCase]:
+    """The combined stream's cases: `geometries` seeded nose + body
+    geometries of the batched distribution (draw_nose_case; the grid level
+    is drawn per geometry, ni = base_ni 2^k), each at every Mach number of
+    `machs`, geometry by geometry."""
+    from dataclasses import replace
+
+    out = []
+    for s in range(first_seed, first_seed + geometries):
+        g = draw_nose_case(s, levels=levels, base_ni=base_ni)
+        out.extend(replace(g, mach=m) for m in machs)
+    return out
