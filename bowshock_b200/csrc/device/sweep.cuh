@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(TILE_THREADS) lusgs_update_kernel(const CaseDe
   const int i = (tile.y % tiles_i) * TI + threadIdx.x % TI;
   const int j = (tile.y / tiles_i) * TJ + threadIdx.x / TI;
   bool bad = false;
-  if (i < ni && j < nj) {
+  if (i < ni && j < nj && int(threadIdx.x) < TI * TJ) {
     const R gamma = R(cd.gamma);
     const int64_t k = cd.cell + i + int64_t(j) * ni;
     const Cons<R> q0 = q.load(k);

@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(TILE_THREADS) dt_kernel(const CaseDev* cases, 
   const int tiles_i = (ni + TI - 1) / TI;
   const int i = (tile.y % tiles_i) * TI + threadIdx.x % TI;
   const int j = (tile.y / tiles_i) * TJ + threadIdx.x / TI;
-  if (i >= ni || j >= nj) return;
+  if (i >= ni || j >= nj || int(threadIdx.x) >= TI * TJ) return;
   const R gamma = R(cd.gamma);
   const int64_t k = cd.cell + i + int64_t(j) * ni;
   const Prim<R> w = to_prim(q.load(k), gamma);
