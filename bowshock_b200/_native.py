@@ -85,6 +85,9 @@ SIGNATURES: dict[str, list] = {
     "bs_batch_set_free_stream": [_vp],
     "bs_batch_solve": [_vp, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32,
                        C.c_int32, C.POINTER(abi.SolveResult)],
+    "bs_batch_set_anderson": [_vp, C.c_int32, C.c_int32],
+    "bs_batch_anderson_restarts": [_vp, _ip],
+    "bs_engine_set_anderson": [_vp, C.c_int32, C.c_int32],
     "bs_batch_forebody_drag": [_vp, C.c_int32, C.c_double, C.c_double, C.c_double, _dp],
     "bs_batch_read_primitives": [_vp, C.c_int32, _dp],
     "bs_batch_density_residual_norms": [_vp, _dp],

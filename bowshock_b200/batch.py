@@ -68,6 +68,17 @@ class CudaBatch:
                    1 if relative else 0, max_steps, check_every, out)
         return list(out)
 
+    def set_anderson(self, depth: int, plain_steps: int = 30) -> None:
+        """Anderson acceleration of later LU-SGS solves: `depth` differences
+        kept (0: plain steps), after `plain_steps` plain steps."""
+        self._call("bs_batch_set_anderson", int(depth), int(plain_steps))
+
+    def anderson_restarts(self) -> np.ndarray:
+        """Per case, the times the last solve's acceleration forgot its history."""
+        out = np.zeros(self.n, np.int32)
+        self._call("bs_batch_anderson_restarts", out.ctypes.data_as(C.POINTER(C.c_int32)))
+        return out
+
     def forebody_drag(self, c: int, free: FreeStream, base_radius: float) -> float:
         cd = C.c_double()
         self._call("bs_batch_forebody_drag", c, free.pressure, free.dynamic_pressure,

@@ -316,9 +316,24 @@ static __global__ void __launch_bounds__(512) lusgs_sweep_kernel(const SweepArgs
   if (j == 0) A.cfl[c] = fminf(A.cfl_max[c], A.cfl[c] * A.growth[c]);
 }
 
-// applyImplicitUpdate (src/engine-cpu/euler2d.ts:816-847) for every cell of
-// every active case: Q += alpha dQ with alpha halved until density and
-// pressure stay within a factor of two; flags non-physical results.
+// applyImplicitUpdate (src/engine-cpu/euler2d.ts:816-847) for one cell:
+// Q + alpha dQ with alpha halved until density and pressure stay within a
+// factor of two of Q's.
+template <class R>
+__device__ __forceinline__ Cons<R> implicit_update(const Cons<R>& q0, float4 d4, R gamma) {
+  const R p0 = pressure_of(q0.rho, q0.mu, q0.mv, q0.e, gamma);
+  const R d0 = R(d4.x), d1 = R(d4.y), d2 = R(d4.z), d3 = R(d4.w);
+  R alpha = R(1);
+  for (int tries = 0; tries < 30; tries++) {
+    const R rho1 = q0.rho + alpha * d0;
+    const R p1 = pressure_of(rho1, q0.mu + alpha * d1, q0.mv + alpha * d2, q0.e + alpha * d3, gamma);
+    if (rho1 > R(0.5) * q0.rho && rho1 < R(2) * q0.rho && p1 > R(0.5) * p0 && p1 < R(2) * p0) break;
+    alpha *= R(0.5);
+  }
+  return {q0.rho + alpha * d0, q0.mu + alpha * d1, q0.mv + alpha * d2, q0.e + alpha * d3};
+}
+
+// The update for every cell of every active case; flags non-physical results.
 template <class R>
 __global__ void __launch_bounds__(TILE_THREADS) lusgs_update_kernel(const CaseDev* cases,
                                                                     const int2* tiles,
@@ -338,18 +353,7 @@ __global__ void __launch_bounds__(TILE_THREADS) lusgs_update_kernel(const CaseDe
   if (i < ni && j < nj && int(threadIdx.x) < TI * TJ) {
     const R gamma = R(cd.gamma);
     const int64_t k = cd.cell + i + int64_t(j) * ni;
-    const Cons<R> q0 = q.load(k);
-    const float4 d4 = dq[cd.skew + skew_slot(i, j, nj)];
-    const R p0 = pressure_of(q0.rho, q0.mu, q0.mv, q0.e, gamma);
-    const R d0 = R(d4.x), d1 = R(d4.y), d2 = R(d4.z), d3 = R(d4.w);
-    R alpha = R(1);
-    for (int tries = 0; tries < 30; tries++) {
-      const R rho1 = q0.rho + alpha * d0;
-      const R p1 = pressure_of(rho1, q0.mu + alpha * d1, q0.mv + alpha * d2, q0.e + alpha * d3, gamma);
-      if (rho1 > R(0.5) * q0.rho && rho1 < R(2) * q0.rho && p1 > R(0.5) * p0 && p1 < R(2) * p0) break;
-      alpha *= R(0.5);
-    }
-    const Cons<R> q1{q0.rho + alpha * d0, q0.mu + alpha * d1, q0.mv + alpha * d2, q0.e + alpha * d3};
+    const Cons<R> q1 = implicit_update(q.load(k), dq[cd.skew + skew_slot(i, j, nj)], gamma);
     q.store(k, q1);
     bad = !is_physical(q1, gamma);
   }

@@ -239,6 +239,10 @@ bs_status bs_engine_solve(bs_engine* engine, int32_t method, double cfl, double 
   });
 }
 
+bs_status bs_engine_set_anderson(bs_engine* engine, int32_t depth, int32_t plain_steps) {
+  BS_ENGINE_CALL(engine, { return engine->solver->set_anderson(depth, plain_steps); });
+}
+
 }  // extern "C"
 
 // ---- batches ---------------------------------------------------------------
@@ -356,6 +360,21 @@ bs_status bs_batch_solve(bs_batch* batch, int32_t method, double cfl, double ome
       results[k].initial_residual = r[k].initial_residual;
       results[k].drag = 0;
     }
+    return BS_OK;
+  });
+}
+
+bs_status bs_batch_set_anderson(bs_batch* batch, int32_t depth, int32_t plain_steps) {
+  BS_BATCH_CALL(batch, { return batch->solver->set_anderson(depth, plain_steps); });
+}
+
+bs_status bs_batch_anderson_restarts(bs_batch* batch, int32_t* restarts) {
+  BS_BATCH_CALL(batch, {
+    if (restarts == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+    std::vector<int> r(batch->solver->n_cases());
+    const bs_status s = batch->solver->anderson_restarts(r.data());
+    if (s != BS_OK) return s;
+    for (size_t k = 0; k < r.size(); k++) restarts[k] = int32_t(r[k]);
     return BS_OK;
   });
 }

@@ -8,6 +8,7 @@
 #include <cstring>
 
 #include "common.hpp"
+#include "device/anderson.cuh"
 #include "device/fields.cuh"
 #include "device/sweep.cuh"
 #include "device/tile.cuh"
@@ -102,6 +103,9 @@ struct GraphKey {
 
 constexpr int kMethodExplicit = 0;
 constexpr int kMethodImplicit = 1;
+// LU-SGS steps with Anderson acceleration (graphs of their own; the C ABI's
+// method stays LU-SGS, the acceleration is a setting of the batch).
+constexpr int kMethodAnderson = 2;
 
 // The launch geometry of a group of cases: its tile list, case list, widest
 // case and stream. The whole batch is one lane; a batch of several cases is
@@ -698,6 +702,26 @@ class Solver final : public SolverBase {
     return BS_OK;
   }
 
+  bs_status set_anderson(int depth, int plain_steps) override {
+    if (depth < 0 || depth > bsd::kMaxAndersonDepth || plain_steps < 0)
+      return fail(BS_INVALID_ARGUMENT, "Anderson acceleration keeps 0 to 16 differences after plain_steps >= 0");
+    anderson_depth_ = depth;
+    anderson_plain_ = plain_steps;
+    return BS_OK;
+  }
+
+  bs_status anderson_restarts(int* out) override {
+    if (ac_.p == nullptr) {
+      for (int c = 0; c < n_; c++) out[c] = 0;
+      return BS_OK;
+    }
+    std::vector<bsd::AndersonCase> h(n_);
+    BS_CUDA(cudaMemcpyAsync(h.data(), ac_.p, n_ * sizeof(bsd::AndersonCase), cudaMemcpyDeviceToHost, stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    for (int c = 0; c < n_; c++) out[c] = h[c].restarts;
+    return BS_OK;
+  }
+
   bs_status solve(int method, double cfl, double omega, double tolerance, int relative,
                   int max_steps, int check_every, std::vector<CaseResult>& results) override {
     if (!(tolerance > 0) || max_steps < 0 || check_every < 1)
@@ -708,9 +732,11 @@ class Solver final : public SolverBase {
       BS_TRY(ensure_implicit());
       BS_TRY(set_implicit_params(cfl, omega, 1.0));
       BS_TRY(set_implicit_cfl(cfl));
+      if (anderson_depth_ > 0) BS_TRY(reset_anderson());
     } else {
       BS_TRY(ensure_explicit());
     }
+    const bool accelerate = method == kMethodImplicit && anderson_depth_ > 0;
     results.assign(n_, CaseResult{});
     launches_ = 0;
     BS_CUDA(cudaEventRecord(ev0_, stream_));
@@ -734,7 +760,14 @@ class Solver final : public SolverBase {
     while (done < n_ && step < max_steps) {
       const int chunk = int(std::min<int64_t>(check_every, max_steps - step));
       BS_CUDA(cudaMemsetAsync(norm_.p, 0, n_ * sizeof(double), stream_));
-      BS_TRY(run_steps(method, chunk, true));
+      if (accelerate) {
+        // Plain steps up to anderson_plain_, accelerated ones after.
+        const int plain = int(std::max<int64_t>(0, std::min<int64_t>(chunk, anderson_plain_ - step)));
+        if (plain > 0) BS_TRY(run_steps(kMethodImplicit, plain, plain == chunk));
+        if (chunk > plain) BS_TRY(run_steps(kMethodAnderson, chunk - plain, true));
+      } else {
+        BS_TRY(run_steps(method, chunk, true));
+      }
       step += chunk;
       BS_CUDA(cudaMemcpyAsync(sums.data(), norm_.p, n_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
       BS_CUDA(cudaMemcpyAsync(status.data(), status_.p, n_ * sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
@@ -814,6 +847,42 @@ class Solver final : public SolverBase {
     if (rec_.p != nullptr) return BS_OK;
     BS_CUDA(rec_.alloc(5 * size_t(total_skew_)));
     BS_CUDA(dq_.alloc(total_skew_));
+    return BS_OK;
+  }
+
+  // The acceleration's arrays for the current depth, and a fresh history:
+  // no columns, no previous iterate, |f|^2's smallest value +inf.
+  bs_status reset_anderson() {
+    const int m = anderson_depth_;
+    if (anderson_alloc_depth_ != m) {
+      BS_CUDA(adx_.alloc(size_t(m) * total_cells_));
+      BS_CUDA(adf_.alloc(size_t(m) * total_cells_));
+      BS_CUDA(alastf_.alloc(total_cells_));
+      for (int v = 0; v < 4; v++) BS_CUDA(alastx_[v].alloc(total_cells_));
+      BS_CUDA(ac_.alloc(n_));
+      BS_CUDA(aacc_.alloc(size_t(n_) * (1 + 2 * m)));
+      BS_CUDA(agram_.alloc(size_t(n_) * m * m));
+      BS_CUDA(agamma_.alloc(size_t(n_) * m));
+      anderson_alloc_depth_ = m;
+      // Graphs of accelerated steps hold the old arrays.
+      for (auto it = graphs_.begin(); it != graphs_.end();) {
+        if (it->first.method == kMethodAnderson) {
+          cudaGraphExecDestroy(it->second);
+          graph_launches_.erase(it->first);
+          it = graphs_.erase(it);
+        } else {
+          ++it;
+        }
+      }
+    }
+    bsd::AndersonCase fresh{};
+    fresh.best = HUGE_VAL;
+    std::vector<bsd::AndersonCase> h(n_, fresh);
+    BS_CUDA(cudaMemcpyAsync(ac_.p, h.data(), n_ * sizeof(bsd::AndersonCase), cudaMemcpyHostToDevice, stream_));
+    BS_CUDA(cudaMemsetAsync(aacc_.p, 0, size_t(n_) * (1 + 2 * m) * sizeof(double), stream_));
+    BS_CUDA(cudaMemsetAsync(agram_.p, 0, size_t(n_) * m * m * sizeof(double), stream_));
+    BS_CUDA(cudaMemsetAsync(agamma_.p, 0, size_t(n_) * m * sizeof(double), stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
     return BS_OK;
   }
 
@@ -937,6 +1006,43 @@ class Solver final : public SolverBase {
     return launch_update_on(lane);
   }
 
+  // One LU-SGS step with Anderson acceleration: the residual pass and the
+  // sweeps as for a plain step, then the acceleration's kernels in place of
+  // the update.
+  bs_status record_anderson_step_on(const LaneView& lane, bool norm) {
+    const bsd::StateView<R> q = q_view();
+    BS_TRY(launch_tile_on<bsd::MODE_PREPARE>(lane, q, q, q, 0, 1, false, norm ? norm_.p : nullptr,
+                                             nullptr, false));
+    BS_TRY(launch_sweep_on(lane));
+    bsd::AndersonArgs<R> A{};
+    A.cases = d_cases_.p;
+    A.tiles = lane.tiles;
+    A.case_list = lane.case_list;
+    A.n_cases = lane.n_cases;
+    A.active = d_active_.p;
+    A.q = q;
+    A.last_x = {alastx_[0].p, alastx_[1].p, alastx_[2].p, alastx_[3].p};
+    A.dq = dq_.p;
+    A.last_f = alastf_.p;
+    A.dx = adx_.p;
+    A.df = adf_.p;
+    A.total = total_cells_;
+    A.depth = anderson_depth_;
+    A.ac = ac_.p;
+    A.acc = aacc_.p;
+    A.gram = agram_.p;
+    A.gamma = agamma_.p;
+    A.status = status_.p;
+    bsd::anderson_fnorm_kernel<R><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
+    bsd::anderson_push_kernel<R><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
+    bsd::anderson_solve_kernel<R><<<(lane.n_cases + 63) / 64, 64, 0, lane.stream>>>(A);
+    bsd::anderson_apply_kernel<R><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
+    bsd::anderson_fallback_kernel<R><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
+    launches_ += 5;
+    BS_CUDA(cudaGetLastError());
+    return BS_OK;
+  }
+
   bs_status launch_sweep() { return launch_sweep_on(whole()); }
   bs_status launch_update() { return launch_update_on(whole()); }
 
@@ -970,7 +1076,7 @@ class Solver final : public SolverBase {
     if (lanes_.size() < 2) return false;
     // Forward Euler copies whole arenas and global stepping reduces over the
     // batch: those run as one lane.
-    return method == kMethodImplicit ||
+    return method == kMethodImplicit || method == kMethodAnderson ||
            (!any_global_dt_ && cases_[0].cfg.integrator != BS_FORWARD_EULER);
   }
 
@@ -980,6 +1086,8 @@ class Solver final : public SolverBase {
         const bool norm = norm_last && s == count - 1;
         if (method == kMethodExplicit)
           BS_TRY(record_explicit_step(norm));
+        else if (method == kMethodAnderson)
+          BS_TRY(record_anderson_step_on(whole(), norm));
         else
           BS_TRY(record_implicit_step(norm));
       }
@@ -994,6 +1102,8 @@ class Solver final : public SolverBase {
         const bool norm = norm_last && s == count - 1;
         if (method == kMethodExplicit)
           BS_TRY(record_explicit_step_on(lane, norm));
+        else if (method == kMethodAnderson)
+          BS_TRY(record_anderson_step_on(lane, norm));
         else
           BS_TRY(record_implicit_step_on(lane, norm));
       }
@@ -1120,6 +1230,12 @@ class Solver final : public SolverBase {
   int64_t launches_ = 0;
   double last_solve_ms_ = 0;
   int64_t last_solve_launches_ = 0;
+  // Anderson acceleration: settings and its per-case history.
+  int anderson_depth_ = 0, anderson_plain_ = 30, anderson_alloc_depth_ = 0;
+  DevBuf<float4> adx_, adf_, alastf_;
+  DevBuf<R> alastx_[4];
+  DevBuf<bsd::AndersonCase> ac_;
+  DevBuf<double> aacc_, agram_, agamma_;
 };
 
 }  // namespace

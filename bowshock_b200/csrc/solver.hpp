@@ -76,6 +76,11 @@ class SolverBase {
   virtual double last_solve_ms() const = 0;
   // Kernel launches made by the last solve.
   virtual int64_t last_solve_launches() const = 0;
+  // Anderson acceleration of the LU-SGS steps of later solves: `depth`
+  // differences kept (0: plain steps), after `plain_steps` plain steps.
+  virtual bs_status set_anderson(int depth, int plain_steps) = 0;
+  // Per case, the times the last solve's acceleration forgot its history.
+  virtual bs_status anderson_restarts(int* out) = 0;
 };
 
 // precision: 64 (FP64 state and residual, FP32 LU-SGS operator) or 32 (all FP32).

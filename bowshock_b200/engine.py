@@ -178,6 +178,12 @@ class CudaEuler2D:
             self.set_implicit_cfl(cfl)
         self._call("bs_engine_iterate_implicit", int(count), float(cfl), float(omega), float(growth))
 
+    def set_anderson(self, depth: int, plain_steps: int = 30) -> None:
+        """Anderson acceleration of later LU-SGS solves (AndersonMixing,
+        src/solver/anderson.ts): `depth` differences kept, 0 for plain steps,
+        after `plain_steps` plain steps."""
+        self._call("bs_engine_set_anderson", int(depth), int(plain_steps))
+
     def solve(self, method: str = "lusgs", tolerance: float = 1e-6, relative: bool = False,
               max_steps: int = 100000, check_every: int = 20, cfl: float = 5.0,
               omega: float = 1.5) -> abi.SolveResult:

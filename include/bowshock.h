@@ -260,6 +260,8 @@ BS_API bs_status bs_engine_steps(bs_engine *engine, int64_t *steps);
 BS_API bs_status bs_engine_solve(bs_engine *engine, int32_t method, double cfl, double omega,
                           double tolerance, int32_t relative, int32_t max_steps,
                           int32_t check_every, bs_solve_result *result);
+/* As bs_batch_set_anderson, for the engine's later bs_engine_solve calls. */
+BS_API bs_status bs_engine_set_anderson(bs_engine *engine, int32_t depth, int32_t plain_steps);
 
 /* ---- an LU-SGS step that allocates nothing -------------------------------- */
 
@@ -332,6 +334,20 @@ BS_API bs_status bs_batch_flow_field(bs_batch *batch, int32_t c, int32_t field, 
 BS_API bs_status bs_batch_solve(bs_batch *batch, int32_t method, double cfl, double omega,
                                 double tolerance, int32_t relative, int32_t max_steps,
                                 int32_t check_every, bs_solve_result *results);
+
+/* Anderson acceleration of the LU-SGS steps of later bs_batch_solve calls
+ * (method 1): after `plain_steps` plain steps, x <- x + f - (dX + dF) gamma
+ * with the last `depth` differences of the iterates and of their LU-SGS
+ * corrections f, gamma minimising |f - dF gamma| (AndersonMixing,
+ * src/solver/anderson.ts:20-123, applied as src/analysis/transonic-flow.ts:
+ * 183-206 applies it: the history is forgotten after a non-physical
+ * accelerated state, which is replaced by the plain update, and when |f|^2
+ * exceeds 100 times its smallest value since the last restart). depth 0 (the
+ * default) keeps plain steps; at most 16. The steady state, and the residual
+ * test that stops a case, are those of the plain steps. */
+BS_API bs_status bs_batch_set_anderson(bs_batch *batch, int32_t depth, int32_t plain_steps);
+/* Per case, the times the last solve's acceleration forgot its history. */
+BS_API bs_status bs_batch_anderson_restarts(bs_batch *batch, int32_t *restarts);
 
 /* As bs_engine_forebody_drag, for case `c`. */
 BS_API bs_status bs_batch_forebody_drag(bs_batch *batch, int32_t c, double p_inf, double q_inf,

@@ -81,6 +81,31 @@ def main() -> None:
         "mach": 2.0, "nj": 12, "explicit_steps": 6000, "residual_below": 1e-12,
         "drag_equal_within": 1e-12,
     }
+    # Anderson acceleration (src/solver/anderson.ts): its own known answers,
+    # and the accelerated LU-SGS steps on the same cone.
+    plain = re.search(r"new AndersonMixing\(3, (\d+)\);\s*const x = Float64Array\.from\(\[([^\]]*)\]\);"
+                      r"\s*const f = Float64Array\.from\(\[([^\]]*)\]\);\s*"
+                      r"expect\(Array\.from\(a\.next\(x, f\)\)\)\.toEqual\(\[([^\]]*)\]\)", t)
+    linear = re.search(r"const n = (\d+);\s*const diag = .*?1 / \(1 \+ \((\d+) \* k\) / \(n - 1\)\)\).*?"
+                       r"new AndersonMixing\(n, (\d+)\);\s*for \(let k = 0; k < (\d+); k\+\+\).*?"
+                       r"toBeLessThan\(([0-9e.-]+) \* error.*?toBeGreaterThan\(([0-9.]+) \* error", t, re.S)
+    lusgs = re.search(r"s\.iterateImplicit\((\d+), (\d+)\);\s*const n = 4 \* grid\.ni \* grid\.nj;\s*"
+                      r"const anderson = new AndersonMixing\(n, (\d+)\);\s*for \(let k = 0; k < (\d+) .*?"
+                      r"implicitCorrection\((\d+)\)", t, re.S)
+    nums = lambda g: [float(v) for v in g.split(",")]
+    out["anderson"] = {
+        "source": f"{f}:{find_line(t, 'without history takes the plain step')}",
+        "plain_step": {"depth": int(plain.group(1)), "x": nums(plain.group(2)), "f": nums(plain.group(3)),
+                       "next": nums(plain.group(4))},
+        "linear": {"n": int(linear.group(1)), "stiffness": int(linear.group(2)), "depth": int(linear.group(3)),
+                   "steps": int(linear.group(4)), "accelerated_below": float(linear.group(5)),
+                   "plain_above": float(linear.group(6)),
+                   "correction": "(b - diag x) / 4, diag_k = 1 / (1 + stiffness k / (n - 1)), b_k = sin(k + 1)"},
+        "lusgs": {"source": f"{f}:{find_line(t, 'Anderson-accelerated LU-SGS gives the same drag')}",
+                  "plain_steps": int(lusgs.group(1)), "plain_cfl": float(lusgs.group(2)),
+                  "depth": int(lusgs.group(3)), "max_steps": int(lusgs.group(4)), "cfl": float(lusgs.group(5)),
+                  "residual_below": 1e-12, "drag_equal_within": 1e-12},
+    }
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {OUT}")
 

@@ -1,0 +1,123 @@
+"""Anderson-accelerated LU-SGS on the GPU (bs_batch_set_anderson,
+bs_engine_set_anderson): the reference's own accelerated case reaches the
+explicit scheme's drag; cases where plain LU-SGS settles into a cycle
+converge, to the drag of the oracle's accelerated steps (oracle/anderson.py,
+the restatement of src/solver/anderson.ts); accelerated solves keep the
+plain solves' drags and take the oracle's number of steps."""
+from __future__ import annotations
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from bowshock_b200.batch import CudaBatch
+from bowshock_b200.engine import CudaEuler2D
+from bowshock_b200.workloads import case_from, draw_nose_case, ogive_case
+from oracle.anderson import AndersonMixing
+from oracle.oracle import OracleEuler2D
+from test_oracle_golden import implicit_case
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "reference_known_answers.json").read_text())["anderson"]
+
+
+def test_accelerated_lusgs_reaches_the_explicit_drag():
+    # tests/engine-cpu/implicit.test.ts:285-298: 30 LU-SGS steps at CFL 10,
+    # then accelerated steps (depth 8) at CFL 1000. The GPU's FP32 operator
+    # takes the residual to 1e-10 here (as its plain LU-SGS does), not 1e-12.
+    g, cfg, free = implicit_case()
+    ga = GOLDEN["lusgs"]
+    explicit = OracleEuler2D(cfg)
+    explicit.set_uniform(free.state)
+    explicit.iterate(g["explicit_steps"])
+    cd_ref = explicit.forebody_drag(free.pressure, free.dynamic_pressure, 0.5)
+    with CudaEuler2D(cfg, 64) as e:
+        e.set_uniform(free.state)
+        e.iterate_implicit(ga["plain_steps"], ga["plain_cfl"])
+        e.set_anderson(ga["depth"], 0)
+        r = e.solve("lusgs", 1e-10, max_steps=ga["max_steps"], check_every=10, cfl=ga["cfl"])
+        cd = e.forebody_drag(free, 0.5)
+    assert r.status == 0 and r.residual < 1e-10
+    assert abs(cd / cd_ref - 1) < 1e-7
+
+
+def _oracle_anderson_run(case, depth=8, cfl=5.0, tol=1e-8, max_steps=4000, plain_steps=30):
+    """The oracle's LU-SGS steps accelerated by oracle.anderson, applied as
+    src/analysis/transonic-flow.ts:183-206 applies it; returns the oracle
+    and the steps taken."""
+    o = OracleEuler2D(case.config)
+    o.set_uniform(case.free.state)
+    a = AndersonMixing(4 * o.n_cells, depth)
+    best, c, n = np.inf, 1.0, 0
+    while n < max_steps:
+        if n < plain_steps:
+            o.iterate_implicit(1, cfl)
+        else:
+            x = o.conserved()
+            f = o.implicit_correction(cfl)
+            nf = float(f @ f)
+            if nf > 100 * best:
+                a.reset()
+                best = nf
+            best = min(best, nf)
+            o.set_conserved(a.next(x, f))
+        n += 1
+        if n % 20 == 0 and o.density_residual_norm() <= tol:
+            break
+    return o, n
+
+
+def _oracle_anderson(case):
+    o, _ = _oracle_anderson_run(case)
+    f = case.free
+    return o.density_residual_norm(), o.forebody_drag(f.pressure, f.dynamic_pressure, case.body.nose.base_radius)
+
+
+def _oracle_anderson_steps(case):
+    return _oracle_anderson_run(case)[1]
+
+
+@pytest.mark.parametrize("seed", [236, 772])
+def test_cases_that_cycle_under_plain_steps_converge(seed):
+    # Ellipsoid noses above Mach 4 on 40 x 20 cells: plain LU-SGS settles
+    # into a cycle (residual 0.3-0.5 after thousands of steps, the oracle's
+    # too); accelerated, they converge.
+    case = case_from(draw_nose_case(seed, levels=(0,)))
+    with CudaBatch([case.config], precision=64) as b:
+        b.set_free_stream()
+        plain = b.solve("lusgs", 1e-6, max_steps=3000, cfl=5.0)[0]
+        b.set_free_stream()
+        b.set_anderson(8, 30)
+        acc = b.solve("lusgs", 1e-8, max_steps=4000, cfl=5.0)[0]
+        cd = b.forebody_drag(0, case.free, case.body.nose.base_radius)
+        restarts = b.anderson_restarts()
+    assert plain.status != 0 and plain.residual > 1e-3
+    assert acc.status == 0 and acc.residual < 1e-8
+    assert restarts.shape == (1,) and restarts[0] >= 0
+    r_oracle, cd_oracle = _oracle_anderson(case)
+    assert r_oracle < 1e-8
+    assert abs(cd / cd_oracle - 1) < 1e-6
+
+
+@pytest.mark.parametrize("mach", [1.5, 2.5])
+def test_accelerated_steps_follow_the_oracle_and_keep_the_drag(mach):
+    # The tangent ogive of the drag curve on 80 x 40 cells, LU-SGS at CFL 5
+    # to 1e-8. Acceleration shortens the Mach 1.5 solve and lengthens the
+    # Mach 2.5 one, on the GPU as with the oracle's FP64 restatement of the
+    # reference's algorithm; the step counts agree, and so do the drags of
+    # the plain and the accelerated solve.
+    case = ogive_case(mach, 80, 40)
+    runs = {}
+    for depth in (0, 8):
+        with CudaBatch([case.config], precision=64) as b:
+            b.set_free_stream()
+            b.set_anderson(depth, 30)
+            r = b.solve("lusgs", 1e-8, max_steps=4000, cfl=5.0)[0]
+            runs[depth] = (r.status, r.steps, b.forebody_drag(0, case.free, 0.5))
+    assert runs[0][0] == 0 and runs[8][0] == 0
+    assert abs(runs[8][2] / runs[0][2] - 1) < 1e-7
+    steps_oracle = _oracle_anderson_steps(case)
+    assert abs(runs[8][1] - steps_oracle) <= 0.15 * steps_oracle + 20
