@@ -33,11 +33,14 @@ class BatchSolve:
 
 
 def solve_cases(cases, starts: list[np.ndarray] | None = None, max_steps: int = 5000,
-                keep_fields: bool = False, tolerance: float = TOLERANCE) -> BatchSolve:
+                keep_fields: bool = False, tolerance: float = TOLERANCE, anderson: int = 0) -> BatchSolve:
     """All `cases` in one batch by LU-SGS CFL 5 to RMS d(rho)/dt <= `tolerance`
-    (1e-6), from the free stream or from `starts` (primitives per case)."""
+    (1e-6), from the free stream or from `starts` (primitives per case);
+    `anderson` > 0 accelerates the steps with that many differences."""
     batch = CudaBatch([c.config for c in cases], precision=64)
     try:
+        if anderson:
+            batch.set_anderson(anderson, 30)
         if starts is None:
             batch.set_free_stream()
         else:
@@ -112,12 +115,14 @@ def predicted_starts(net: WarmStartNet, cases) -> list[np.ndarray]:
 
 
 def warm_solve(net: WarmStartNet, cases, max_steps: int = 5000, warm_steps: int = 2500,
-               tolerance: float = TOLERANCE) -> tuple[BatchSolve, list[int]]:
+               tolerance: float = TOLERANCE, fallback_anderson: int = 0) -> tuple[BatchSolve, list[int]]:
     """Warm-started batch; cases whose warm start fails (non-physical, or not
     converged within `warm_steps`, about three times a typical cold solve
     here) are solved again from the free stream within `max_steps` (their
-    steps and time are added). Returns the combined result and the indices
-    that fell back."""
+    steps and time are added), by plain LU-SGS steps or, with
+    `fallback_anderson` > 0, Anderson-accelerated ones (which converge the
+    cases whose plain steps settle into a cycle but slow most others).
+    Returns the combined result and the indices that fell back."""
     t0 = time.perf_counter()
     starts = predicted_starts(net, cases)
     predict_s = time.perf_counter() - t0
@@ -126,7 +131,8 @@ def warm_solve(net: WarmStartNet, cases, max_steps: int = 5000, warm_steps: int 
     warm.predict_s = predict_s
     failed = [k for k, s in enumerate(warm.status) if s != 0]
     if failed:
-        cold = solve_cases([cases[k] for k in failed], max_steps=max_steps, tolerance=tolerance)
+        cold = solve_cases([cases[k] for k in failed], max_steps=max_steps, tolerance=tolerance,
+                           anderson=fallback_anderson)
         for j, k in enumerate(failed):
             warm.status[k] = cold.status[j]
             warm.steps[k] += cold.steps[j]
