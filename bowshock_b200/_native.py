@@ -108,6 +108,14 @@ SIGNATURES: dict[str, list] = {
                           C.POINTER(abi.ConeFlow)],
     "bs_oblique_shock": [C.c_double, C.c_double, C.c_double, C.POINTER(abi.Shock)],
     "bs_normal_shock": [C.c_double, C.c_double, C.POINTER(abi.Shock)],
+    "bs_cone_flow_field": [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32, _dp, _dp, _dp,
+                           C.POINTER(abi.ConeFlow)],
+    "bs_shock_state": [C.POINTER(abi.Primitive), C.c_double, C.c_double, C.c_double, C.c_double,
+                       C.POINTER(abi.FittedShock)],
+    "bs_compatible_shock": [C.POINTER(abi.Primitive), C.c_double, C.c_double, C.c_double, C.c_double,
+                            C.c_double, C.c_double, C.c_double, C.POINTER(abi.FittedShock)],
+    "bs_column_positions": [C.c_int32, _dp, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, _dp,
+                            _ip],
     "bs_batch_iterate": [_vp, C.c_int32],
     "bs_batch_flow_field": [_vp, C.c_int32, C.c_int32, C.POINTER(abi.Primitive), C.c_double, _dp],
     "bs_batch_set_active": [_vp, _ip],

@@ -136,6 +136,15 @@ class ConeFlow(C.Structure):
     ]
 
 
+class FittedShock(C.Structure):
+    _fields_ = [
+        ("state", Primitive),
+        ("speed", C.c_double),
+        ("normal_velocity", C.c_double),
+        ("mach", C.c_double),
+    ]
+
+
 class Shock(C.Structure):
     _fields_ = [
         ("beta", C.c_double),

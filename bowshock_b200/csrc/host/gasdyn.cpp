@@ -5,6 +5,8 @@
 // angle match the reference's.
 #include "gasdyn.hpp"
 
+#include <functional>
+
 #include <algorithm>
 #include <cmath>
 #include <limits>
@@ -117,7 +119,8 @@ void rk4(double theta, double vr, double vt, double h, double gamma, double* r, 
 // vanishes (integrateToCone, taylor-maccoll.ts:78-145). Returns false if no
 // cone corresponds to this shock.
 bool integrate_to_cone(double mach, double beta, double gamma, double tol, double* cone,
-                       double* surface_speed) {
+                       double* surface_speed,
+                       const std::function<void(double, double, double)>& record = nullptr) {
   NormalShock ns;
   if (!normal_shock(mach * std::sin(beta), gamma, &ns).empty()) return false;
   const double delta = deflection_angle(mach, beta, gamma);
@@ -127,6 +130,7 @@ bool integrate_to_cone(double mach, double beta, double gamma, double tol, doubl
   double vt = -speed * std::sin(beta - delta);
   double theta = beta;
   double h = -1e-4 * beta;
+  if (record) record(theta, vr, vt);
   while (theta > 1e-12) {
     h = std::max(h, -0.5 * theta);
     double fr, ft, hr, ht, r2, t2;
@@ -149,11 +153,13 @@ bool integrate_to_cone(double mach, double beta, double gamma, double tol, doubl
       const double f = vt / (vt - nextT);
       *cone = theta + f * h;
       *surface_speed = vr + f * (nextR - vr);
+      if (record) record(*cone, *surface_speed, 0);
       return true;
     }
     theta += h;
     vr = nextR;
     vt = nextT;
+    if (record) record(theta, vr, vt);
     h *= std::min(2.0, 0.9 * std::pow(tol / std::max(err, 1e-300), 0.2));
   }
   return false;
@@ -207,6 +213,94 @@ std::string taylor_maccoll(double mach, double cone, double gamma, double tol, C
   out->surface_pressure_coefficient =
       (out->surface_pressure_ratio - 1) / (0.5 * gamma * mach * mach);
   return "";
+}
+
+std::string cone_flow_field(double mach, double cone, double gamma, double tol, ConeField* out) {
+  std::string e = taylor_maccoll(mach, cone, gamma, tol, &out->flow);
+  if (!e.empty()) return e;
+  out->theta.clear();
+  out->vr.clear();
+  out->vt.clear();
+  double c, speed;
+  if (!integrate_to_cone(mach, out->flow.shock_angle, gamma, tol, &c, &speed,
+                         [&](double t, double r, double v) {
+                           out->theta.push_back(t);
+                           out->vr.push_back(r);
+                           out->vt.push_back(v);
+                         }))
+    return "integration failed to reach the cone";
+  // V_theta' at each sample for the Hermite interpolant of V_theta.
+  out->vtt.resize(out->theta.size());
+  for (size_t k = 0; k < out->theta.size(); k++) {
+    double dr;
+    tm_derivatives(out->theta[k], out->vr[k], out->vt[k], gamma, &dr, &out->vtt[k]);
+  }
+  out->lowest = std::min(out->theta.back(), cone);
+  return "";
+}
+
+std::string ConeField::at(double ray, double* speed, double* flow_angle) const {
+  const size_t n = theta.size();
+  if (!(ray <= theta[0] + 1e-15 && ray >= lowest - 1e-15)) return "the ray lies outside the conical flow";
+  const double polar = std::min(std::max(ray, theta[n - 1]), theta[0]);
+  size_t k = 0;
+  while (k < n - 2 && theta[k + 1] > polar) k++;
+  const double h = theta[k + 1] - theta[k];
+  const double t = (polar - theta[k]) / h;
+  auto hermite = [&](double f0, double f1, double d0, double d1) {
+    return (2 * t * t * t - 3 * t * t + 1) * f0 + (t * t * t - 2 * t * t + t) * h * d0 +
+           (-2 * t * t * t + 3 * t * t) * f1 + (t * t * t - t * t) * h * d1;
+  };
+  const double r = hermite(vr[k], vr[k + 1], vt[k], vt[k + 1]);
+  const double v = hermite(vt[k], vt[k + 1], vtt[k], vtt[k + 1]);
+  *speed = std::hypot(r, v);
+  *flow_angle = polar + std::atan2(v, r);
+  return "";
+}
+
+ShockState shock_state(const double free[4], double gamma, double mach, double nx, double ny) {
+  const double a = std::sqrt(gamma * free[3] / free[0]);
+  const double vn = free[1] * nx + free[2] * ny;
+  const double speed = mach * a + vn;
+  const double m2 = mach * mach;
+  const double density_ratio = ((gamma + 1) * m2) / ((gamma - 1) * m2 + 2);
+  const double pressure_ratio = 1 + ((2 * gamma) / (gamma + 1)) * (m2 - 1);
+  // The relative normal speed is M a ahead of the shock and M a over the
+  // density ratio behind it; behind it in the lab frame, along n:
+  const double normal_velocity = speed - (mach * a) / density_ratio;
+  ShockState s;
+  s.w[0] = free[0] * density_ratio;
+  s.w[1] = free[1] + (normal_velocity - vn) * nx;
+  s.w[2] = free[2] + (normal_velocity - vn) * ny;
+  s.w[3] = free[3] * pressure_ratio;
+  s.speed = speed;
+  s.normal_velocity = normal_velocity;
+  s.mach = mach;
+  return s;
+}
+
+ShockState compatible_shock(const double free[4], double gamma, double nx, double ny, double rho,
+                            double a, double p, double un) {
+  const double impedance = rho * a;
+  const double target = p + impedance * un;
+  auto mismatch = [&](double m) {
+    const ShockState s = shock_state(free, gamma, m, nx, ny);
+    return s.w[3] + impedance * s.normal_velocity - target;
+  };
+  double mach = 1;
+  if (mismatch(1) < 0) {
+    double low = 1, high = 2;
+    while (mismatch(high) < 0) high *= 2;
+    for (int k = 0; k < 100 && high - low > 1e-15 * high; k++) {
+      const double mid = 0.5 * (low + high);
+      if (mismatch(mid) < 0)
+        low = mid;
+      else
+        high = mid;
+    }
+    mach = 0.5 * (low + high);
+  }
+  return shock_state(free, gamma, mach, nx, ny);
 }
 
 }  // namespace bs

@@ -166,4 +166,68 @@ bs_status bs_normal_shock(double mach, double gamma, bs_shock* out) {
   return bs::ok();
 }
 
+bs_status bs_cone_flow_field(double mach, double cone_angle, double gamma, double tolerance, int32_t n,
+                             const double* polar, double* speed, double* flow_angle, bs_cone_flow* flow) {
+  if (n < 0 || (n > 0 && (polar == nullptr || speed == nullptr || flow_angle == nullptr)))
+    return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  bs::ConeField f;
+  std::string e = bs::cone_flow_field(mach, cone_angle, gamma, tolerance > 0 ? tolerance : 1e-13, &f);
+  if (!e.empty()) return bs::fail(BS_INVALID_ARGUMENT, e);
+  for (int32_t k = 0; k < n; k++) {
+    e = f.at(polar[k], &speed[k], &flow_angle[k]);
+    if (!e.empty()) return bs::fail(BS_INVALID_ARGUMENT, e);
+  }
+  if (flow != nullptr) {
+    flow->shock_angle = f.flow.shock_angle;
+    flow->post_shock_mach = f.flow.post_shock_mach;
+    flow->post_shock_pressure_ratio = f.flow.post_shock_pressure_ratio;
+    flow->surface_mach = f.flow.surface_mach;
+    flow->surface_pressure_ratio = f.flow.surface_pressure_ratio;
+    flow->surface_pressure_coefficient = f.flow.surface_pressure_coefficient;
+  }
+  return bs::ok();
+}
+
+static void to_fitted(const bs::ShockState& s, bs_fitted_shock* out) {
+  out->state.rho = s.w[0];
+  out->state.u = s.w[1];
+  out->state.v = s.w[2];
+  out->state.p = s.w[3];
+  out->speed = s.speed;
+  out->normal_velocity = s.normal_velocity;
+  out->mach = s.mach;
+}
+
+bs_status bs_shock_state(const bs_primitive* free, double gamma, double mach, double nx, double ny,
+                         bs_fitted_shock* out) {
+  if (free == nullptr || out == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  if (!(mach >= 1)) return bs::fail(BS_INVALID_ARGUMENT, "a shock needs a relative Mach number of at least 1");
+  const double f[4] = {free->rho, free->u, free->v, free->p};
+  to_fitted(bs::shock_state(f, gamma, mach, nx, ny), out);
+  return bs::ok();
+}
+
+bs_status bs_compatible_shock(const bs_primitive* free, double gamma, double nx, double ny, double rho, double a,
+                              double p, double un, bs_fitted_shock* out) {
+  if (free == nullptr || out == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  if (!(rho > 0 && a > 0)) return bs::fail(BS_INVALID_ARGUMENT, "the flow behind needs rho > 0 and a > 0");
+  const double f[4] = {free->rho, free->u, free->v, free->p};
+  to_fitted(bs::compatible_shock(f, gamma, nx, ny, rho, a, p, un), out);
+  return bs::ok();
+}
+
+bs_status bs_column_positions(int32_t n_breakpoints, const double* breakpoints, bs_density_fn density, void* user,
+                              int32_t refinement, int32_t total, int32_t capacity, double* out, int32_t* n_out) {
+  if (n_breakpoints < 2 || breakpoints == nullptr || density == nullptr || out == nullptr || n_out == nullptr)
+    return bs::fail(BS_INVALID_ARGUMENT, "column positions need two breakpoints, a density and an output");
+  if (!(refinement >= 1)) return bs::fail(BS_INVALID_ARGUMENT, "the refinement must be at least 1");
+  const std::vector<double> bp(breakpoints, breakpoints + n_breakpoints);
+  const std::vector<double> xs =
+      bs::column_positions(bp, [&](double x) { return density(x, user); }, refinement, total);
+  if (int64_t(xs.size()) > capacity) return bs::fail(BS_INVALID_ARGUMENT, "more positions than the output holds");
+  for (size_t k = 0; k < xs.size(); k++) out[k] = xs[k];
+  *n_out = int32_t(xs.size());
+  return bs::ok();
+}
+
 }  // extern "C"

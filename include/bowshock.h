@@ -461,6 +461,40 @@ typedef struct bs_shock {
 BS_API bs_status bs_oblique_shock(double mach, double theta, double gamma, bs_shock *out);
 BS_API bs_status bs_normal_shock(double mach, double gamma, bs_shock *out);
 
+/* The Taylor-Maccoll flow on rays between the cone and its shock
+ * (coneFlowField, src/validation/taylor-maccoll.ts:227-275): for each of the
+ * n polar angles, the speed over the maximum speed and the flow angle; the
+ * cone solution itself in *flow. BS_INVALID_ARGUMENT if a ray lies outside
+ * the conical flow or the shock detaches. */
+BS_API bs_status bs_cone_flow_field(double mach, double cone_angle, double gamma, double tolerance,
+                                    int32_t n, const double *polar, double *speed, double *flow_angle,
+                                    bs_cone_flow *flow);
+
+/* The state behind a shock of outward normal (nx, ny) met by the free stream
+ * at relative normal Mach number `mach`, the shock's speed along the normal
+ * and the post-shock normal velocity (shockState,
+ * src/solver/shock-fitting.ts:50-78). */
+typedef struct bs_fitted_shock {
+  bs_primitive state;
+  double speed, normal_velocity, mach;
+} bs_fitted_shock;
+BS_API bs_status bs_shock_state(const bs_primitive *free, double gamma, double mach, double nx, double ny,
+                                bs_fitted_shock *out);
+/* The shock consistent with the flow behind it (compatibleShock,
+ * src/solver/shock-fitting.ts:87-111): behind-state density, sound speed,
+ * pressure and normal velocity extrapolated to the face. */
+BS_API bs_status bs_compatible_shock(const bs_primitive *free, double gamma, double nx, double ny, double rho,
+                                     double a, double p, double un, bs_fitted_shock *out);
+
+/* Node positions along a line of breakpoints by an integrated density
+ * (columnPositions, src/grid/spacing.ts:31-71): `total` > 0 asks for exactly
+ * that many intervals. Writes at most `capacity` positions, their count in
+ * *n_out (BS_INVALID_ARGUMENT if more are needed). */
+typedef double (*bs_density_fn)(double x, void *user);
+BS_API bs_status bs_column_positions(int32_t n_breakpoints, const double *breakpoints, bs_density_fn density,
+                                     void *user, int32_t refinement, int32_t total, int32_t capacity,
+                                     double *out, int32_t *n_out);
+
 /* Autotuning of a batch (no counterpart in the reference): times `steps`
  * steps of `method` (0 explicit, 1 LU-SGS with cfl, omega) from the current
  * state with 1, 2, 4, ... up to 64 lanes (concurrent groups of cases, each on

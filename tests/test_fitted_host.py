@@ -1,0 +1,115 @@
+"""Host pieces of the fitted bow shock against the reference's own tests
+(tests/solver/shock-fitting.test.ts:9-121): the Rankine-Hugoniot state
+behind a fitted shock, the shock compatible with the flow behind it, and
+the Taylor-Maccoll field on rays that starts a fit on a sharp nose."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from bowshock_b200.config import Primitive2D
+from bowshock_b200.fitted import column_positions, compatible_shock, cone_flow_field, shock_state
+from bowshock_b200.grid import normal_shock, oblique_shock
+
+GAMMA = 1.4
+DEG = math.pi / 180
+
+
+def free_at(mach: float) -> Primitive2D:
+    return Primitive2D(1.0, mach * math.sqrt(GAMMA), 0.0, 1.0)
+
+
+@pytest.mark.parametrize("mach", [1.2, 2, 3, 5])
+def test_a_normal_shock_at_the_free_stream_mach_stands_still(mach):
+    s = shock_state(free_at(mach), GAMMA, mach, -1.0, 0.0)
+    exact = normal_shock(mach, GAMMA)
+    assert abs(s.speed) < 1e-13
+    assert abs(s.state.p - exact.pressure_ratio) < 1e-12
+    assert abs(s.state.rho - exact.density_ratio) < 1e-12
+    a2 = math.sqrt(GAMMA * s.state.p / s.state.rho)
+    assert abs(math.hypot(s.state.u, s.state.v) / a2 - exact.downstream_mach) < 1e-12
+
+
+@pytest.mark.parametrize("mach,theta", [(2, 10), (3, 20), (5, 8)])
+def test_an_oblique_shock_at_the_wave_angle_turns_the_flow_by_the_wedge(mach, theta):
+    exact = oblique_shock(mach, theta * DEG, GAMMA)
+    b = exact.beta
+    s = shock_state(free_at(mach), GAMMA, mach * math.sin(b), -math.sin(b), math.cos(b))
+    assert abs(s.speed) < 1e-13
+    assert abs(s.state.p - exact.pressure_ratio) < 1e-12
+    assert abs(math.atan2(s.state.v, s.state.u) - theta * DEG) < 1e-12
+
+
+def test_fluxes_are_continuous_across_the_shock_in_its_own_frame():
+    rng = np.random.default_rng(71)
+    for _ in range(300):
+        mach_free, mach_rel, angle = rng.uniform(1.05, 6), rng.uniform(1, 4), rng.uniform(0, 2 * math.pi)
+        free = free_at(mach_free)
+        nx, ny = math.cos(angle), math.sin(angle)
+        s = shock_state(free, GAMMA, mach_rel, nx, ny)
+
+        def flux(w):
+            un = w.u * nx + w.v * ny - s.speed
+            ut = -w.u * ny + w.v * nx
+            h = GAMMA / (GAMMA - 1) * w.p / w.rho + 0.5 * (un * un + ut * ut)
+            return [w.rho * un, w.rho * un * un + w.p, w.rho * un * ut, w.rho * un * h]
+
+        before, after = flux(free), flux(s.state)
+        scale = [before[0], before[1], abs(before[0]) * 10 + 1, abs(before[3])]
+        for k in range(4):
+            assert abs(after[k] - before[k]) < 1e-12 * max(abs(scale[k]), 1)
+
+
+def _behind(w, p=None):
+    return dict(rho=w.rho, a=math.sqrt(GAMMA * w.p / w.rho), p=w.p if p is None else p, un=-w.u)
+
+
+def test_the_exact_post_shock_state_behind_gives_a_standing_shock():
+    free = free_at(3)
+    w = shock_state(free, GAMMA, 3, -1, 0).state
+    b = _behind(w)
+    assert abs(compatible_shock(free, GAMMA, -1, 0, b["rho"], b["a"], b["p"], b["un"]).speed) < 1e-12
+
+
+def test_higher_pressure_behind_moves_the_shock_out_and_lower_moves_it_in():
+    free = free_at(3)
+    w = shock_state(free, GAMMA, 3, -1, 0).state
+    up = _behind(w, 1.05 * w.p)
+    down = _behind(w, 0.95 * w.p)
+    assert compatible_shock(free, GAMMA, -1, 0, up["rho"], up["a"], up["p"], up["un"]).speed > 0
+    assert compatible_shock(free, GAMMA, -1, 0, down["rho"], down["a"], down["p"], down["un"]).speed < 0
+
+
+def test_where_no_shock_fits_it_is_a_mach_wave():
+    free = free_at(2)
+    nx, ny = -math.sin(45 * DEG), math.cos(45 * DEG)
+    s = compatible_shock(free, GAMMA, nx, ny, 1.0, math.sqrt(GAMMA), 1.0, free.u * nx + free.v * ny)
+    assert abs(s.state.p - 1) < 1e-14 and abs(s.state.rho - 1) < 1e-14 and s.mach == 1.0
+
+
+def test_cone_field_meets_the_shock_and_the_cone():
+    cone = 20 * DEG
+    speed, angle, flow = cone_flow_field(3.0, cone, GAMMA, [cone])
+    # On the cone the flow runs along the surface at the surface Mach number.
+    assert abs(angle[0] - cone) < 1e-10
+    mach_surface = math.sqrt(2 / ((GAMMA - 1) * (1 / speed[0] ** 2 - 1)))
+    assert abs(mach_surface - flow.surface_mach) < 1e-9
+    # Just behind the shock the flow is turned by the oblique shock's deflection.
+    beta = flow.shock_angle
+    _, behind, _ = cone_flow_field(3.0, cone, GAMMA, [beta])
+    tan_d = 2 / math.tan(beta) * (9 * math.sin(beta) ** 2 - 1) / (9 * (GAMMA + math.cos(2 * beta)) + 2)
+    assert abs(behind[0] - math.atan(tan_d)) < 1e-10
+    # Between them the flow angle falls monotonically from the deflection to the cone.
+    rays = np.linspace(cone, beta, 50)
+    _, angles, _ = cone_flow_field(3.0, cone, GAMMA, rays)
+    assert np.all(np.diff(angles) < 0)
+
+
+def test_column_positions_follow_the_density():
+    xs = column_positions([0.0, 1.0, 3.0], lambda x: 10.0, 1)
+    assert xs[0] == 0.0 and xs[-1] == 3.0 and 1.0 in xs
+    assert len(xs) == 31 and np.allclose(np.diff(xs), 0.1)
+    exact = column_positions([0.0, 2.0], lambda x: 1.0 + x, 1, total=12)
+    assert len(exact) == 13
