@@ -114,6 +114,10 @@ SIGNATURES: dict[str, list] = {
                        C.POINTER(abi.FittedShock)],
     "bs_compatible_shock": [C.POINTER(abi.Primitive), C.c_double, C.c_double, C.c_double, C.c_double,
                             C.c_double, C.c_double, C.c_double, C.POINTER(abi.FittedShock)],
+    "bs_body_radius": [C.POINTER(abi.Body), C.c_int32, _dp, _dp],
+    "bs_nose_slopes": [C.POINTER(abi.Body), _dp, _dp],
+    "bs_sharp_fit_columns": [C.POINTER(abi.Body), C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_double,
+                             C.c_double, C.c_int32, _dp, _ip],
     "bs_column_positions": [C.c_int32, _dp, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, _dp,
                             _ip],
     "bs_batch_iterate": [_vp, C.c_int32],

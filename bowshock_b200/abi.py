@@ -41,7 +41,7 @@ LIMITER = {
 RECONSTRUCTION = {"perVariable": 0, "shared": 1, "sharedScaled": 2}
 INTEGRATOR = {"forwardEuler": 0, "ssprk2": 1, "ssprk3": 2}
 TIME_STEPPING = {"local": 0, "global": 1}
-BC_KIND = {"inflow": 0, "outflow": 1, "wall": 2, "farField": 3, "periodic": 4}
+BC_KIND = {"inflow": 0, "outflow": 1, "wall": 2, "farField": 3, "periodic": 4, "faceStates": 5}
 SIDES = ("iMin", "iMax", "jMin", "jMax")
 SIDE = {name: k for k, name in enumerate(SIDES)}
 GRID_UNGATED = 1

@@ -6,6 +6,7 @@
 #include "../common.hpp"
 #include "bowshock.h"
 #include "gasdyn.hpp"
+#include "geometry.hpp"
 #include "grids.hpp"
 
 struct bs_grid {
@@ -224,6 +225,42 @@ bs_status bs_column_positions(int32_t n_breakpoints, const double* breakpoints, 
   const std::vector<double> bp(breakpoints, breakpoints + n_breakpoints);
   const std::vector<double> xs =
       bs::column_positions(bp, [&](double x) { return density(x, user); }, refinement, total);
+  if (int64_t(xs.size()) > capacity) return bs::fail(BS_INVALID_ARGUMENT, "more positions than the output holds");
+  for (size_t k = 0; k < xs.size(); k++) out[k] = xs[k];
+  *n_out = int32_t(xs.size());
+  return bs::ok();
+}
+
+bs_status bs_body_radius(const bs_body* body, int32_t n, const double* x, double* r) {
+  if (body == nullptr || n < 0 || (n > 0 && (x == nullptr || r == nullptr)))
+    return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  const bs::Body b = to_body(*body);
+  const std::string e = bs::validate_body(b);
+  if (!e.empty()) return bs::fail(BS_INVALID_ARGUMENT, e);
+  for (int32_t k = 0; k < n; k++) r[k] = bs::body_radius(b, x[k]);
+  return bs::ok();
+}
+
+bs_status bs_nose_slopes(const bs_body* body, double* tip, double* base) {
+  if (body == nullptr || tip == nullptr || base == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  const bs::Body b = to_body(*body);
+  const std::string e = bs::validate_body(b);
+  if (!e.empty()) return bs::fail(BS_INVALID_ARGUMENT, e);
+  *tip = bs::nose_tip_slope(b.nose);
+  *base = bs::nose_base_slope(b.nose);
+  return bs::ok();
+}
+
+bs_status bs_sharp_fit_columns(const bs_body* body, double beta, double x0, int32_t nj, int32_t refinement,
+                               double aspect, double density, int32_t capacity, double* out, int32_t* n_out) {
+  if (body == nullptr || out == nullptr || n_out == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  if (!(nj >= 2 && refinement >= 1 && beta > 0 && beta < M_PI / 2 && x0 > 0 && aspect > 0 && density > 0))
+    return bs::fail(BS_INVALID_ARGUMENT, "sharp fitted columns need nj >= 2, refinement >= 1, 0 < beta < pi/2");
+  const bs::Body b = to_body(*body);
+  const std::string e = bs::validate_body(b);
+  if (!e.empty()) return bs::fail(BS_INVALID_ARGUMENT, e);
+  if (!(x0 < b.nose.length)) return bs::fail(BS_INVALID_ARGUMENT, "the domain must start on the nose");
+  const std::vector<double> xs = bs::sharp_fit_columns(b, beta, x0, nj, refinement, aspect, density);
   if (int64_t(xs.size()) > capacity) return bs::fail(BS_INVALID_ARGUMENT, "more positions than the output holds");
   for (size_t k = 0; k < xs.size(); k++) out[k] = xs[k];
   *n_out = int32_t(xs.size());

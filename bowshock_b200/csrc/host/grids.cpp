@@ -610,6 +610,21 @@ std::string blunt_body_grid(const Body& body, const BluntGridOptions& o, Grid* o
   return "";
 }
 
+std::vector<double> sharp_fit_columns(const Body& body, double beta, double x0, int nj, int refinement,
+                                      double aspect, double density) {
+  const double L = body.nose.length, R = body.nose.base_radius;
+  const double x_end = body_length(body);
+  auto guess = [&](double x) { return std::max(x * std::tan(beta) - body_radius(body, x), 1e-12 * L); };
+  auto spacing = [&](double x) {
+    const double h = guess(x);
+    const double b = std::min(std::log1p(h / R), 2 * std::log(10.0));
+    return (aspect * h * b * std::exp(b / 2)) / (std::expm1(b) * nj);
+  };
+  const std::vector<double> bp = body.cylinder_length > 0 ? std::vector<double>{x0, L, x_end}
+                                                          : std::vector<double>{x0, L};
+  return column_positions(bp, [&](double x) { return density / spacing(x); }, refinement, 0);
+}
+
 std::string ramp_grid(int ni, int nj, double x_min, double x_corner, double x_max, double height,
                       double angle, Grid* out) {
   if (!(x_min < x_corner && x_corner < x_max)) return "the corner must lie inside";

@@ -73,6 +73,15 @@ struct BluntGridOptions {
 std::string blunt_body_grid(const Body& body, const BluntGridOptions& options, Grid* out,
                             bool* quality_error);
 
+// The column positions of a sharp nose's fitted grid (sharpFitProblem,
+// src/analysis/fitted-flow.ts:380-395): from `x0` to the end of the body,
+// the breakpoints at the nose's end and the body's, spaced `aspect` times the
+// geometric mean of the wall and outer cell heights of the first guess of
+// the shock, the tip cone's shock line at angle `beta`; `nj` cells across
+// (refined), `density` the columns' density factor.
+std::vector<double> sharp_fit_columns(const Body& body, double beta, double x0, int nj, int refinement,
+                                      double aspect, double density);
+
 // rampGrid (src/grid/shapes.ts:30-52).
 std::string ramp_grid(int ni, int nj, double x_min, double x_corner, double x_max, double height,
                       double angle, Grid* out);

@@ -6,11 +6,16 @@ native library.
 from __future__ import annotations
 
 import ctypes as C
+import math
+from dataclasses import dataclass
 
 import numpy as np
 
 from . import _native, abi
-from .config import Primitive2D
+from .config import (Boundary, Euler2DConfig, FreeStream, Primitive2D, StructuredGrid, free_stream_at,
+                     steady_drag_config)
+from .engine import forebody_pressure_drag
+from .grid import Body, normal_shock, taylor_maccoll
 
 _DENSITY = C.CFUNCTYPE(C.c_double, C.c_double, C.c_void_p)
 
@@ -65,3 +70,172 @@ def column_positions(breakpoints, density, refinement: int = 1, total: int = 0) 
     _native.check(L.bs_column_positions(len(bp), bp.ctypes.data_as(dp), C.cast(cb, C.c_void_p), None,
                                         int(refinement), int(total), cap, out.ctypes.data_as(dp), C.byref(n)), L)
     return out[:n.value].copy()
+
+
+# ---- the sharp-nose fit problem ----------------------------------------------
+
+SHARP_START = 1e-3       # the solved domain starts at this fraction of the nose (fitted-flow.ts:79)
+SHARP_ASPECT = 2.0       # cells along the body: this many times the across spacing (:84)
+SOLVED_CYLINDER = 1.0    # shortest cylinder solved behind a nose, calibers (:131)
+SPEED_TOLERANCE = 1e-12  # the fit stops when every shock face is slower than this times a_inf (:86)
+RESIDUAL_TOLERANCE = 1e-12  # ... and the residual is below this, relative (:88)
+MAX_ASPECT = 10.0        # the quality gates' largest aspect ratio (src/grid/quality.ts)
+
+
+def line_strength(h, radius: float):
+    """lineStrength (src/grid/blunt-grid.ts:560-562)."""
+    return np.minimum(np.log1p(np.asarray(h) / radius), 2 * math.log(MAX_ASPECT))
+
+
+def stretched_fraction(b, j, nj: int):
+    """stretchedFraction (src/grid/blunt-grid.ts:565-567)."""
+    return np.expm1(b * j / nj) / np.expm1(b)
+
+
+@dataclass
+class FitProblem:
+    """What a fit needs (FitProblem, src/analysis/fitted-flow.ts:192-217):
+    straight grid lines from the body with fixed node fractions, starting
+    shock heights, the inflow plane's states (sharp noses), the start field
+    and the drag of the part ahead of the solved domain."""
+
+    line_x: np.ndarray       # (ni + 1,) line origins on the body
+    line_y: np.ndarray
+    line_dx: np.ndarray      # unit directions
+    line_dy: np.ndarray
+    fractions: np.ndarray    # (ni + 1, nj + 1) node fractions of each line's height
+    heights: np.ndarray      # (ni + 1,) starting shock heights
+    nj: int
+    base_radius: float
+    gamma: float
+    mach: float
+    free: Primitive2D
+    inflow: np.ndarray | None   # (nj, 4) primitives outside the iMin faces, or None (axis)
+    initial: np.ndarray      # (ni nj, 4) primitives, cell (i, j) at i + j ni
+    first_node: str          # 'fixed' or 'symmetry'
+    tip_drag: float          # drag coefficient of the nose ahead of the domain
+
+    @property
+    def ni(self) -> int:
+        return len(self.line_x) - 1
+
+    def nodes(self, heights=None) -> tuple[np.ndarray, np.ndarray]:
+        """gridOnLines (src/grid/blunt-grid.ts:602-620): node (i, j) at
+        i + j (ni + 1), each line cut at its own height."""
+        h = self.heights if heights is None else np.asarray(heights, np.float64)
+        d = h[None, :] * self.fractions.T                   # (nj + 1, ni + 1)
+        x = self.line_x[None, :] + d * self.line_dx[None, :]
+        y = self.line_y[None, :] + d * self.line_dy[None, :]
+        return x.ravel(), y.ravel()
+
+    def grid(self, heights=None) -> StructuredGrid:
+        x, y = self.nodes(heights)
+        return StructuredGrid(self.ni, self.nj, x, y)
+
+    def config(self, heights=None) -> Euler2DConfig:
+        """The engine on the grid (engineConfig, fitted-flow.ts:90-112): the
+        steady scheme, iMin the inflow plane's face states (sharp) or a wall
+        (the axis ahead of a blunt nose), iMax outflow, jMin the wall, jMax
+        the fitted shock's face states."""
+        i_min = Boundary("faceStates") if self.inflow is not None else Boundary("wall")
+        return steady_drag_config(self.grid(heights), self.free, self.gamma, boundaries={
+            "iMin": i_min, "iMax": Boundary("outflow"), "jMin": Boundary("wall"),
+            "jMax": Boundary("faceStates")})
+
+    def drag(self, wall) -> float:
+        """The forebody drag from the wall's fluxes, with the tip's."""
+        fs = FreeStream(self.free, 1.0, 0.5 * self.free.u ** 2)
+        return forebody_pressure_drag(wall, fs, self.base_radius) + self.tip_drag
+
+
+def _body_radius(body: Body, x) -> np.ndarray:
+    L = _native.load()
+    x = np.ascontiguousarray(np.atleast_1d(x), np.float64)
+    r = np.empty_like(x)
+    dp = C.POINTER(C.c_double)
+    _native.check(L.bs_body_radius(C.byref(body.to_abi()), len(x), x.ctypes.data_as(dp), r.ctypes.data_as(dp)), L)
+    return r
+
+
+def _nose_slopes(body: Body) -> tuple[float, float]:
+    L = _native.load()
+    tip, base = C.c_double(), C.c_double()
+    _native.check(L.bs_nose_slopes(C.byref(body.to_abi()), C.byref(tip), C.byref(base)), L)
+    return tip.value, base.value
+
+
+def sharp_fit_problem(asked: Body, mach: float, nj: int = 10, refinement: int = 1, gamma: float = 1.4,
+                      column_density: float = 1.0) -> FitProblem:
+    """sharpFitProblem (src/analysis/fitted-flow.ts:332-465): the flow between
+    a sharp nose and its fitted shock, from a plane normal to the axis just
+    behind the tip, where the tip cone's conical flow (Taylor-Maccoll) comes
+    in, on vertical lines that keep the fractions of the tip shock's first
+    guess. Raises ValueError where the reference refuses the nose."""
+    R = asked.nose.base_radius
+    body = Body(asked.nose, max(asked.cylinder_length, SOLVED_CYLINDER * 2 * R))
+    L = body.nose.length
+    x_end = L + body.cylinder_length
+    free = free_stream_at(mach, gamma).state
+    tip_slope, base_slope = _nose_slopes(body)
+    if not math.isfinite(tip_slope):
+        raise ValueError("the nose is blunt: it needs the blunt fit")
+    tip_angle = math.atan(tip_slope)
+    try:
+        _, _, cone = cone_flow_field(mach, tip_angle, gamma, [tip_angle])
+    except _native.BowshockError as e:
+        raise ValueError(f"at Mach {mach} the bow shock cannot stay attached to a tip of "
+                         f"{math.degrees(tip_angle):.1f} deg half-angle") from e
+    beta = cone.shock_angle
+    enthalpy = gamma / (gamma - 1) + 0.5 * free.u * free.u
+    v_max = math.sqrt(2 * enthalpy)
+    jump = normal_shock(mach * math.sin(beta), gamma)
+    entropy = jump.pressure_ratio / jump.density_ratio ** gamma
+
+    def conical(polar) -> np.ndarray:
+        rays = np.clip(np.atleast_1d(np.asarray(polar, np.float64)), tip_angle, beta)
+        speed, angle, _ = cone_flow_field(mach, tip_angle, gamma, rays)
+        v = speed * v_max
+        a2 = (gamma - 1) * (enthalpy - 0.5 * v * v)
+        rho = (a2 / gamma / entropy) ** (1 / (gamma - 1))
+        return np.stack([rho, v * np.cos(angle), v * np.sin(angle), entropy * rho ** gamma], 1)
+
+    nj = nj * refinement
+    x0 = SHARP_START * L
+
+    def guess(x):
+        x = np.atleast_1d(np.asarray(x, np.float64))
+        return np.maximum(x * math.tan(beta) - _body_radius(body, x), 1e-12 * L)
+
+    L_ = _native.load()
+    cap = 1 << 20
+    xs = np.empty(cap, np.float64)
+    count = C.c_int32()
+    _native.check(L_.bs_sharp_fit_columns(C.byref(body.to_abi()), beta, x0, nj, refinement, SHARP_ASPECT,
+                                          column_density, cap, xs.ctypes.data_as(C.POINTER(C.c_double)),
+                                          C.byref(count)), L_)
+    xs = xs[:count.value].copy()
+    h = guess(xs)
+    b = line_strength(h, R)
+    fractions = stretched_fraction(b[:, None], np.arange(nj + 1)[None, :], nj)
+    n = len(xs)
+    problem = FitProblem(xs.copy(), _body_radius(body, xs), np.zeros(n), np.ones(n), fractions, h.copy(), nj, R,
+                         gamma, mach, free, None, np.empty(0), "fixed", 0.0)
+    X, Y = problem.nodes()
+    X = X.reshape(nj + 1, n)
+    Y = Y.reshape(nj + 1, n)
+    # The inflow plane's faces take the conical flow at their midpoints.
+    mx, my = 0.5 * (X[:-1, 0] + X[1:, 0]), 0.5 * (Y[:-1, 0] + Y[1:, 0])
+    problem.inflow = conical(np.arctan2(my, mx))
+    # The axial Mach number of the conical flow is least on the surface.
+    surface = conical(tip_angle)[0]
+    a_s = math.sqrt(gamma * surface[3] / surface[0])
+    surface_mach = math.hypot(surface[1], surface[2]) / a_s
+    if not surface[1] / a_s > 1 and (not surface_mach > 1 or base_slope > 0):
+        raise ValueError(f"at Mach {mach} the flow behind a tip of {math.degrees(tip_angle):.1f} deg half-angle "
+                         "crosses the starting plane subsonically")
+    cx = 0.25 * (X[:-1, :-1] + X[:-1, 1:] + X[1:, :-1] + X[1:, 1:])
+    cy = 0.25 * (Y[:-1, :-1] + Y[:-1, 1:] + Y[1:, :-1] + Y[1:, 1:])
+    problem.initial = conical(np.arctan2(cy, cx).ravel())
+    r0 = float(_body_radius(body, x0)[0])
+    problem.tip_drag = taylor_maccoll(mach, tip_angle, gamma).surface_pressure_coefficient * (r0 / R) ** 2
+    return problem

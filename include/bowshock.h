@@ -94,7 +94,11 @@ typedef enum bs_bc_kind {
   BS_BC_OUTFLOW = 1,
   BS_BC_WALL = 2,
   BS_BC_FAR_FIELD = 3,
-  BS_BC_PERIODIC = 4
+  BS_BC_PERIODIC = 4,
+  /* States outside each face given per face, with an optional flux imposed
+   * per face ('faceStates', src/engine-cpu/euler2d.ts:42, 356-390): the
+   * fitted shock's sides (bs_fit_*); batches and engines refuse it. */
+  BS_BC_FACE_STATES = 5
 } bs_bc_kind;
 
 /* Side (src/engine-cpu/euler2d.ts:32). */
@@ -485,6 +489,22 @@ BS_API bs_status bs_shock_state(const bs_primitive *free, double gamma, double m
  * pressure and normal velocity extrapolated to the face. */
 BS_API bs_status bs_compatible_shock(const bs_primitive *free, double gamma, double nx, double ny, double rho,
                                      double a, double p, double un, bs_fitted_shock *out);
+
+/* The body's radius at axial position x (bodyRadius, src/geometry/body.ts:25-28),
+ * for n positions. */
+BS_API bs_status bs_body_radius(const bs_body *body, int32_t n, const double *x, double *r);
+/* The nose profile's slope dr/dx at the tip (infinite for a blunt tip) and at
+ * the base (noseTipSlope / noseBaseSlope, src/geometry/nose.ts:145-196). */
+BS_API bs_status bs_nose_slopes(const bs_body *body, double *tip, double *base);
+
+/* The column positions of a sharp nose's fitted grid (sharpFitProblem,
+ * src/analysis/fitted-flow.ts:380-395): from x0 to the end of the body, with
+ * the nose's end as a breakpoint, spaced `aspect` times the geometric mean of
+ * the wall and outer cell heights under the tip cone's shock line at angle
+ * beta, nj cells across (refined). At most `capacity` positions. */
+BS_API bs_status bs_sharp_fit_columns(const bs_body *body, double beta, double x0, int32_t nj,
+                                      int32_t refinement, double aspect, double density, int32_t capacity,
+                                      double *out, int32_t *n_out);
 
 /* Node positions along a line of breakpoints by an integrated density
  * (columnPositions, src/grid/spacing.ts:31-71): `total` > 0 asks for exactly

@@ -378,6 +378,10 @@ class Engine {
     }
   };
   State st, stage_buf[2], res;
+  // 'faceStates' sides: the state outside each face, and the flux imposed
+  // on each face if any (setFaceStates / setFaceFluxes, :356-398).
+  std::vector<Prim<T>> face_states_[4];
+  std::vector<T> face_fluxes_[4];
   std::vector<T> dt;
   int64_t steps = 0;
   double time = 0;
@@ -403,6 +407,12 @@ class Engine {
     cfg = c;
     ni = c.ni;
     nj = c.nj;
+    for (int side = 0; side < 4; side++) {
+      face_fluxes_[side].clear();
+      face_states_[side].clear();
+      if (c.boundaries[side].kind == BS_BC_FACE_STATES)
+        face_states_[side].assign(side < 2 ? nj : ni, Prim<T>{T(1), T(0), T(0), T(1)});
+    }
     e = compute_metrics(ni, nj, x, y, c.geometry == BS_AXISYMMETRIC, m64);
     if (!e.empty()) return e;
     // The FP32 instantiation rounds gamma as the GPU engine does
@@ -507,10 +517,12 @@ class Engine {
           ghost_cells(side, t, g, gc);
           const size_t ghost = gc[0];
           const size_t source = kind == BS_BC_PERIODIC ? gc[2] : gc[1];
-          if (kind == BS_BC_INFLOW || kind == BS_BC_FAR_FIELD) {
+          if (kind == BS_BC_INFLOW || kind == BS_BC_FAR_FIELD || kind == BS_BC_FACE_STATES) {
             Prim<T> w;
             if (kind == BS_BC_INFLOW) {
               w = bc_state(side);
+            } else if (kind == BS_BC_FACE_STATES) {
+              w = face_states_[side][t];
             } else {
               size_t g0[3];
               ghost_cells(side, t, 0, g0);
@@ -570,6 +582,13 @@ class Engine {
   }
 
   // computeResidual (:1208-1296).
+  // The flux imposed on boundary face t of a side into f; false if none (:392-398).
+  bool imposed_flux(int side, int t, T* f) const {
+    if (side < 0 || face_fluxes_[side].empty()) return false;
+    for (int k = 0; k < 4; k++) f[k] = face_fluxes_[side][4 * size_t(t) + k];
+    return true;
+  }
+
   void compute_residual(State& u) {
     fill_ghosts(u);
     std::fill(res.rho.begin(), res.rho.end(), T(0));
@@ -592,10 +611,12 @@ class Engine {
       for (int i = 0; i <= ni; i++) {
         const size_t fi = i + size_t(j) * (ni + 1);
         const int side = i == 0 ? BS_IMIN : i == ni ? BS_IMAX : -1;
-        Prim<T> l, r;
-        face_states(u, true, i, j, l, r);
-        wall_mirrored(side, inx[fi], iny[fi], l, r);
-        face_flux_2d(cfg.flux, l, r, inx[fi], iny[fi], gamma, f);
+        if (!imposed_flux(side, j, f)) {
+          Prim<T> l, r;
+          face_states(u, true, i, j, l, r);
+          wall_mirrored(side, inx[fi], iny[fi], l, r);
+          face_flux_2d(cfg.flux, l, r, inx[fi], iny[fi], gamma, f);
+        }
         accumulate(index(i - 1, j), index(i, j), iarea[fi]);
       }
     }
@@ -603,10 +624,12 @@ class Engine {
       for (int i = 0; i < ni; i++) {
         const size_t fj = i + size_t(j) * ni;
         const int side = j == 0 ? BS_JMIN : j == nj ? BS_JMAX : -1;
-        Prim<T> l, r;
-        face_states(u, false, i, j, l, r);
-        wall_mirrored(side, jnx[fj], jny[fj], l, r);
-        face_flux_2d(cfg.flux, l, r, jnx[fj], jny[fj], gamma, f);
+        if (!imposed_flux(side, i, f)) {
+          Prim<T> l, r;
+          face_states(u, false, i, j, l, r);
+          wall_mirrored(side, jnx[fj], jny[fj], l, r);
+          face_flux_2d(cfg.flux, l, r, jnx[fj], jny[fj], gamma, f);
+        }
         accumulate(index(i, j - 1), index(i, j), jarea[fj]);
       }
     }

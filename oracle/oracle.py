@@ -46,6 +46,8 @@ def lib() -> C.CDLL:
             "bso_metrics": [vp, dp, dp, dp],
             "bso_set_primitives": [vp, dp],
             "bso_set_conserved": [vp, dp],
+            "bso_set_face_states": [vp, C.c_int, dp],
+            "bso_set_face_fluxes": [vp, C.c_int, dp],
             "bso_iterate": [vp, C.c_int],
             "bso_iterate_implicit": [vp, C.c_int, C.c_double, C.c_double],
             "bso_implicit_correction": [vp, C.c_double, C.c_double, dp],
@@ -142,6 +144,21 @@ class OracleEuler2D:
     def set_uniform(self, s) -> None:
         w = np.tile(np.array([s.rho, s.u, s.v, s.p], dtype=np.float64), self.n_cells)
         self.set_primitives(w)
+
+    def set_face_states(self, side: str, prims: np.ndarray) -> None:
+        """setFaceStates (src/engine-cpu/euler2d.ts:356-366): primitives
+        outside each face of a 'faceStates' side."""
+        p = np.ascontiguousarray(prims, dtype=np.float64).reshape(-1)
+        _check(lib().bso_set_face_states(self._h, abi.SIDE[side], _dp(p)))
+
+    def set_face_fluxes(self, side: str, fluxes: np.ndarray | None) -> None:
+        """setFaceFluxes (:368-390): fluxes per unit area imposed on each face
+        of a 'faceStates' side, or None for the Riemann flux."""
+        if fluxes is None:
+            _check(lib().bso_set_face_fluxes(self._h, abi.SIDE[side], None))
+            return
+        f = np.ascontiguousarray(fluxes, dtype=np.float64).reshape(-1)
+        _check(lib().bso_set_face_fluxes(self._h, abi.SIDE[side], _dp(f)))
 
     def set_conserved(self, q: np.ndarray) -> None:
         q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1)

@@ -142,6 +142,42 @@ int bso_set_conserved(void* h, const double* q) {
   });
 }
 
+// setFaceStates / setFaceFluxes (src/engine-cpu/euler2d.ts:356-390) for a
+// 'faceStates' side: primitives (4 per face), and fluxes per unit area (4
+// per face) or null to go back to the Riemann flux.
+int bso_set_face_states(void* h, int side, const double* prim) {
+  return with_engine(h, [&](auto& e) {
+    using T = decltype(e.gamma);
+    if (side < 0 || side > 3 || e.cfg.boundaries[side].kind != BS_BC_FACE_STATES) {
+      g_error = "the side does not take face states";
+      return BS_INVALID_ARGUMENT;
+    }
+    const int along = side < 2 ? e.nj : e.ni;
+    e.face_states_[side].resize(along);
+    for (int t = 0; t < along; t++)
+      e.face_states_[side][t] = {T(prim[4 * t]), T(prim[4 * t + 1]), T(prim[4 * t + 2]), T(prim[4 * t + 3])};
+    return BS_OK;
+  });
+}
+
+int bso_set_face_fluxes(void* h, int side, const double* flux) {
+  return with_engine(h, [&](auto& e) {
+    using T = decltype(e.gamma);
+    if (side < 0 || side > 3 || e.cfg.boundaries[side].kind != BS_BC_FACE_STATES) {
+      g_error = "the side does not take face fluxes";
+      return BS_INVALID_ARGUMENT;
+    }
+    const int along = side < 2 ? e.nj : e.ni;
+    if (flux == nullptr) {
+      e.face_fluxes_[side].clear();
+    } else {
+      e.face_fluxes_[side].resize(4 * size_t(along));
+      for (size_t k = 0; k < 4 * size_t(along); k++) e.face_fluxes_[side][k] = T(flux[k]);
+    }
+    return BS_OK;
+  });
+}
+
 int bso_iterate(void* h, int steps) {
   return with_engine(h, [&](auto& e) {
     if (!e.iterate(steps)) {

@@ -113,3 +113,53 @@ def test_column_positions_follow_the_density():
     assert len(xs) == 31 and np.allclose(np.diff(xs), 0.1)
     exact = column_positions([0.0, 2.0], lambda x: 1.0 + x, 1, total=12)
     assert len(exact) == 13
+
+
+def test_sharp_fit_problem_lays_lines_under_the_tip_cone_shock():
+    from bowshock_b200.fitted import sharp_fit_problem
+    from bowshock_b200.workloads import cone_body
+
+    p = sharp_fit_problem(cone_body(20, 4.0), 3.0, nj=10)
+    assert p.nj == 10 and p.ni > 100 and p.first_node == "fixed"
+    assert np.all(np.diff(p.line_x) > 0) and np.all(p.line_dx == 0) and np.all(p.line_dy == 1)
+    assert np.allclose(p.fractions[:, 0], 0) and np.allclose(p.fractions[:, -1], 1)
+    beta = cone_flow_field(3.0, 20 * DEG, GAMMA, [20 * DEG])[2].shock_angle
+    on_nose = p.line_x < 0.5 / math.tan(20 * DEG)
+    assert np.allclose((p.line_y + p.heights)[on_nose], p.line_x[on_nose] * math.tan(beta), rtol=1e-12)
+    assert p.inflow.shape == (10, 4) and p.initial.shape == (p.ni * 10, 4)
+    with pytest.raises(ValueError):
+        sharp_fit_problem(cone_body(45, 4.0), 1.5, nj=10)
+
+
+def test_oracle_face_states_keep_a_uniform_stream():
+    from bowshock_b200.config import Boundary, grid_from_function, steady_drag_config
+    from oracle.oracle import OracleEuler2D
+
+    free = free_at(2.0)
+    grid = grid_from_function(12, 8, lambda i, j: (0.1 * i, 0.05 + 0.1 * j + 0.01 * i))
+    cfg = steady_drag_config(grid, free, boundaries={
+        "iMin": Boundary("faceStates"), "iMax": Boundary("outflow"), "jMin": Boundary("outflow"),
+        "jMax": Boundary("faceStates")})
+    o = OracleEuler2D(cfg)
+    o.set_uniform(free)
+    w = np.array([free.rho, free.u, free.v, free.p])
+    o.set_face_states("iMin", np.tile(w, (8, 1)))
+    o.set_face_states("jMax", np.tile(w, (12, 1)))
+    o.iterate(20)
+    assert np.allclose(o.primitives().reshape(-1, 4), w, atol=1e-12)
+
+
+def test_oracle_fit_moves_the_shock_towards_rest_and_the_conical_drag():
+    # A few hundred fitted steps on the Mach 3, 20 deg cone (nj = 10): the
+    # shock slows by orders of magnitude and the drag is already within a few
+    # 1e-3 of Taylor-Maccoll (the reference measured +0.1017 % converged).
+    from bowshock_b200.fitted import sharp_fit_problem
+    from bowshock_b200.grid import taylor_maccoll
+    from bowshock_b200.workloads import cone_body
+    from oracle.shock_fitting import fit_shock
+
+    p = sharp_fit_problem(cone_body(20, 4.0), 3.0, nj=10)
+    f = fit_shock(p, 150)
+    assert f.speeds[-1] < 0.02 * f.speeds[0]
+    exact = taylor_maccoll(3.0, 20 * DEG, GAMMA).surface_pressure_coefficient
+    assert abs(p.drag(f.engine.boundary_fluxes("jMin")) / exact - 1) < 3e-3
