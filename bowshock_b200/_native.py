@@ -116,6 +116,16 @@ SIGNATURES: dict[str, list] = {
                             C.c_double, C.c_double, C.c_double, C.POINTER(abi.FittedShock)],
     "bs_body_radius": [C.POINTER(abi.Body), C.c_int32, _dp, _dp],
     "bs_nose_slopes": [C.POINTER(abi.Body), _dp, _dp],
+    "bs_fit_create": [C.POINTER(abi.Config), _dp, _dp, _dp, _dp, _dp, _dp, C.POINTER(abi.Primitive), _dp,
+                      C.c_int32, _dp, C.POINTER(_vp)],
+    "bs_fit_destroy": [_vp],
+    "bs_fit_iterate": [_vp, C.c_int32],
+    "bs_fit_check": [_vp, _dp, _dp],
+    "bs_fit_solve": [_vp, C.c_double, C.c_double, C.c_int32, C.c_int32, _ip, _ip, _dp, _dp],
+    "bs_fit_heights": [_vp, _dp],
+    "bs_fit_nodes": [_vp, _dp, _dp],
+    "bs_fit_read_primitives": [_vp, _dp],
+    "bs_fit_forebody_drag": [_vp, C.c_double, C.c_double, C.c_double, _dp],
     "bs_sharp_fit_columns": [C.POINTER(abi.Body), C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_double,
                              C.c_double, C.c_int32, _dp, _ip],
     "bs_column_positions": [C.c_int32, _dp, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, _dp,

@@ -56,6 +56,10 @@ struct CaseDev {
   double cfl;     // explicit CFL number
   double inflow_prim[4][4];  // (rho, u, v, p) outside each inflow / far-field side
   double inflow_cons[4][4];  // the same as conserved variables
+  // 'faceStates' sides: the conserved state outside each face (4 per face,
+  // FP64), and the flux per unit area imposed on each face or null.
+  const double* face_state[4] = {};
+  const double* face_flux[4] = {};
 };
 
 template <class R>
@@ -112,6 +116,11 @@ __device__ __forceinline__ Cons<R> cell_or_ghost(const CaseDev& cd, const Metric
     f = m.jface[cd.jface + i + int64_t(nj) * ni];
   }
   const int kind = cd.bc[side];
+  if (kind == BS_BC_FACE_STATES) {
+    // Both ghost layers hold the state given outside the face.
+    const double* s = cd.face_state[side] + 4 * (side < 2 ? ij : ii);
+    return {R(s[0]), R(s[1]), R(s[2]), R(s[3])};
+  }
   if (kind == BS_BC_INFLOW) {
     if (inflow_from_prim) {
       const double* s = cd.inflow_prim[side];

@@ -126,10 +126,16 @@ __global__ void __launch_bounds__(TILE_THREADS, kMinBlocks) tile_kernel(const Ti
       const int gi = i0 + fl, gj = j0 + fr;
       const float4 fm = A.m.iface[cd.iface + gi + int64_t(gj) * (ni + 1)];
       const int sj = fr + 2, si = fl + 2;
-      face_states(cd.recon, cd.limiter, Wat(sj, si - 2), Wat(sj, si - 1), Wat(sj, si),
-                  Wat(sj, si + 1), gamma, wall_side(cd, gi, ni, BS_IMIN, BS_IMAX), R(fm.x),
-                  R(fm.y), left, right);
-      face_flux(cd.flux, left, right, R(fm.x), R(fm.y), gamma, flux);
+      const double* imposed = (gi == 0 || gi == ni) ? cd.face_flux[gi == 0 ? BS_IMIN : BS_IMAX] : nullptr;
+      if (imposed != nullptr) {
+#pragma unroll
+        for (int v = 0; v < 4; v++) flux[v] = R(imposed[4 * gj + v]);
+      } else {
+        face_states(cd.recon, cd.limiter, Wat(sj, si - 2), Wat(sj, si - 1), Wat(sj, si),
+                    Wat(sj, si + 1), gamma, wall_side(cd, gi, ni, BS_IMIN, BS_IMAX), R(fm.x),
+                    R(fm.y), left, right);
+        face_flux(cd.flux, left, right, R(fm.x), R(fm.y), gamma, flux);
+      }
       const R area = R(fm.z);
 #pragma unroll
       for (int v = 0; v < 4; v++) Fi[v][fr][fl] = flux[v] * area;
@@ -139,10 +145,16 @@ __global__ void __launch_bounds__(TILE_THREADS, kMinBlocks) tile_kernel(const Ti
       const int gi = i0 + fl, gj = j0 + fr;
       const float4 fm = A.m.jface[cd.jface + gi + int64_t(gj) * ni];
       const int sj = fr + 2, si = fl + 2;
-      face_states(cd.recon, cd.limiter, Wat(sj - 2, si), Wat(sj - 1, si), Wat(sj, si),
-                  Wat(sj + 1, si), gamma, wall_side(cd, gj, nj, BS_JMIN, BS_JMAX), R(fm.x),
-                  R(fm.y), left, right);
-      face_flux(cd.flux, left, right, R(fm.x), R(fm.y), gamma, flux);
+      const double* imposed = (gj == 0 || gj == nj) ? cd.face_flux[gj == 0 ? BS_JMIN : BS_JMAX] : nullptr;
+      if (imposed != nullptr) {
+#pragma unroll
+        for (int v = 0; v < 4; v++) flux[v] = R(imposed[4 * gi + v]);
+      } else {
+        face_states(cd.recon, cd.limiter, Wat(sj - 2, si), Wat(sj - 1, si), Wat(sj, si),
+                    Wat(sj + 1, si), gamma, wall_side(cd, gj, nj, BS_JMIN, BS_JMAX), R(fm.x),
+                    R(fm.y), left, right);
+        face_flux(cd.flux, left, right, R(fm.x), R(fm.y), gamma, flux);
+      }
       const R area = R(fm.z);
 #pragma unroll
       for (int v = 0; v < 4; v++) Fj[v][fr][fl] = flux[v] * area;

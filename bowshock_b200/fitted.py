@@ -239,3 +239,112 @@ def sharp_fit_problem(asked: Body, mach: float, nj: int = 10, refinement: int = 
     r0 = float(_body_radius(body, x0)[0])
     problem.tip_drag = taylor_maccoll(mach, tip_angle, gamma).surface_pressure_coefficient * (r0 / R) ** 2
     return problem
+
+
+# ---- the fitted solve on the GPU -----------------------------------------------
+
+class CudaFit:
+    """A fit problem solved with its bow shock fitted, on the GPU (bs_fit_*):
+    every step the shock boundary, an explicit step, the shock's move, the
+    new grid and the remap, replayed from CUDA graphs."""
+
+    def __init__(self, problem: FitProblem):
+        self._lib = _native.load()
+        self.problem = problem
+        cfg = problem.config()
+        dp = C.POINTER(C.c_double)
+        arrays = [np.ascontiguousarray(a, np.float64) for a in (
+            problem.line_x, problem.line_y, problem.line_dx, problem.line_dy, problem.fractions.reshape(-1),
+            problem.heights)]
+        inflow = None if problem.inflow is None else np.ascontiguousarray(problem.inflow, np.float64).reshape(-1)
+        initial = np.ascontiguousarray(problem.initial, np.float64).reshape(-1)
+        h = C.c_void_p()
+        _native.check(self._lib.bs_fit_create(
+            C.byref(cfg.to_abi()), *[a.ctypes.data_as(dp) for a in arrays], C.byref(_prim(problem.free)),
+            None if inflow is None else inflow.ctypes.data_as(dp), 1 if problem.first_node == "symmetry" else 0,
+            initial.ctypes.data_as(dp), C.byref(h)), self._lib)
+        self._h = h
+        self._keep = (arrays, inflow, initial)
+
+    def destroy(self) -> None:
+        if self._h:
+            self._lib.bs_fit_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+    def _call(self, name: str, *args) -> None:
+        _native.check(getattr(self._lib, name)(self._h, *args), self._lib)
+
+    def iterate(self, steps: int) -> None:
+        self._call("bs_fit_iterate", int(steps))
+
+    def check(self) -> tuple[float, float]:
+        """(largest shock speed of the last move over a_inf, relative residual)."""
+        s, r = C.c_double(), C.c_double()
+        self._call("bs_fit_check", C.byref(s), C.byref(r))
+        return s.value, r.value
+
+    def solve(self, max_iterations: int, speed_tolerance: float = SPEED_TOLERANCE,
+              residual_tolerance: float = RESIDUAL_TOLERANCE, check_every: int = 100):
+        """fitShock's loop (shock-fitting.ts:248-311): (converged, iterations,
+        max speed, relative residual)."""
+        it, conv = C.c_int32(), C.c_int32()
+        s, r = C.c_double(), C.c_double()
+        self._call("bs_fit_solve", speed_tolerance, residual_tolerance, int(max_iterations), int(check_every),
+                   C.byref(it), C.byref(conv), C.byref(s), C.byref(r))
+        return bool(conv.value), it.value, s.value, r.value
+
+    def heights(self) -> np.ndarray:
+        out = np.empty(self.problem.ni + 1)
+        self._call("bs_fit_heights", out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out
+
+    def primitives(self) -> np.ndarray:
+        out = np.empty(4 * self.problem.ni * self.problem.nj)
+        self._call("bs_fit_read_primitives", out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out.reshape(-1, 4)
+
+    def drag(self) -> float:
+        """The problem's drag: the wall's forebody drag and the tip's."""
+        f = self.problem.free
+        d = C.c_double()
+        self._call("bs_fit_forebody_drag", f.p, 0.5 * f.rho * (f.u ** 2 + f.v ** 2), self.problem.base_radius,
+                   C.byref(d))
+        return d.value + self.problem.tip_drag
+
+
+def settle(fit: CudaFit, max_iterations: int, noise: float = 1e-8, speed_tolerance: float = 1e-6,
+           check_every: int = 250):
+    """The GPU fit's stopping rule (fitShockGpu, src/engine-gpu/shock-fitting-gpu.ts:
+    135-170): every `check_every` steps the drag is added to a SettlingValue of
+    `noise`; the fit has converged once the drag has settled and the shock
+    moves slower than `speed_tolerance` times a_inf. Here the state is FP64 and
+    the metrics FP32: the shock's speeds settle near 1e-7 (the reference's
+    all-FP32 engine: 1e-6 to 4e-6, against its tolerance of 3e-5).
+    Returns (converged, iterations, max speed, drag)."""
+    from .verification import SettlingValue
+
+    settling = SettlingValue(noise)
+    done, speed, drag = 0, math.inf, math.nan
+    while done < max_iterations:
+        n = min(check_every, max_iterations - done)
+        fit.iterate(n)
+        done += n
+        speed, _ = fit.check()
+        drag = fit.drag()
+        if not math.isfinite(drag):
+            break
+        if settling.add(drag) and speed < speed_tolerance:
+            return True, done, speed, drag
+    return False, done, speed, drag

@@ -497,6 +497,47 @@ BS_API bs_status bs_body_radius(const bs_body *body, int32_t n, const double *x,
  * the base (noseTipSlope / noseBaseSlope, src/geometry/nose.ts:145-196). */
 BS_API bs_status bs_nose_slopes(const bs_body *body, double *tip, double *base);
 
+/* ---- the fitted bow shock (fitShock, src/solver/shock-fitting.ts:170-314) ---
+ *
+ * One case whose jMax side is its bow shock: a curve of nodes on straight
+ * lines from the body (origin (line_x, line_y), unit direction (line_dx,
+ * line_dy), ni + 1 lines), node j of line i at fraction
+ * fractions[i (nj + 1) + j] of the line's height heights[i]. Every step, on
+ * the GPU: the shock compatible with the flow in the two cells below each
+ * jMax face fills that face's ghosts and imposes its flux; one explicit step
+ * (config: SSP-RK with local time steps; iMin the inflow plane's face states,
+ * i_min_states 4 primitives per face, or the axis as a wall; jMin the wall;
+ * iMax outflow; jMax BS_BC_FACE_STATES); each node moves along its line by
+ * the shock's speed times half the top cell's height over its fastest signal;
+ * the grid is rebuilt and the flow interpolated along the lines. first_node:
+ * 0 keeps the first node ('fixed', a sharp tip), 1 keeps the shock normal to
+ * the axis ('symmetry'). initial: 4 primitives per cell, cell (i, j) at
+ * i + j ni. A fit is not re-entrant (BS_BUSY). */
+typedef struct bs_fit bs_fit;
+BS_API bs_status bs_fit_create(const bs_config *config, const double *line_x, const double *line_y,
+                               const double *line_dx, const double *line_dy, const double *fractions,
+                               const double *heights, const bs_primitive *free, const double *i_min_states,
+                               int32_t first_node, const double *initial, bs_fit **out);
+BS_API bs_status bs_fit_destroy(bs_fit *fit);
+BS_API bs_status bs_fit_iterate(bs_fit *fit, int32_t steps);
+/* The largest shock speed of the last move over the free stream's sound
+ * speed, and the density residual of the current flow (its shock boundary
+ * applied) over the larger of the starting flow's and the free stream's on
+ * the first grid. */
+BS_API bs_status bs_fit_check(bs_fit *fit, double *max_speed, double *residual);
+/* Steps in checks of check_every until both fall below their tolerances
+ * (*converged 1) or max_iterations steps are taken. */
+BS_API bs_status bs_fit_solve(bs_fit *fit, double speed_tolerance, double residual_tolerance,
+                              int32_t max_iterations, int32_t check_every, int32_t *iterations,
+                              int32_t *converged, double *max_speed, double *residual);
+BS_API bs_status bs_fit_heights(bs_fit *fit, double *heights);
+BS_API bs_status bs_fit_nodes(bs_fit *fit, double *x, double *y);
+BS_API bs_status bs_fit_read_primitives(bs_fit *fit, double *primitives);
+/* The forebody pressure drag of the jMin wall (FP64 on the GPU), as
+ * bs_engine_forebody_drag. */
+BS_API bs_status bs_fit_forebody_drag(bs_fit *fit, double p_inf, double q_inf, double base_radius,
+                                      double *drag);
+
 /* The column positions of a sharp nose's fitted grid (sharpFitProblem,
  * src/analysis/fitted-flow.ts:380-395): from x0 to the end of the body, with
  * the nose's end as a breakpoint, spaced `aspect` times the geometric mean of

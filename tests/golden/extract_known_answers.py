@@ -106,6 +106,24 @@ def main() -> None:
                   "depth": int(lusgs.group(3)), "max_steps": int(lusgs.group(4)), "cfl": float(lusgs.group(5)),
                   "residual_below": 1e-12, "drag_equal_within": 1e-12},
     }
+    # The fitted bow shock on the Mach 3, 20 deg cone (cylinder 4): the drag's
+    # error against Taylor-Maccoll measured when the reference's test was
+    # written, and the bounds the test asserts.
+    f = "tests/analysis/fitted-flow.test.ts"
+    t = (REF / f).read_text()
+    m = re.search(r"Measured when\s*//\s*written: \+([0-9.]+)% on 10 cells across, \+([0-9.]+)% on that grid", t)
+    bounds = re.search(r"expect\(Math\.abs\(fine\)\)\.toBeLessThan\(([0-9e.-]+)\);\s*"
+                       r"expect\(coarse / fine\)\.toBeGreaterThan\(([0-9.]+)\);\s*"
+                       r"expect\(coarse / fine\)\.toBeLessThan\(([0-9.]+)\);\s*"
+                       r"expect\(Math\.abs\(fine - \(coarse - fine\) / 3\)\)\.toBeLessThan\(([0-9e.-]+)\)", t)
+    out["fitted_cone_mach3"] = {
+        "source": f"{f}:{find_line(t, 'Mach 3, 20 deg cone: drag within')}",
+        "body": {"shape": "conical", "half_angle_deg": 20, "base_radius": 0.5, "cylinder": 4},
+        "mach": 3.0, "nj": 10, "refinements": [1, 2],
+        "measured_rel_err": [float(m.group(1)) / 100, float(m.group(2)) / 100],
+        "fine_below": float(bounds.group(1)), "ratio_above": float(bounds.group(2)),
+        "ratio_below": float(bounds.group(3)), "extrapolated_within": float(bounds.group(4)),
+    }
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {OUT}")
 

@@ -163,3 +163,27 @@ def test_oracle_fit_moves_the_shock_towards_rest_and_the_conical_drag():
     assert f.speeds[-1] < 0.02 * f.speeds[0]
     exact = taylor_maccoll(3.0, 20 * DEG, GAMMA).surface_pressure_coefficient
     assert abs(p.drag(f.engine.boundary_fluxes("jMin")) / exact - 1) < 3e-3
+
+
+def test_fit_create_refuses_a_grid_without_a_shock_side():
+    import ctypes as C
+
+    from bowshock_b200 import _native, abi
+    from bowshock_b200.config import Boundary
+    from bowshock_b200.fitted import sharp_fit_problem
+    from bowshock_b200.workloads import cone_body
+
+    p = sharp_fit_problem(cone_body(20, 4.0), 3.0, nj=10)
+    cfg = p.config()
+    cfg.boundaries["jMax"] = Boundary("outflow")
+    L = _native.load()
+    dp = C.POINTER(C.c_double)
+    arrays = [np.ascontiguousarray(a, np.float64) for a in (p.line_x, p.line_y, p.line_dx, p.line_dy,
+                                                               p.fractions.reshape(-1), p.heights)]
+    inflow = np.ascontiguousarray(p.inflow, np.float64).reshape(-1)
+    initial = np.ascontiguousarray(p.initial, np.float64).reshape(-1)
+    h = C.c_void_p()
+    st = L.bs_fit_create(C.byref(cfg.to_abi()), *[a.ctypes.data_as(dp) for a in arrays],
+                         C.byref(abi.Primitive(p.free.rho, p.free.u, p.free.v, p.free.p)), inflow.ctypes.data_as(dp),
+                         0, initial.ctypes.data_as(dp), C.byref(h))
+    assert st == abi.BS_INVALID_ARGUMENT and b"jMax" in L.bs_last_error()

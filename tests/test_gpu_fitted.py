@@ -1,0 +1,66 @@
+"""The fitted bow shock on the GPU (bs_fit_*): step for step against the
+oracle's restatement of fitShock (oracle/shock_fitting.py), and the
+reference's own test of the method (tests/analysis/fitted-flow.test.ts:36-59):
+on the Mach 3, 20 deg cone the drag is within 0.03 % of Taylor-Maccoll on the
+grid refined once and converges at second order, to the values the
+reference measured (+0.1017 % and +0.0251 %)."""
+from __future__ import annotations
+
+import json
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from bowshock_b200.fitted import CudaFit, settle, sharp_fit_problem
+from bowshock_b200.grid import taylor_maccoll
+from bowshock_b200.workloads import cone_body
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "reference_known_answers.json").read_text())[
+    "fitted_cone_mach3"]
+
+
+def _problem(refinement: int = 1):
+    b = GOLDEN["body"]
+    return sharp_fit_problem(cone_body(b["half_angle_deg"], b["cylinder"]), GOLDEN["mach"], nj=GOLDEN["nj"],
+                             refinement=refinement)
+
+
+def test_fitted_steps_follow_the_oracle():
+    # 150 steps from the conical start: the GPU (FP64 state, FP32 metrics
+    # rebuilt after every move) and the FP64 oracle agree on the shock's
+    # heights, the flow and the drag.
+    from oracle.shock_fitting import fit_shock
+
+    p = _problem()
+    with CudaFit(p) as g:
+        g.iterate(150)
+        h, w, d = g.heights(), g.primitives(), g.drag()
+        speed, _ = g.check()
+    o = fit_shock(p, 150)
+    wo = o.engine.primitives().reshape(-1, 4)
+    assert np.max(np.abs(h - o.heights)) < 1e-7 * np.max(o.heights)
+    assert np.max(np.abs(w - wo) / np.abs(wo).max(axis=0)) < 1e-5
+    assert abs(d / p.drag(o.engine.boundary_fluxes("jMin")) - 1) < 1e-6
+    assert abs(speed / o.speeds[-1] - 1) < 2e-3
+
+
+def test_fitted_cone_drag_converges_at_second_order_to_taylor_maccoll():
+    exact = taylor_maccoll(GOLDEN["mach"], GOLDEN["body"]["half_angle_deg"] * math.pi / 180, 1.4) \
+        .surface_pressure_coefficient
+    errors = []
+    for r in GOLDEN["refinements"]:
+        with CudaFit(_problem(r)) as g:
+            converged, _, speed, drag = settle(g, 60000 * r, check_every=250 * r)
+        assert converged and speed < 1e-6
+        errors.append(drag / exact - 1)
+    coarse, fine = errors
+    assert abs(fine) < GOLDEN["fine_below"]
+    assert GOLDEN["ratio_above"] < coarse / fine < GOLDEN["ratio_below"]
+    assert abs(fine - (coarse - fine) / 3) < GOLDEN["extrapolated_within"]
+    # The values the reference measured, to the digits it gives.
+    for e, measured in zip(errors, GOLDEN["measured_rel_err"]):
+        assert abs(e - measured) < 5e-7
