@@ -125,6 +125,7 @@ SIGNATURES: dict[str, list] = {
     "bs_fit_heights": [_vp, _dp],
     "bs_fit_nodes": [_vp, _dp, _dp],
     "bs_fit_read_primitives": [_vp, _dp],
+    "bs_fit_wall_fluxes": [_vp, C.POINTER(abi.FaceFlux)],
     "bs_fit_forebody_drag": [_vp, C.c_double, C.c_double, C.c_double, _dp],
     "bs_sharp_fit_columns": [C.POINTER(abi.Body), C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_double,
                              C.c_double, C.c_int32, _dp, _ip],

@@ -355,6 +355,29 @@ class FittedSolver {
     return BS_OK;
   }
 
+  // The jMin wall's faces (boundaryFluxes('jMin'), src/engine-cpu/euler2d.ts:
+  // 499-525): midpoint, outward normal, area and the FP64 flux.
+  bs_status wall_fluxes(bs_face_flux* out) {
+    double force = 0;
+    std::vector<double> f(4 * size_t(ni_));
+    FIT_TRY(wall(0.0, f.data(), &force));
+    std::vector<double> g(3 * size_t(ni_)), x(ni_ + 1), y(ni_ + 1);
+    FIT_CUDA(cudaMemcpy(g.data(), bgeom_.p + 3 * size_t(2 * nj_), g.size() * sizeof(double),
+                        cudaMemcpyDeviceToHost));
+    FIT_CUDA(cudaMemcpy(x.data(), x_.p, (ni_ + 1) * sizeof(double), cudaMemcpyDeviceToHost));
+    FIT_CUDA(cudaMemcpy(y.data(), y_.p, (ni_ + 1) * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int t = 0; t < ni_; t++) {
+      bs_face_flux& o = out[t];
+      o.x = 0.5 * (x[t] + x[t + 1]);
+      o.y = 0.5 * (y[t] + y[t + 1]);
+      o.nx = -g[3 * t];
+      o.ny = -g[3 * t + 1];
+      o.area = g[3 * t + 2];
+      for (int v = 0; v < 4; v++) o.flux[v] = f[4 * t + v];
+    }
+    return BS_OK;
+  }
+
   int ni() const { return ni_; }
   int nj() const { return nj_; }
   int iterations() const { return iterations_; }
@@ -536,6 +559,13 @@ bs_status bs_fit_read_primitives(bs_fit* fit, double* primitives) {
   FIT_CALL(fit, {
     if (primitives == nullptr) return fail(BS_INVALID_ARGUMENT, "null argument");
     return fit->solver.primitives(primitives);
+  });
+}
+
+bs_status bs_fit_wall_fluxes(bs_fit* fit, bs_face_flux* out) {
+  FIT_CALL(fit, {
+    if (out == nullptr) return fail(BS_INVALID_ARGUMENT, "null argument");
+    return fit->solver.wall_fluxes(out);
   });
 }
 

@@ -315,6 +315,12 @@ class CudaFit:
         self._call("bs_fit_read_primitives", out.ctypes.data_as(C.POINTER(C.c_double)))
         return out.reshape(-1, 4)
 
+    def wall_fluxes(self) -> list:
+        """The jMin wall's faces (boundaryFluxes('jMin')), FP64 on the GPU."""
+        out = (abi.FaceFlux * self.problem.ni)()
+        self._call("bs_fit_wall_fluxes", out)
+        return list(out)
+
     def drag(self) -> float:
         """The problem's drag: the wall's forebody drag and the tip's."""
         f = self.problem.free
@@ -348,3 +354,102 @@ def settle(fit: CudaFit, max_iterations: int, noise: float = 1e-8, speed_toleran
         if settling.add(drag) and speed < speed_tolerance:
             return True, done, speed, drag
     return False, done, speed, drag
+
+
+# ---- the blunt-nose fit problem -------------------------------------------------
+
+CAPTURED_START_STEPS = 3000   # captured steps that start a blunt family (fitted-flow.ts:943)
+MAX_BLUNT_EXTENSION = 7       # calibers of cylinder the blunt body may gain (:163)
+FITTED_MAX_SIZE_RATIO = 1.3   # the fitted grids' size-ratio gate (src/grid/quality.ts:64-68)
+SMOOTHING_PASSES = 20         # 1-2-1 passes over a captured shock (shock-fitting.ts:389)
+
+
+def captured_shock_heights(prims: np.ndarray, x: np.ndarray, y: np.ndarray, lines: np.ndarray,
+                           free: Primitive2D) -> np.ndarray:
+    """capturedShockHeights (src/solver/shock-fitting.ts:360-386): on each
+    line the outer face of the outermost cell whose pressure rose by more
+    than 5 % of its column's peak rise, smoothed by 20 passes of 1-2-1
+    (mirrored at the ends). prims (nj, ni, 4); x, y (nj + 1, ni + 1); lines
+    (ni + 1, 4) as (x, y, dx, dy)."""
+    nj, ni = prims.shape[:2]
+    h = np.empty(ni + 1)
+    for i in range(ni + 1):
+        c = min(i, ni - 1)
+        p = prims[:, c, 3]
+        peak = max(free.p, float(p.max()))
+        threshold = max(0.05 * (peak - free.p), 1e-4 * free.p)
+        above = np.nonzero(p - free.p > threshold)[0]
+        top = int(above[-1]) if len(above) else 0
+        lx, ly, dx, dy = lines[i]
+        h[i] = (x[top + 1, i] - lx) * dx + (y[top + 1, i] - ly) * dy
+    for _ in range(SMOOTHING_PASSES):
+        c = h.copy()
+        h[0] = 0.5 * (c[0] + c[1])
+        h[1:-1] = 0.25 * c[:-2] + 0.5 * c[1:-1] + 0.25 * c[2:]
+        h[-1] = 0.5 * (c[-1] + c[-2])
+    return h
+
+
+def blunt_fit_problem(asked: Body, mach: float, nj: int = 20, gamma: float = 1.4) -> FitProblem:
+    """bluntFitProblem at refinement 1 (src/analysis/fitted-flow.ts:467-730)
+    for noses whose blunt grid is at the body's scale (spheres and
+    ellipsoids): the body's cylinder lengthened a caliber at a time until
+    its C grid meets the fitted grids' size-ratio gate (solvedBluntBody,
+    :140-185); a captured solution on that grid (3,000 explicit steps from
+    the free stream, here on the GPU engine) whose shock, smoothed, is the
+    starting shock; the grid's lines keeping the node fractions of that
+    height; the start field taken at the same fraction of the shock layer
+    (shockLayerStart, :735-768); the first shock node normal to the axis."""
+    from .engine import CudaEuler2D
+    from .grid import blunt_body_grid, grid_quality
+
+    if asked.nose.shape.kind != "ellipsoid":
+        raise ValueError("the blunt fit here takes spheres and ellipsoids (noses whose grid is at the body's scale)")
+    R = asked.nose.base_radius
+    caliber = 2 * R
+    shortest = max(asked.cylinder_length, SOLVED_CYLINDER * caliber)
+    chosen = None
+    for extra in range(MAX_BLUNT_EXTENSION + 1):
+        body = Body(asked.nose, shortest + extra * caliber)
+        grid = blunt_body_grid(body, nj, mach, gated=False).grid
+        if chosen is None:
+            chosen = (body, grid)
+        if grid_quality(grid).max_size_ratio <= FITTED_MAX_SIZE_RATIO:
+            chosen = (body, grid)
+            break
+    body, grid = chosen
+    free = free_stream_at(mach, gamma).state
+    cfg = steady_drag_config(grid, free, gamma, boundaries={
+        "iMin": Boundary("wall"), "iMax": Boundary("outflow"), "jMin": Boundary("wall"),
+        "jMax": Boundary("inflow", free)})
+    with CudaEuler2D(cfg) as e:
+        e.set_uniform(free)
+        e.iterate(CAPTURED_START_STEPS)
+        captured = e.primitives().reshape(grid.nj, grid.ni, 4)
+    ni = grid.ni
+    X = grid.x.reshape(nj + 1, ni + 1)
+    Y = grid.y.reshape(nj + 1, ni + 1)
+    # The generator's lines: from the body node to the outer one.
+    ex, ey = X[nj] - X[0], Y[nj] - Y[0]
+    length = np.hypot(ex, ey)
+    lines = np.stack([X[0], Y[0], ex / length, ey / length], 1)
+    heights = captured_shock_heights(captured, X, Y, lines, free)
+    fractions = stretched_fraction(line_strength(heights, R)[:, None], np.arange(nj + 1)[None, :], nj)
+    # shockLayerStart: each fitted cell at its fraction of the shock layer,
+    # linear between the captured cells of its column either side.
+    along = (X - lines[:, 0]) * lines[:, 2] + (Y - lines[:, 1]) * lines[:, 3]
+    frac = along / heights[None, :]                                   # (nj + 1, ni + 1)
+    centre = 0.25 * (frac[:-1, :-1] + frac[:-1, 1:] + frac[1:, :-1] + frac[1:, 1:])   # (nj, ni)
+    fa = fractions.T                                                  # (nj + 1, ni + 1)
+    s = 0.25 * (fa[:-1, :-1] + fa[1:, :-1] + fa[:-1, 1:] + fa[1:, 1:])
+    initial = np.empty((nj, ni, 4))
+    for i in range(ni):
+        for j in range(nj):
+            jj = 0
+            while jj < nj - 2 and centre[jj + 1, i] < s[j, i]:
+                jj += 1
+            c0 = centre[jj, i]
+            t = min(max((s[j, i] - c0) / (centre[jj + 1, i] - c0), 0.0), 1.0)
+            initial[j, i] = captured[jj, i] + t * (captured[jj + 1, i] - captured[jj, i])
+    return FitProblem(lines[:, 0].copy(), lines[:, 1].copy(), lines[:, 2].copy(), lines[:, 3].copy(), fractions,
+                      heights, nj, R, gamma, mach, free, None, initial.reshape(-1, 4), "symmetry", 0.0)

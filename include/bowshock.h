@@ -533,6 +533,8 @@ BS_API bs_status bs_fit_solve(bs_fit *fit, double speed_tolerance, double residu
 BS_API bs_status bs_fit_heights(bs_fit *fit, double *heights);
 BS_API bs_status bs_fit_nodes(bs_fit *fit, double *x, double *y);
 BS_API bs_status bs_fit_read_primitives(bs_fit *fit, double *primitives);
+/* The jMin wall's fluxes, ni faces, as bs_engine_boundary_fluxes. */
+BS_API bs_status bs_fit_wall_fluxes(bs_fit *fit, bs_face_flux *out);
 /* The forebody pressure drag of the jMin wall (FP64 on the GPU), as
  * bs_engine_forebody_drag. */
 BS_API bs_status bs_fit_forebody_drag(bs_fit *fit, double p_inf, double q_inf, double base_radius,

@@ -124,6 +124,15 @@ def main() -> None:
         "fine_below": float(bounds.group(1)), "ratio_above": float(bounds.group(2)),
         "ratio_below": float(bounds.group(3)), "extrapolated_within": float(bounds.group(4)),
     }
+    hm = re.search(r"Measured when written: \+([0-9.]+)% \(nj = (\d+)\); with the captured shock \+([0-9.]+)%", t)
+    tol = re.search(r"expect\(Math\.abs\(p / pitot - 1\)\)\.toBeLessThan\(([0-9e.-]+)\)", t)
+    out["fitted_hemisphere_mach2"] = {
+        "source": f"{f}:{find_line(t, 'Mach 2 hemisphere-cylinder')}",
+        "body": {"shape": "ellipsoid", "length": 0.5, "base_radius": 0.5, "cylinder": 4},
+        "mach": 2.0, "nj": int(hm.group(2)),
+        "measured_rel_err": float(hm.group(1)) / 100, "captured_rel_err": float(hm.group(3)) / 100,
+        "within": float(tol.group(1)),
+    }
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {OUT}")
 

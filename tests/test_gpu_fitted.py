@@ -64,3 +64,52 @@ def test_fitted_cone_drag_converges_at_second_order_to_taylor_maccoll():
     # The values the reference measured, to the digits it gives.
     for e, measured in zip(errors, GOLDEN["measured_rel_err"]):
         assert abs(e - measured) < 5e-7
+
+
+HEMI = json.loads((Path(__file__).parent / "golden" / "reference_known_answers.json").read_text())[
+    "fitted_hemisphere_mach2"]
+
+
+def _hemisphere():
+    from bowshock_b200.fitted import blunt_fit_problem
+    from bowshock_b200.grid import Body, Nose, NoseShape
+
+    b = HEMI["body"]
+    body = Body(Nose(NoseShape(b["shape"]), b["length"], b["base_radius"]), b["cylinder"])
+    return blunt_fit_problem(body, HEMI["mach"], nj=HEMI["nj"])
+
+
+def test_blunt_fit_follows_the_oracle():
+    # The hemisphere-cylinder from its captured start: the shock's axis node
+    # kept normal to the axis; GPU and oracle agree after 100 steps.
+    from oracle.shock_fitting import fit_shock
+
+    p = _hemisphere()
+    assert p.first_node == "symmetry" and p.inflow is None
+    with CudaFit(p) as g:
+        g.iterate(100)
+        h, w, d = g.heights(), g.primitives(), g.drag()
+    o = fit_shock(p, 100)
+    wo = o.engine.primitives().reshape(-1, 4)
+    assert np.max(np.abs(h - o.heights)) < 1e-6 * np.max(o.heights)
+    assert np.max(np.abs(w - wo) / np.abs(wo).max(axis=0)) < 1e-4
+    assert abs(d / p.drag(o.engine.boundary_fluxes("jMin")) - 1) < 1e-5
+
+
+def test_hemisphere_stagnation_pressure_is_the_pitot_value():
+    # tests/analysis/fitted-flow.test.ts:61-74: the wall pressure at the
+    # stagnation point, behind the fitted normal shock, within 1e-4 of the
+    # pitot pressure (the reference measured +0.0076 %; captured, +9.7 %).
+    from bowshock_b200.grid import normal_shock
+
+    p = _hemisphere()
+    with CudaFit(p) as g:
+        converged, _, speed, _ = settle(g, 60000, check_every=250)
+        face = g.wall_fluxes()[0]
+    assert converged and speed < 1e-6
+    g_ = p.gamma
+    shock = normal_shock(HEMI["mach"], g_)
+    m2 = shock.downstream_mach
+    pitot = shock.pressure_ratio * (1 + 0.5 * (g_ - 1) * m2 * m2) ** (g_ / (g_ - 1))
+    wall = face.flux[1] * face.nx + face.flux[2] * face.ny
+    assert abs(wall / pitot - 1) < HEMI["within"]
