@@ -625,6 +625,81 @@ def run_stream(args) -> None:
     }), flush=True)
 
 
+def run_fitted(args) -> None:
+    """The fitted bow shock (bs_fit_*): the Mach 3, 20 deg cone on 4-caliber
+    cylinder at nj = 10 refined 1, 2 and 4 times (drag against Taylor-Maccoll,
+    observed order, the second-order extrapolation), and the Mach 2
+    hemisphere-cylinder at nj = 20 (stagnation-point wall pressure against the
+    pitot value), each settled as the reference's GPU fit settles; `value`
+    counts fitted solves per second of wall time on the GPU. Beside it the
+    oracle's restatement of the fitted iteration (FP64, one host thread) over
+    a bounded sample of the nj = 10 cone's steps."""
+    import math
+
+    import torch
+
+    from bowshock_b200.fitted import CudaFit, blunt_fit_problem, settle, sharp_fit_problem
+    from bowshock_b200.grid import Body, Nose, NoseShape, normal_shock, taylor_maccoll
+    from bowshock_b200.workloads import cone_body
+
+    torch.cuda.set_device(0)
+    exact = taylor_maccoll(3.0, 20 * math.pi / 180, 1.4).surface_pressure_coefficient
+    rows, total_s, fits = [], 0.0, 0
+    errors = []
+    for r in (1, 2, 4):
+        p = sharp_fit_problem(cone_body(20, 4.0), 3.0, nj=10, refinement=r)
+        with CudaFit(p) as g:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            converged, it, speed, drag = settle(g, 60000 * r, check_every=250 * r)
+            dt = time.perf_counter() - t0
+        total_s += dt
+        fits += 1
+        errors.append(drag / exact - 1)
+        rows.append({"case": f"cone 20 deg, Mach 3, refinement {r}", "cells": p.ni * p.nj, "converged": converged,
+                     "steps": it, "max_speed": speed, "drag": drag, "rel_err_vs_taylor_maccoll": drag / exact - 1,
+                     "wall_s": dt, "us_per_step": 1e6 * dt / max(1, it)})
+    order = math.log(abs((errors[0] - errors[1]) / (errors[1] - errors[2]))) / math.log(2)
+    hemi = blunt_fit_problem(Body(Nose(NoseShape("ellipsoid"), 0.5, 0.5), 4.0), 2.0, nj=20)
+    with CudaFit(hemi) as g:
+        t0 = time.perf_counter()
+        converged, it, speed, drag = settle(g, 60000, check_every=250)
+        dt = time.perf_counter() - t0
+        face = g.wall_fluxes()[0]
+    total_s += dt
+    fits += 1
+    s = normal_shock(2.0, 1.4)
+    pitot = s.pressure_ratio * (1 + 0.2 * s.downstream_mach ** 2) ** 3.5
+    rows.append({"case": "hemisphere-cylinder, Mach 2, nj 20", "cells": hemi.ni * hemi.nj, "converged": converged,
+                 "steps": it, "max_speed": speed, "drag": drag,
+                 "stagnation_pressure_rel_err_vs_pitot": (face.flux[1] * face.nx + face.flux[2] * face.ny) / pitot - 1,
+                 "wall_s": dt, "us_per_step": 1e6 * dt / max(1, it)})
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle.shock_fitting import fit_shock
+
+        p = sharp_fit_problem(cone_body(20, 4.0), 3.0, nj=10)
+        sample = 400
+        t0 = time.perf_counter()
+        fit_shock(p, sample)
+        sec = time.perf_counter() - t0
+        cpu = {"value": sample / sec, "unit": "fitted steps/s", "cores": 1, "kind": "port",
+               "sample": f"{sample} fitted steps of the nj = 10 cone (1,890 cells) by oracle/shock_fitting.py, "
+                         "a Python-driven restatement on the FP64 oracle",
+               "gpu_steps_per_s": rows[0]["steps"] / rows[0]["wall_s"]}
+    print(json.dumps({
+        "metric": "fitted bow-shock solves/s (drag settled, shock at rest), one case at a time",
+        "value": fits / total_s, "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "cone 20 deg Mach 3 on 4-caliber cylinder at nj = 10, refined 1, 2, 4; "
+                               "hemisphere-cylinder Mach 2 at nj = 20; SSP-RK2 CFL 0.8 local steps, HLLC, "
+                               "van Albada (shared scaled), axisymmetric"},
+        "fits": rows, "observed_order": order,
+        "extrapolated_rel_err": errors[2] - (errors[1] - errors[2]) / 3,
+        "cpu_baseline": cpu,
+    }), flush=True)
+
+
 def run_gemm(args) -> None:
     """Throughput of the warm-start network's tensor-core GEMM (tcgen05, bf16
     in, FP32 accumulate) on the network's layer shapes at large batches."""
@@ -729,7 +804,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--probe", type=int, default=0,
                     help="run this many LU-SGS steps of the batch with per-kernel timing and exit")
-    ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart", "stream", "gemm", "stencil", "verified"], default="drag-curve")
+    ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart", "stream", "fitted", "gemm", "stencil", "verified"], default="drag-curve")
     ap.add_argument("--train-cases", type=int, default=4096, help="warm start: training seeds")
     ap.add_argument("--eval-cases", type=int, default=512, help="warm start: held-out seeds")
     ap.add_argument("--train-steps", type=int, default=3000, help="warm start: Adam steps")
@@ -764,6 +839,9 @@ def main() -> None:
         return
     if args.workload == "stream":
         run_stream(args)
+        return
+    if args.workload == "fitted":
+        run_fitted(args)
         return
     if args.workload == "gemm":
         run_gemm(args)
