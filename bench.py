@@ -674,6 +674,19 @@ def run_fitted(args) -> None:
                  "steps": it, "max_speed": speed, "drag": drag,
                  "stagnation_pressure_rel_err_vs_pitot": (face.flux[1] * face.nx + face.flux[2] * face.ny) / pitot - 1,
                  "wall_s": dt, "us_per_step": 1e6 * dt / max(1, it)})
+    from bowshock_b200.fitted import verified_fitted_drag
+
+    t0 = time.perf_counter()
+    vf = verified_fitted_drag(cone_body(20, 4.0), 3.0, tolerance=1e-4, max_refinement=8)
+    vdt = time.perf_counter() - t0
+    verified = {"case": "cone 20 deg, Mach 3, base nj 20", "kind": vf.kind, "wall_s": vdt}
+    if vf.result is not None:
+        v = vf.result
+        verified.update({"value": v.estimate.value, "band": v.uncertainty, "verified": v.verified,
+                         "extrapolated": v.estimate.extrapolated, "order": v.estimate.order,
+                         "exact_taylor_maccoll": exact, "exact_inside_band": abs(v.estimate.value - exact) <= v.uncertainty,
+                         "levels": [{"refinement": rep.refinement, "cells": rep.ni * rep.nj, "steps": rep.iterations,
+                                     "drag": rep.drag} for rep in vf.reports]})
     cpu = None
     if not args.no_cpu_baseline:
         from oracle.shock_fitting import fit_shock
@@ -694,7 +707,7 @@ def run_fitted(args) -> None:
         "config": {"workload": "cone 20 deg Mach 3 on 4-caliber cylinder at nj = 10, refined 1, 2, 4; "
                                "hemisphere-cylinder Mach 2 at nj = 20; SSP-RK2 CFL 0.8 local steps, HLLC, "
                                "van Albada (shared scaled), axisymmetric"},
-        "fits": rows, "observed_order": order,
+        "fits": rows, "observed_order": order, "verified_fitted_drag": verified,
         "extrapolated_rel_err": errors[2] - (errors[1] - errors[2]) / 3,
         "cpu_baseline": cpu,
     }), flush=True)

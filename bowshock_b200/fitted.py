@@ -453,3 +453,146 @@ def blunt_fit_problem(asked: Body, mach: float, nj: int = 20, gamma: float = 1.4
             initial[j, i] = captured[jj, i] + t * (captured[jj + 1, i] - captured[jj, i])
     return FitProblem(lines[:, 0].copy(), lines[:, 1].copy(), lines[:, 2].copy(), lines[:, 3].copy(), fractions,
                       heights, nj, R, gamma, mach, free, None, initial.reshape(-1, 4), "symmetry", 0.0)
+
+
+# ---- verified fitted drag -------------------------------------------------------
+
+FITTED_BASE_NJ = 20            # base grid cells across (fitted-flow.ts:1003)
+FALLBACK_COLUMN_DENSITY = 1.5  # a sharp family whose grid fails only the gates, solved again (:70)
+FITTED_DRAG_FLOOR = 7e-5       # systematic error of the fitted drag, relative (src/analysis/verified-drag.ts:132)
+FITTED_NOISE = 1e-8            # the GPU fit's drag settles to this, relative
+FITTED_MIN_ANGLE = 12.0        # the fitted grids' quality gates (src/grid/quality.ts:24-38, 64-68), degrees
+FITTED_MIN_WALL_ANGLE = 50.0
+FITTED_MAX_ASPECT = 13.0
+
+
+class FitNotConverged(Exception):
+    def __init__(self, refinement: int, reason: str):
+        super().__init__(reason)
+        self.refinement = refinement
+
+
+class FitRefused(FitNotConverged):
+    pass
+
+
+class GridRefused(FitRefused):
+    pass
+
+
+def fitted_grid_failure(grid: StructuredGrid) -> str | None:
+    """fittedGridFailure (fitted-flow.ts:293-306): the fitted grids' gates."""
+    from .grid import grid_quality
+
+    q = grid_quality(grid)
+    f = []
+    if not q.min_area > 0:
+        f.append("a cell has non-positive area")
+    if not q.min_angle >= FITTED_MIN_ANGLE * math.pi / 180:
+        f.append(f"cell angle {math.degrees(q.min_angle):.1f} deg below {FITTED_MIN_ANGLE:.1f} deg")
+    if not q.min_wall_angle >= FITTED_MIN_WALL_ANGLE * math.pi / 180:
+        f.append(f"wall cell angle {math.degrees(q.min_wall_angle):.1f} deg below {FITTED_MIN_WALL_ANGLE:.1f} deg")
+    if not q.max_size_ratio <= FITTED_MAX_SIZE_RATIO:
+        f.append(f"neighbouring cells differ in size by {q.max_size_ratio:.2f} (limit {FITTED_MAX_SIZE_RATIO:g})")
+    if not q.max_aspect_ratio <= FITTED_MAX_ASPECT:
+        f.append(f"cell aspect ratio {q.max_aspect_ratio:.1f} above {FITTED_MAX_ASPECT:g}")
+    if not f:
+        return None
+    return f"the grid on the fitted shock fails its quality checks ({'; '.join(f)}): a limit of the present grids"
+
+
+def base_mach(problem: FitProblem, asked_end: float, prims: np.ndarray) -> float:
+    """baseMach (fitted-flow.ts:262-291): the smallest axial Mach number
+    across the layer at the end of the body asked for (infinite if the
+    domain ends there). prims (nj, ni, 4)."""
+    x = problem.line_x
+    n = len(x) - 1
+    tol = 1e-12 * abs(asked_end)
+    if not x[n] > asked_end + tol:
+        return math.inf
+    g = problem.gamma
+    axial = prims[:, :, 1] / np.sqrt(g * prims[:, :, 3] / prims[:, :, 0])     # (nj, ni)
+    hit = np.nonzero(np.abs(x - asked_end) <= tol)[0]
+    if len(hit) and hit[0] > 0:
+        return float(axial[:, hit[0] - 1].min())
+    centre = 0.5 * (x[:-1] + x[1:])
+    a = 0
+    while a + 2 < n and centre[a + 1] <= asked_end:
+        a += 1
+    t = min(max((asked_end - centre[a]) / (centre[a + 1] - centre[a]), 0.0), 1.0)
+    return float(((1 - t) * axial[:, a] + t * axial[:, a + 1]).min())
+
+
+def fitted_case_failure(problem: FitProblem, asked_end: float, grid: StructuredGrid, prims: np.ndarray) -> str | None:
+    """fittedCaseFailure (fitted-flow.ts:308-330): the grid's gates, a
+    supersonic outflow and a supersonic flow at the end of the body asked for."""
+    e = fitted_grid_failure(grid)
+    if e is not None:
+        return e
+    g = problem.gamma
+    last = prims[:, -1]
+    outflow = float((last[:, 1] / np.sqrt(g * last[:, 3] / last[:, 0])).min())
+    if not outflow > 1:
+        return f"the flow leaves the grid at an axial Mach number of {outflow:.3f}, where the outflow condition does not hold"
+    base = base_mach(problem, asked_end, prims)
+    if not base > 1:
+        return f"the flow at the end of the body is subsonic (axial Mach number {base:.3f}), so what lies behind it could reach the body"
+    return None
+
+
+def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance: float = 1e-4,
+                         max_refinement: int = 8, floor: float = FITTED_DRAG_FLOOR,
+                         iterations_per_refinement: int = 60000, on_level=None):
+    """verifiedFittedDrag (fitted-flow.ts:1005-1075) for sharp noses, on the
+    GPU fit: grids refined by 2 from 20 cells across until the drag's band
+    (grid convergence index plus `floor`) is within `tolerance`; a grid
+    whose fit does not settle, or whose flow fails the checks, stops the run
+    without a value, but a family whose grid fails only the quality gates is
+    solved again with 1.5 times as many columns. Returns a
+    verified_drag.VerifiedDrag."""
+    from .verification import refine_until_verified
+    from .verified_drag import LevelReport, VerifiedDrag
+
+    asked_end = body.nose.length + body.cylinder_length
+    reports: list = []
+
+    def family(density: float):
+        def solve_at(r: int) -> float:
+            p = sharp_fit_problem(body, mach, nj=FITTED_BASE_NJ, refinement=r, gamma=gamma, column_density=density)
+            with CudaFit(p) as g:
+                converged, it, speed, drag = settle(g, iterations_per_refinement * r, check_every=250 * r)
+                if not converged:
+                    raise FitNotConverged(r, f"the fit stopped after {it} iterations with the shock moving at "
+                                             f"{speed:.1e} of the sound speed")
+                x = np.empty((p.ni + 1) * (p.nj + 1))
+                y = np.empty_like(x)
+                g._call("bs_fit_nodes", x.ctypes.data_as(C.POINTER(C.c_double)),
+                        y.ctypes.data_as(C.POINTER(C.c_double)))
+                grid = StructuredGrid(p.ni, p.nj, x, y)
+                prims = g.primitives().reshape(p.nj, p.ni, 4)
+            e = fitted_grid_failure(grid)
+            if e is not None:
+                raise GridRefused(r, e)
+            e = fitted_case_failure(p, asked_end, grid, prims)
+            if e is not None:
+                raise FitRefused(r, e)
+            rep = LevelReport(r, p.ni, p.nj, it, drag)
+            reports.append(rep)
+            if on_level is not None:
+                on_level(rep)
+            return drag
+
+        return refine_until_verified(solve_at, tolerance, floor, max_refinement, 0.5, FITTED_NOISE)
+
+    try:
+        try:
+            return VerifiedDrag("solved", family(1.0), reports)
+        except GridRefused:
+            reports.clear()
+            return VerifiedDrag("solved", family(FALLBACK_COLUMN_DENSITY), reports)
+    except FitRefused as e:
+        return VerifiedDrag("invalid", None, reports, e.refinement, str(e))
+    except FitNotConverged as e:
+        return VerifiedDrag("not-converged", None, reports, e.refinement, str(e))
+    except ValueError as e:
+        return VerifiedDrag("invalid", None, reports, 1, str(e))

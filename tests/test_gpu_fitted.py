@@ -113,3 +113,21 @@ def test_hemisphere_stagnation_pressure_is_the_pitot_value():
     pitot = shock.pressure_ratio * (1 + 0.5 * (g_ - 1) * m2 * m2) ** (g_ / (g_ - 1))
     wall = face.flux[1] * face.nx + face.flux[2] * face.ny
     assert abs(wall / pitot - 1) < HEMI["within"]
+
+
+def test_verified_fitted_drag_of_the_cone_contains_the_exact_drag():
+    # verifiedFittedDrag (src/analysis/fitted-flow.ts:1005-1075) on the GPU
+    # fit: grids of 20 cells across refined by 2 until the band is within
+    # 1e-4; the Taylor-Maccoll drag of the cone lies inside the band.
+    from bowshock_b200.fitted import verified_fitted_drag
+
+    b = GOLDEN["body"]
+    exact = taylor_maccoll(GOLDEN["mach"], b["half_angle_deg"] * math.pi / 180, 1.4).surface_pressure_coefficient
+    out = verified_fitted_drag(cone_body(b["half_angle_deg"], b["cylinder"]), GOLDEN["mach"], tolerance=1e-4,
+                               max_refinement=8)
+    assert out.kind == "solved", out.reason
+    v = out.result
+    assert v.verified and v.uncertainty <= 1e-4
+    assert abs(v.estimate.value - exact) <= v.uncertainty
+    assert [r for r, _ in v.levels] == [1, 2, 4, 8][:len(v.levels)] and len(v.levels) >= 4
+    assert abs(v.estimate.extrapolated - exact) < 2e-5 * exact
