@@ -674,7 +674,29 @@ def run_fitted(args) -> None:
                  "steps": it, "max_speed": speed, "drag": drag,
                  "stagnation_pressure_rel_err_vs_pitot": (face.flux[1] * face.nx + face.flux[2] * face.ny) / pitot - 1,
                  "wall_s": dt, "us_per_step": 1e6 * dt / max(1, it)})
-    from bowshock_b200.fitted import verified_fitted_drag
+    from bowshock_b200.fitted import settle_many, verified_fitted_drag
+    from bowshock_b200.workloads import drag_sweep_machs, ogive_body
+
+    # The drag curve of the headline's tangent ogive, fitted: 16 Mach numbers
+    # at once, one stream each, against the same fits one after another.
+    curve_problems = [sharp_fit_problem(ogive_body(3.0, 4.0), m, nj=20) for m in drag_sweep_machs()]
+    curve_fits = [CudaFit(p) for p in curve_problems]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    outs = settle_many(curve_fits, 60000, check_every=250)
+    concurrent_s = time.perf_counter() - t0
+    for f in curve_fits:
+        f.destroy()
+    one = CudaFit(curve_problems[0])
+    t0 = time.perf_counter()
+    settle(one, 60000, check_every=250)
+    single_s = time.perf_counter() - t0
+    one.destroy()
+    curve = {"case": "tangent ogive fineness 3 + 4-caliber cylinder, Mach 1.5..3.0 (16), nj 20",
+             "cells": curve_problems[0].ni * curve_problems[0].nj, "converged": sum(1 for o in outs if o[0]),
+             "wall_s": concurrent_s, "solves_per_s": len(outs) / concurrent_s,
+             "single_first_case_wall_s": single_s, "steps": [o[1] for o in outs],
+             "drags": [o[3] for o in outs]}
 
     t0 = time.perf_counter()
     vf = verified_fitted_drag(cone_body(20, 4.0), 3.0, tolerance=1e-4, max_refinement=8)
@@ -707,7 +729,7 @@ def run_fitted(args) -> None:
         "config": {"workload": "cone 20 deg Mach 3 on 4-caliber cylinder at nj = 10, refined 1, 2, 4; "
                                "hemisphere-cylinder Mach 2 at nj = 20; SSP-RK2 CFL 0.8 local steps, HLLC, "
                                "van Albada (shared scaled), axisymmetric"},
-        "fits": rows, "observed_order": order, "verified_fitted_drag": verified,
+        "fits": rows, "observed_order": order, "verified_fitted_drag": verified, "fitted_drag_curve": curve,
         "extrapolated_rel_err": errors[2] - (errors[1] - errors[2]) / 3,
         "cpu_baseline": cpu,
     }), flush=True)

@@ -542,7 +542,7 @@ def fitted_case_failure(problem: FitProblem, asked_end: float, grid: StructuredG
 
 def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance: float = 1e-4,
                          max_refinement: int = 8, floor: float = FITTED_DRAG_FLOOR,
-                         iterations_per_refinement: int = 60000, on_level=None):
+                         iterations_per_refinement: int = 200000, on_level=None, on_fallback=None):
     """verifiedFittedDrag (fitted-flow.ts:1005-1075) for sharp noses, on the
     GPU fit: grids refined by 2 from 20 cells across until the drag's band
     (grid convergence index plus `floor`) is within `tolerance`; a grid
@@ -587,12 +587,26 @@ def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance:
     try:
         try:
             return VerifiedDrag("solved", family(1.0), reports)
-        except GridRefused:
+        except GridRefused as e:
+            if on_fallback is not None:
+                on_fallback(e.refinement, str(e))
             reports.clear()
-            return VerifiedDrag("solved", family(FALLBACK_COLUMN_DENSITY), reports)
+            return VerifiedDrag("solved", family(FALLBACK_COLUMN_DENSITY), reports,
+                                column_density=FALLBACK_COLUMN_DENSITY)
     except FitRefused as e:
         return VerifiedDrag("invalid", None, reports, e.refinement, str(e))
     except FitNotConverged as e:
         return VerifiedDrag("not-converged", None, reports, e.refinement, str(e))
     except ValueError as e:
         return VerifiedDrag("invalid", None, reports, 1, str(e))
+
+
+def settle_many(fits: list[CudaFit], max_iterations: int, noise: float = 1e-8, speed_tolerance: float = 1e-6,
+                check_every: int = 250) -> list:
+    """settle() for many fits at once, one host thread each: every fit has
+    its own stream and its calls release the interpreter lock, so their
+    small, launch-bound steps overlap on the GPU."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=max(1, len(fits))) as pool:
+        return list(pool.map(lambda f: settle(f, max_iterations, noise, speed_tolerance, check_every), fits))

@@ -66,6 +66,7 @@ class VerifiedDrag:
     reports: list[LevelReport] = field(default_factory=list)
     refinement: int | None = None
     reason: str | None = None
+    column_density: float | None = None   # fitted families solved with more columns than usual
 
 
 def outflow_mach(gamma: float, ni: int, nj: int, cell) -> float:

@@ -133,6 +133,33 @@ def main() -> None:
         "measured_rel_err": float(hm.group(1)) / 100, "captured_rel_err": float(hm.group(3)) / 100,
         "within": float(tol.group(1)),
     }
+    # The 3-caliber tangent ogive: at Mach 1.35 (axially subsonic tip) the
+    # page's family and its coarser one; at Mach 1.5 on 30 calibers of
+    # cylinder the fallback to more columns.
+    fam = re.search(r"nj = 20 to 160.*?converged to 1e-10 of its drag\):\s*([0-9.]+), ([0-9.]+),\s*//\s*([0-9.]+), "
+                    r"([0-9.]+), at orders.*?extrapolated\s*//\s*to ([0-9.]+)", t, re.S)
+    coarse = re.search(r"\+([0-9.e-]+) and \+([0-9.e-]+) of that value, falling by ([0-9]+\.[0-9]+)", t)
+    ob = re.search(r"expect\(fine\)\.toBeLessThan\(([0-9e.-]+)\);\s*expect\(coarse / fine\)\.toBeGreaterThan\(([0-9.]+)\);"
+                   r"\s*expect\(coarse / fine\)\.toBeLessThan\(([0-9.]+)\);", t)
+    base = re.search(r"expect\(result\.levels\[0\]!\.value\)\.toBe\(([0-9.]+)\)", t)
+    out["fitted_ogive_mach1_35"] = {
+        "source": f"{f}:{find_line(t, 'Mach 1.35, 3-caliber tangent ogive')}",
+        "body": {"shape": "ogive", "parameter": 1, "length": 3, "base_radius": 0.5, "cylinder": 2},
+        "mach": 1.35, "family_nj20": [float(fam.group(k)) for k in range(1, 5)],
+        "extrapolated": float(fam.group(5)),
+        "coarse_family_nj10_rel": [float(coarse.group(1)), float(coarse.group(2))],
+        "coarse_family_ratio": float(coarse.group(3)),
+        "fine_below": float(ob.group(1)), "ratio_above": float(ob.group(2)), "ratio_below": float(ob.group(3)),
+        "verified_nj20_value": float(base.group(1)),
+    }
+    fb = re.search(r"aspect ratio of ([0-9.]+) \(measured\s*//\s*when written\), above the (\d+) allowed", t)
+    fv = re.search(r"Measured when written: ([0-9.]+) on (\d+) columns", t)
+    out["fitted_ogive_fallback_mach1_5"] = {
+        "source": f"{f}:{find_line(t, 'a sharp nose whose usual grid fails only the quality gates')}",
+        "body": {"shape": "ogive", "parameter": 1, "length": 3, "base_radius": 0.5, "cylinder": 30},
+        "mach": 1.5, "aspect_ratio": float(fb.group(1)), "aspect_limit": int(fb.group(2)),
+        "value": float(fv.group(1)), "columns": int(fv.group(2)), "equal_within": 1e-12,
+    }
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {OUT}")
 
