@@ -5,18 +5,18 @@
 //                        the two cells below it (compatibleShock, :87-111):
 //                        its post-shock state fills the ghosts, its physical
 //                        flux is imposed on the face, its speed is kept;
-//   (the explicit step, with those held)
+//   (the explicit step, with those held; its last stage writes q_old)
 //   fit_move_kernel      one block: each shock node moves along its line by
 //                        W dt / (n . line), W from the face on its axis side,
 //                        dt half the top cell's height over its fastest
 //                        signal; the axis node keeps the shock normal to the
 //                        axis ('symmetry') or stays ('fixed');
-//   fit_nodes_kernel, fit_metrics_kernel  the grid on the new heights (each
-//                        node at its fixed fraction of its line's height)
-//                        and its metrics, FP64 computed, stored as the solver
-//                        stores them (src/grid/structured.ts:94-168);
-//   fit_remap_kernel     the flow interpolated along the lines onto the new
-//                        grid (remapAlongLines, :324-358).
+//   fit_regrid_kernel    the grid on the new heights (each node at its fixed
+//                        fraction of its line's height) and its metrics,
+//                        FP64 computed, stored as the solver stores them
+//                        (src/grid/structured.ts:94-168), and the flow
+//                        interpolated along the lines onto it
+//                        (remapAlongLines, :324-358), in one launch.
 // Everything is FP64 except the stored face and cell metrics (FP32, as for
 // every grid here).
 #pragma once
@@ -48,8 +48,8 @@ struct FitArgs {
   float4* jface;
   float2* cellm;
   double* bgeom;             // boundary faces iMin, iMax, jMin, jMax: (nx, ny, area)
-  StateView<double> q;       // the state
-  StateView<double> q_old;   // a copy of it before the remap
+  StateView<double> q;       // the state at the start of a step, and after the remap
+  StateView<double> q_old;   // the state after the step's last stage, on the grid before the move
 };
 
 __device__ __forceinline__ void fit_shock_state(const FitArgs& A, double mach, double nx, double ny, double w[4],
@@ -78,8 +78,8 @@ __device__ __forceinline__ void fit_top_normal(const FitArgs& A, int i, double* 
   *ny = len > 0 ? -dx / len : 0;
 }
 
-__device__ __forceinline__ Prim<double> fit_prim(const FitArgs& A, int i, int j) {
-  return to_prim(A.q.load(int64_t(i) + int64_t(j) * A.ni), A.gamma);
+__device__ __forceinline__ Prim<double> fit_prim(const FitArgs& A, const StateView<double>& q, int i, int j) {
+  return to_prim(q.load(int64_t(i) + int64_t(j) * A.ni), A.gamma);
 }
 
 __global__ void fit_boundary_kernel(const FitArgs A) {
@@ -87,7 +87,7 @@ __global__ void fit_boundary_kernel(const FitArgs A) {
   if (i >= A.ni) return;
   double nx, ny;
   fit_top_normal(A, i, &nx, &ny);
-  const Prim<double> c1 = fit_prim(A, i, A.nj - 1), c2 = fit_prim(A, i, A.nj - 2);
+  const Prim<double> c1 = fit_prim(A, A.q, i, A.nj - 1), c2 = fit_prim(A, A.q, i, A.nj - 2);
   const double g = A.gamma;
   const double impedance = c1.rho * sqrt(g * c1.p / c1.rho);
   const double p_face = 1.5 * c1.p - 0.5 * c2.p;
@@ -100,18 +100,29 @@ __global__ void fit_boundary_kernel(const FitArgs A) {
   };
   double mach = 1;
   if (mismatch(1.0) < 0) {
-    double low = 1, high = 2;
-    // The mismatch grows as M^2: a finite bracket is found in a few
-    // doublings (the bound only guards non-finite inputs).
-    for (int k = 0; k < 64 && mismatch(high) < 0; k++) high *= 2;
-    for (int k = 0; k < 100 && high - low > 1e-15 * high; k++) {
-      const double mid = 0.5 * (low + high);
-      if (mismatch(mid) < 0)
-        low = mid;
+    // The root of the increasing mismatch, where the reference bisects from
+    // [1, 2] (doubling the top) to a bracket of 1e-15 of its top: Newton
+    // steps kept inside the bracket that every evaluation narrows, halving
+    // it instead where a step would leave it, to the same width. The
+    // mismatch's derivative: dp_s/dM = p 4 gamma M / (gamma + 1) and
+    // du_n,s/dM = 2 a (1 + 1 / M^2) / (gamma + 1).
+    const double gp1 = g + 1;
+    double low = 1, high = INFINITY, m = 1;
+    for (int k = 0; k < 200; k++) {
+      const double f = mismatch(m);
+      if (f == 0) break;  // the root itself
+      if (f < 0)
+        low = m;
       else
-        high = mid;
+        high = m;
+      if (high < INFINITY && high - low <= 1e-15 * high) break;
+      const double df = A.free[3] * 4 * g * m / gp1 + impedance * 2 * A.a_free * (1 + 1 / (m * m)) / gp1;
+      double next = m - f / df;
+      if (next == m) break;  // a step below the last bit
+      if (!(next > low && next < high)) next = high < INFINITY ? 0.5 * (low + high) : 2 * low;
+      m = next;
     }
-    mach = 0.5 * (low + high);
+    mach = m;
   }
   fit_shock_state(A, mach, nx, ny, w, &speed, &un);
   const double energy = w[3] / (g - 1) + 0.5 * w[0] * (w[1] * w[1] + w[2] * w[2]);
@@ -130,7 +141,7 @@ __global__ void fit_boundary_kernel(const FitArgs A) {
 }
 
 // One block: the new heights from the last boundary's speeds and the flow
-// after the step, on the grid before the move.
+// after the step (q_old), on the grid before the move.
 __global__ void fit_move_kernel(const FitArgs A) {
   __shared__ double worst[32];
   const int ni = A.ni, nj = A.nj;
@@ -141,7 +152,7 @@ __global__ void fit_move_kernel(const FitArgs A) {
     const int f = k - 1;
     double nx, ny;
     fit_top_normal(A, f, &nx, &ny);
-    const Prim<double> cell = fit_prim(A, min(k, ni - 1), nj - 1);
+    const Prim<double> cell = fit_prim(A, A.q_old, min(k, ni - 1), nj - 1);
     const int64_t top = k + int64_t(nj) * (ni + 1), below = k + int64_t(nj - 1) * (ni + 1);
     const double height = hypot(A.nx_[top] - A.nx_[below], A.ny_[top] - A.ny_[below]);
     const double dt = (0.5 * height) / (hypot(cell.u, cell.v) + sqrt(g * cell.p / cell.rho));
@@ -176,49 +187,59 @@ __global__ void fit_move_kernel(const FitArgs A) {
   }
 }
 
-// Nodes on the lines at the current heights (gridOnLines, src/grid/blunt-grid.ts:602-620).
-__global__ void fit_nodes_kernel(const FitArgs A) {
-  const int64_t n = int64_t(A.ni + 1) * (A.nj + 1);
-  for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x) {
-    const int i = int(k % (A.ni + 1)), j = int(k / (A.ni + 1));
-    const double* l = A.line + 4 * i;
-    const double d = A.heights[i] * A.fraction[int64_t(i) * (A.nj + 1) + j];
-    A.nx_[k] = l[0] + d * l[2];
-    A.ny_[k] = l[1] + d * l[3];
-  }
+// Node (i, j) on its line at the current heights (gridOnLines,
+// src/grid/blunt-grid.ts:602-620).
+__device__ __forceinline__ void fit_node(const FitArgs& A, int i, int j, double* x, double* y) {
+  const double* l = A.line + 4 * i;
+  const double d = A.heights[i] * A.fraction[int64_t(i) * (A.nj + 1) + j];
+  *x = l[0] + d * l[2];
+  *y = l[1] + d * l[3];
 }
 
-// Metrics of the grid (computeMetrics, src/grid/structured.ts:94-168): i-faces,
-// j-faces and cells in one pass over a flat index, and the boundary faces'
-// FP64 geometry for the wall fluxes.
-__global__ void fit_metrics_kernel(const FitArgs A) {
+// The grid on the new heights and, with `remap`, the flow on it, in one
+// pass over a flat index: the nodes; the metrics (computeMetrics,
+// src/grid/structured.ts:94-168), i-faces, j-faces and cells, FP64 computed
+// from the node positions evaluated here, stored FP32, with the boundary
+// faces' FP64 geometry for the wall fluxes; and the remap along the lines
+// (remapAlongLines, src/solver/shock-fitting.ts:324-358), linear in the
+// primitives between the old cell centres of the column, held at the end
+// cells beyond them, from q_old into q (a node's distance along its line is
+// its height times its fraction: the lines' directions are unit vectors).
+__global__ void fit_regrid_kernel(const FitArgs A, int remap) {
   const int ni = A.ni, nj = A.nj;
-  const int64_t nif = int64_t(ni + 1) * nj, njf = int64_t(ni) * (nj + 1), nc = int64_t(ni) * nj;
-  auto node = [&](int i, int j) { return int64_t(i) + int64_t(j) * (ni + 1); };
-  auto face = [&](int64_t a, int64_t b, double* fx, double* fy, double* fa) {
-    const double dx = A.nx_[b] - A.nx_[a], dy = A.ny_[b] - A.ny_[a];
+  const int64_t nn = int64_t(ni + 1) * (nj + 1), nif = int64_t(ni + 1) * nj, njf = int64_t(ni) * (nj + 1),
+                nc = int64_t(ni) * nj;
+  const int64_t total = nn + nif + njf + nc + (remap ? nc : 0);
+  auto face = [&](int ia, int ja, int ib, int jb, double* fx, double* fy, double* fa) {
+    double xa, ya, xb, yb;
+    fit_node(A, ia, ja, &xa, &ya);
+    fit_node(A, ib, jb, &xb, &yb);
+    const double dx = xb - xa, dy = yb - ya;
     const double length = hypot(dx, dy);
     *fx = length > 0 ? dy / length : 0;
     *fy = length > 0 ? -dx / length : 0;
-    *fa = A.axisym ? length * 0.5 * (A.ny_[a] + A.ny_[b]) : length;
+    *fa = A.axisym ? length * 0.5 * (ya + yb) : length;
   };
-  for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < nif + njf + nc;
-       k += int64_t(gridDim.x) * blockDim.x) {
+  for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < total; k += int64_t(gridDim.x) * blockDim.x) {
     double fx, fy, fa;
-    if (k < nif) {
+    if (k < nn) {
       const int i = int(k % (ni + 1)), j = int(k / (ni + 1));
-      face(node(i, j), node(i, j + 1), &fx, &fy, &fa);
-      A.iface[k] = make_float4(float(fx), float(fy), float(fa), 0.f);
+      fit_node(A, i, j, &A.nx_[k], &A.ny_[k]);
+    } else if (k < nn + nif) {
+      const int64_t m = k - nn;
+      const int i = int(m % (ni + 1)), j = int(m / (ni + 1));
+      face(i, j, i, j + 1, &fx, &fy, &fa);
+      A.iface[m] = make_float4(float(fx), float(fy), float(fa), 0.f);
       if (i == 0 || i == ni) {
         double* g = A.bgeom + 3 * ((i == 0 ? 0 : nj) + j);
         g[0] = fx;
         g[1] = fy;
         g[2] = fa;
       }
-    } else if (k < nif + njf) {
-      const int64_t m = k - nif;
+    } else if (k < nn + nif + njf) {
+      const int64_t m = k - nn - nif;
       const int i = int(m % ni), j = int(m / ni);
-      face(node(i + 1, j), node(i, j), &fx, &fy, &fa);
+      face(i + 1, j, i, j, &fx, &fy, &fa);
       A.jface[m] = make_float4(float(fx), float(fy), float(fa), 0.f);
       if (j == 0 || j == nj) {
         double* g = A.bgeom + 3 * (2 * nj + (j == 0 ? 0 : ni) + i);
@@ -226,48 +247,42 @@ __global__ void fit_metrics_kernel(const FitArgs A) {
         g[1] = fy;
         g[2] = fa;
       }
-    } else {
-      const int64_t m = k - nif - njf;
+    } else if (k < nn + nif + njf + nc) {
+      const int64_t m = k - nn - nif - njf;
       const int i = int(m % ni), j = int(m / ni);
-      const int64_t c[4] = {node(i, j), node(i + 1, j), node(i + 1, j + 1), node(i, j + 1)};
+      double cx[4], cy[4];
+      fit_node(A, i, j, &cx[0], &cy[0]);
+      fit_node(A, i + 1, j, &cx[1], &cy[1]);
+      fit_node(A, i + 1, j + 1, &cx[2], &cy[2]);
+      fit_node(A, i, j + 1, &cx[3], &cy[3]);
       double area = 0, sy = 0;
       for (int e = 0; e < 4; e++) {
-        const int64_t p = c[e], r = c[(e + 1) % 4];
-        const double cross = A.nx_[p] * A.ny_[r] - A.nx_[r] * A.ny_[p];
+        const int r = (e + 1) % 4;
+        const double cross = cx[e] * cy[r] - cx[r] * cy[e];
         area += cross;
-        sy += (A.ny_[p] + A.ny_[r]) * cross;
+        sy += (cy[e] + cy[r]) * cross;
       }
       area *= 0.5;
-      const double cy = sy / (6 * area);
-      A.cellm[m] = make_float2(float(A.axisym ? area * cy : area), float(area));
+      const double ycen = sy / (6 * area);
+      A.cellm[m] = make_float2(float(A.axisym ? area * ycen : area), float(area));
+    } else {
+      const int64_t m = k - nn - nif - njf - nc;
+      const int i = int(m % ni), j = int(m / ni);
+      const double* f0 = A.fraction + int64_t(i) * (nj + 1);
+      const double* f1 = A.fraction + int64_t(i + 1) * (nj + 1);
+      auto column = [&](const double* h, int jj) { return 0.5 * (h[i] * f0[jj] + h[i + 1] * f1[jj]); };
+      const double d = 0.5 * (column(A.heights, j) + column(A.heights, j + 1));
+      auto centre = [&](int jj) { return 0.5 * (column(A.heights_old, jj) + column(A.heights_old, jj + 1)); };
+      int jj = 0;
+      while (jj < nj - 2 && centre(jj + 1) < d) jj++;
+      const double c0 = centre(jj), c1 = centre(jj + 1);
+      const double t = fmin(fmax((d - c0) / (c1 - c0), 0.0), 1.0);
+      const Prim<double> a = to_prim(A.q_old.load(int64_t(i) + int64_t(jj) * ni), A.gamma);
+      const Prim<double> b = to_prim(A.q_old.load(int64_t(i) + int64_t(jj + 1) * ni), A.gamma);
+      const Prim<double> w{a.rho + t * (b.rho - a.rho), a.u + t * (b.u - a.u), a.v + t * (b.v - a.v),
+                           a.p + t * (b.p - a.p)};
+      A.q.store(m, to_cons(w, A.gamma));
     }
-  }
-}
-
-// The flow on the new grid from the copy on the old one, along the lines
-// (remapAlongLines, src/solver/shock-fitting.ts:324-358): linear in the
-// primitives between the old cell centres of the column, held at the end
-// cells beyond them. A node's distance along its line is its height times
-// its fraction (the lines' directions are unit vectors).
-__global__ void fit_remap_kernel(const FitArgs A) {
-  const int ni = A.ni, nj = A.nj;
-  const int64_t n = int64_t(ni) * nj;
-  for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x) {
-    const int i = int(k % ni), j = int(k / ni);
-    const double* f0 = A.fraction + int64_t(i) * (nj + 1);
-    const double* f1 = A.fraction + int64_t(i + 1) * (nj + 1);
-    auto column = [&](const double* h, int jj) { return 0.5 * (h[i] * f0[jj] + h[i + 1] * f1[jj]); };
-    const double d = 0.5 * (column(A.heights, j) + column(A.heights, j + 1));
-    auto centre = [&](int jj) { return 0.5 * (column(A.heights_old, jj) + column(A.heights_old, jj + 1)); };
-    int jj = 0;
-    while (jj < nj - 2 && centre(jj + 1) < d) jj++;
-    const double c0 = centre(jj), c1 = centre(jj + 1);
-    const double t = fmin(fmax((d - c0) / (c1 - c0), 0.0), 1.0);
-    const Prim<double> a = to_prim(A.q_old.load(int64_t(i) + int64_t(jj) * ni), A.gamma);
-    const Prim<double> b = to_prim(A.q_old.load(int64_t(i) + int64_t(jj + 1) * ni), A.gamma);
-    const Prim<double> w{a.rho + t * (b.rho - a.rho), a.u + t * (b.u - a.u), a.v + t * (b.v - a.v),
-                         a.p + t * (b.p - a.p)};
-    A.q.store(k, to_cons(w, A.gamma));
   }
 }
 

@@ -1,8 +1,10 @@
 // One case solved with its bow shock fitted as the outer boundary, all of it
 // on the GPU: the fitted-shock iteration of src/solver/shock-fitting.ts:
-// 170-314 (device/fitted.cuh) around the explicit steps of the cell kernel,
-// replayed from captured CUDA graphs of 16 steps, with the host reading the
-// shock's speed and the residual at checks. C ABI: bs_fit_*.
+// 170-314 (device/fitted.cuh) around the explicit steps of the cell kernel:
+// a step is five launches (the shock boundary, two SSP-RK2 stages, the
+// shock's move, the new grid with the remap), replayed from captured CUDA
+// graphs of 16 steps, with the host reading the shock's speed and the
+// residual at checks. C ABI: bs_fit_*.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -108,6 +110,7 @@ class FittedSolver {
       FIT_CUDA(q_[v].alloc(nc));
       FIT_CUDA(s1_[v].alloc(nc));
       FIT_CUDA(old_[v].alloc(nc));
+      if (cfg.integrator != BS_SSPRK2) FIT_CUDA(s2_[v].alloc(nc));
     }
     FIT_CUDA(dt_.alloc(nc));
     FIT_CUDA(iface_.alloc(size_t(ni + 1) * nj));
@@ -388,10 +391,13 @@ class FittedSolver {
 
   int blocks(int64_t n) const { return int(std::min<int64_t>((n + 255) / 256, 4096)); }
 
-  bs_status launch_grid() {
-    bsd::fit_nodes_kernel<<<blocks(int64_t(ni_ + 1) * (nj_ + 1)), 256, 0, stream_>>>(A_);
-    const int64_t all = int64_t(ni_ + 1) * nj_ + int64_t(ni_) * (nj_ + 1) + int64_t(ni_) * nj_;
-    bsd::fit_metrics_kernel<<<blocks(all), 256, 0, stream_>>>(A_);
+  // The grid on the current heights and its metrics; with `remap`, the flow
+  // in q_old interpolated onto it into q.
+  bs_status launch_grid(bool remap = false) {
+    const int64_t nc = int64_t(ni_) * nj_;
+    const int64_t all = int64_t(ni_ + 1) * (nj_ + 1) + int64_t(ni_ + 1) * nj_ + int64_t(ni_) * (nj_ + 1) + nc +
+                        (remap ? nc : 0);
+    bsd::fit_regrid_kernel<<<blocks(all), 256, 0, stream_>>>(A_, remap ? 1 : 0);
     FIT_CUDA(cudaGetLastError());
     return BS_OK;
   }
@@ -439,26 +445,22 @@ class FittedSolver {
 
   bs_status record_step() {
     FIT_TRY(launch_boundary());
+    // The step's last stage writes the state on the grid before the move
+    // (q_old), which the move reads and the remap carries into q.
     const bsd::StateView<double> q = q_view(), s1 = s1_view();
+    const bsd::StateView<double> old = {old_[0].p, old_[1].p, old_[2].p, old_[3].p};
     if (integrator_ == BS_SSPRK2) {
       FIT_TRY(launch_tile<bsd::MODE_STAGE>(q, s1, 0, 1, true, nullptr));
-      FIT_TRY(launch_tile<bsd::MODE_STAGE>(s1, q, 0.5, 0.5, false, nullptr));
+      FIT_TRY(launch_tile<bsd::MODE_STAGE>(s1, old, 0.5, 0.5, false, nullptr));
     } else {
-      // SSP-RK3 through s1 and the old-state buffer as the second stage.
-      const bsd::StateView<double> s2 = {old_[0].p, old_[1].p, old_[2].p, old_[3].p};
+      const bsd::StateView<double> s2 = {s2_[0].p, s2_[1].p, s2_[2].p, s2_[3].p};
       FIT_TRY(launch_tile<bsd::MODE_STAGE>(q, s1, 0, 1, true, nullptr));
       FIT_TRY(launch_tile<bsd::MODE_STAGE>(s1, s2, 0.75, 0.25, false, nullptr));
-      FIT_TRY(launch_tile<bsd::MODE_STAGE>(s2, q, 1.0 / 3.0, 2.0 / 3.0, false, nullptr));
+      FIT_TRY(launch_tile<bsd::MODE_STAGE>(s2, old, 1.0 / 3.0, 2.0 / 3.0, false, nullptr));
     }
     bsd::fit_move_kernel<<<1, 256, 0, stream_>>>(A_);
     FIT_CUDA(cudaGetLastError());
-    FIT_TRY(launch_grid());
-    const size_t nc = size_t(ni_) * nj_;
-    for (int v = 0; v < 4; v++)
-      FIT_CUDA(cudaMemcpyAsync(old_[v].p, q_[v].p, nc * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-    bsd::fit_remap_kernel<<<blocks(int64_t(nc)), 256, 0, stream_>>>(A_);
-    FIT_CUDA(cudaGetLastError());
-    return BS_OK;
+    return launch_grid(true);
   }
 
   int ni_ = 0, nj_ = 0, n_tiles_ = 0, integrator_ = 0, iterations_ = 0;
@@ -469,7 +471,7 @@ class FittedSolver {
   Buf<bsd::CaseDev> case_;
   Buf<int2> tiles_;
   Buf<double> line_, fraction_, heights_, heights_old_, heights_next_, x_, y_;
-  Buf<double> q_[4], s1_[4], old_[4];
+  Buf<double> q_[4], s1_[4], s2_[4], old_[4];
   Buf<float> dt_;
   Buf<float4> iface_, jface_;
   Buf<float2> cellm_;

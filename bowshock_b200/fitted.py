@@ -330,14 +330,15 @@ class CudaFit:
         return d.value + self.problem.tip_drag
 
 
-def settle(fit: CudaFit, max_iterations: int, noise: float = 1e-8, speed_tolerance: float = 1e-6,
+def settle(fit: CudaFit, max_iterations: int, noise: float = 1e-7, speed_tolerance: float = 1e-6,
            check_every: int = 250):
     """The GPU fit's stopping rule (fitShockGpu, src/engine-gpu/shock-fitting-gpu.ts:
     135-170): every `check_every` steps the drag is added to a SettlingValue of
     `noise`; the fit has converged once the drag has settled and the shock
     moves slower than `speed_tolerance` times a_inf. Here the state is FP64 and
     the metrics FP32: the shock's speeds settle near 1e-7 (the reference's
-    all-FP32 engine: 1e-6 to 4e-6, against its tolerance of 3e-5).
+    all-FP32 engine: 1e-6 to 4e-6, against its tolerance of 3e-5), and the
+    drag at a few 1e-8 on slowly settling fits, hence the noise of 1e-7.
     Returns (converged, iterations, max speed, drag)."""
     from .verification import SettlingValue
 
@@ -460,7 +461,7 @@ def blunt_fit_problem(asked: Body, mach: float, nj: int = 20, gamma: float = 1.4
 FITTED_BASE_NJ = 20            # base grid cells across (fitted-flow.ts:1003)
 FALLBACK_COLUMN_DENSITY = 1.5  # a sharp family whose grid fails only the gates, solved again (:70)
 FITTED_DRAG_FLOOR = 7e-5       # systematic error of the fitted drag, relative (src/analysis/verified-drag.ts:132)
-FITTED_NOISE = 1e-8            # the GPU fit's drag settles to this, relative
+FITTED_NOISE = 1e-7            # the GPU fit's drag settles to this, relative (settle)
 FITTED_MIN_ANGLE = 12.0        # the fitted grids' quality gates (src/grid/quality.ts:24-38, 64-68), degrees
 FITTED_MIN_WALL_ANGLE = 50.0
 FITTED_MAX_ASPECT = 13.0
@@ -601,7 +602,7 @@ def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance:
         return VerifiedDrag("invalid", None, reports, 1, str(e))
 
 
-def settle_many(fits: list[CudaFit], max_iterations: int, noise: float = 1e-8, speed_tolerance: float = 1e-6,
+def settle_many(fits: list[CudaFit], max_iterations: int, noise: float = 1e-7, speed_tolerance: float = 1e-6,
                 check_every: int = 250) -> list:
     """settle() for many fits at once, one host thread each: every fit has
     its own stream and its calls release the interpreter lock, so their

@@ -187,4 +187,4 @@ def test_a_grid_failing_only_the_gates_is_solved_again_with_more_columns():
     assert f"cell aspect ratio {FALLBACK['aspect_ratio']:.1f} above {FALLBACK['aspect_limit']}" in fallbacks[0][1]
     assert out.kind == "solved" and out.column_density == FALLBACK_COLUMN_DENSITY
     assert out.reports[0].ni == FALLBACK["columns"]
-    assert abs(out.result.levels[0][1] / FALLBACK["value"] - 1) < 1e-7
+    assert abs(out.result.levels[0][1] / FALLBACK["value"] - 1) < 3e-7
