@@ -709,6 +709,17 @@ def run_fitted(args) -> None:
                          "exact_taylor_maccoll": exact, "exact_inside_band": abs(v.estimate.value - exact) <= v.uncertainty,
                          "levels": [{"refinement": rep.refinement, "cells": rep.ni * rep.nj, "steps": rep.iterations,
                                      "drag": rep.drag} for rep in vf.reports]})
+    t0 = time.perf_counter()
+    vb = verified_fitted_drag(Body(Nose(NoseShape("ellipsoid"), 0.5, 0.5), 4.0), 2.0, tolerance=1e-4,
+                              max_refinement=8)
+    verified_blunt = {"case": "hemisphere-cylinder, Mach 2, base nj 20", "kind": vb.kind,
+                      "wall_s": time.perf_counter() - t0}
+    if vb.result is not None:
+        v = vb.result
+        verified_blunt.update({"value": v.estimate.value, "band": v.uncertainty, "verified": v.verified,
+                               "extrapolated": v.estimate.extrapolated, "order": v.estimate.order,
+                               "levels": [{"refinement": rep.refinement, "cells": rep.ni * rep.nj,
+                                           "steps": rep.iterations, "drag": rep.drag} for rep in vb.reports]})
     cpu = None
     if not args.no_cpu_baseline:
         from oracle.shock_fitting import fit_shock
@@ -729,7 +740,8 @@ def run_fitted(args) -> None:
         "config": {"workload": "cone 20 deg Mach 3 on 4-caliber cylinder at nj = 10, refined 1, 2, 4; "
                                "hemisphere-cylinder Mach 2 at nj = 20; SSP-RK2 CFL 0.8 local steps, HLLC, "
                                "van Albada (shared scaled), axisymmetric"},
-        "fits": rows, "observed_order": order, "verified_fitted_drag": verified, "fitted_drag_curve": curve,
+        "fits": rows, "observed_order": order, "verified_fitted_drag": verified, "verified_fitted_drag_blunt": verified_blunt,
+        "fitted_drag_curve": curve,
         "extrapolated_rel_err": errors[2] - (errors[1] - errors[2]) / 3,
         "cpu_baseline": cpu,
     }), flush=True)

@@ -391,16 +391,39 @@ def captured_shock_heights(prims: np.ndarray, x: np.ndarray, y: np.ndarray, line
     return h
 
 
-def blunt_fit_problem(asked: Body, mach: float, nj: int = 20, gamma: float = 1.4) -> FitProblem:
-    """bluntFitProblem at refinement 1 (src/analysis/fitted-flow.ts:467-730)
-    for noses whose blunt grid is at the body's scale (spheres and
-    ellipsoids): the body's cylinder lengthened a caliber at a time until
-    its C grid meets the fitted grids' size-ratio gate (solvedBluntBody,
-    :140-185); a captured solution on that grid (3,000 explicit steps from
-    the free stream, here on the GPU engine) whose shock, smoothed, is the
-    starting shock; the grid's lines keeping the node fractions of that
-    height; the start field taken at the same fraction of the shock layer
-    (shockLayerStart, :735-768); the first shock node normal to the axis."""
+@dataclass
+class BluntStart:
+    """What starts a blunt family (BluntStart, fitted-flow.ts:472-490): the
+    body solved, the base grid, its lines (x, y, dx, dy), the captured shock's
+    heights along them and the captured solution (nj, ni, 4)."""
+
+    body: Body
+    asked_end: float
+    grid: StructuredGrid
+    lines: np.ndarray
+    heights: np.ndarray
+    captured: np.ndarray
+    nj: int
+    mach: float
+    gamma: float
+
+
+def _grid_lines(grid: StructuredGrid) -> np.ndarray:
+    """The lines of a C grid from the body node to the outer one: (ni + 1, 4)."""
+    X = grid.x.reshape(grid.nj + 1, grid.ni + 1)
+    Y = grid.y.reshape(grid.nj + 1, grid.ni + 1)
+    ex, ey = X[grid.nj] - X[0], Y[grid.nj] - Y[0]
+    length = np.hypot(ex, ey)
+    return np.stack([X[0], Y[0], ex / length, ey / length], 1)
+
+
+def blunt_start(asked: Body, mach: float, nj: int = 20, gamma: float = 1.4) -> BluntStart:
+    """bluntStart (fitted-flow.ts:498-508) for noses whose blunt grid is at the
+    body's scale (spheres and ellipsoids): the body's cylinder lengthened a
+    caliber at a time until its C grid meets the fitted grids' size-ratio
+    gate (solvedBluntBody, :140-185); 3,000 captured explicit steps from the
+    free stream on it (here on the GPU engine); the captured shock's heights
+    (capturedShockHeights)."""
     from .engine import CudaEuler2D
     from .grid import blunt_body_grid, grid_quality
 
@@ -427,33 +450,88 @@ def blunt_fit_problem(asked: Body, mach: float, nj: int = 20, gamma: float = 1.4
         e.set_uniform(free)
         e.iterate(CAPTURED_START_STEPS)
         captured = e.primitives().reshape(grid.nj, grid.ni, 4)
-    ni = grid.ni
-    X = grid.x.reshape(nj + 1, ni + 1)
-    Y = grid.y.reshape(nj + 1, ni + 1)
-    # The generator's lines: from the body node to the outer one.
-    ex, ey = X[nj] - X[0], Y[nj] - Y[0]
-    length = np.hypot(ex, ey)
-    lines = np.stack([X[0], Y[0], ex / length, ey / length], 1)
+    lines = _grid_lines(grid)
+    X = grid.x.reshape(nj + 1, grid.ni + 1)
+    Y = grid.y.reshape(nj + 1, grid.ni + 1)
     heights = captured_shock_heights(captured, X, Y, lines, free)
-    fractions = stretched_fraction(line_strength(heights, R)[:, None], np.arange(nj + 1)[None, :], nj)
-    # shockLayerStart: each fitted cell at its fraction of the shock layer,
-    # linear between the captured cells of its column either side.
-    along = (X - lines[:, 0]) * lines[:, 2] + (Y - lines[:, 1]) * lines[:, 3]
-    frac = along / heights[None, :]                                   # (nj + 1, ni + 1)
-    centre = 0.25 * (frac[:-1, :-1] + frac[:-1, 1:] + frac[1:, :-1] + frac[1:, 1:])   # (nj, ni)
-    fa = fractions.T                                                  # (nj + 1, ni + 1)
-    s = 0.25 * (fa[:-1, :-1] + fa[1:, :-1] + fa[:-1, 1:] + fa[1:, 1:])
-    initial = np.empty((nj, ni, 4))
-    for i in range(ni):
-        for j in range(nj):
-            jj = 0
-            while jj < nj - 2 and centre[jj + 1, i] < s[j, i]:
-                jj += 1
-            c0 = centre[jj, i]
-            t = min(max((s[j, i] - c0) / (centre[jj + 1, i] - c0), 0.0), 1.0)
-            initial[j, i] = captured[jj, i] + t * (captured[jj + 1, i] - captured[jj, i])
-    return FitProblem(lines[:, 0].copy(), lines[:, 1].copy(), lines[:, 2].copy(), lines[:, 3].copy(), fractions,
-                      heights, nj, R, gamma, mach, free, None, initial.reshape(-1, 4), "symmetry", 0.0)
+    return BluntStart(body, asked.nose.length + asked.cylinder_length, grid, lines, heights, captured, nj, mach,
+                      gamma)
+
+
+def nested_heights(base_lines: np.ndarray, base_heights: np.ndarray, fine_lines: np.ndarray,
+                   refinement: int) -> np.ndarray:
+    """nestedHeights (fitted-flow.ts:788-812): the base heights on every
+    refinement-th line, linear in the line's index between them (weights
+    m / refinement, exact in binary, so every grid of the family nests in
+    the next); refused if the fine grid lacks a base line."""
+    n = len(base_lines) - 1
+    if len(fine_lines) - 1 != refinement * n:
+        raise ValueError("the refined grid does not have the lines of its base grid")
+    scale = math.hypot(base_lines[n, 0] - base_lines[0, 0], base_lines[n, 1] - base_lines[0, 1])
+    for k in range(n + 1):
+        a, b = base_lines[k], fine_lines[refinement * k]
+        if not math.hypot(a[0] - b[0], a[1] - b[1]) <= 1e-12 * scale:
+            raise ValueError("the refined grid does not have the lines of its base grid")
+    out = []
+    for k in range(n):
+        for m in range(refinement):
+            t = m / refinement
+            out.append(base_heights[k] * (1 - t) + base_heights[k + 1] * t)
+    out.append(base_heights[n])
+    return np.array(out)
+
+
+def blunt_fit_family(start: BluntStart):
+    """bluntFitFamily (fitted-flow.ts:683-730): the problem at each
+    refinement from one captured start: the refined grid's lines (which
+    keep every base line), the heights nested between the base ones, each
+    line's node fractions fixed at its height, and the start field at the
+    same fraction of the shock layer (shockLayerStart, :735-768) on the
+    base grid's column; the first shock node normal to the axis."""
+    from .grid import blunt_body_grid
+
+    R = start.body.nose.base_radius
+    free = free_stream_at(start.mach, start.gamma).state
+    X0 = start.grid.x.reshape(start.nj + 1, start.grid.ni + 1)
+    Y0 = start.grid.y.reshape(start.nj + 1, start.grid.ni + 1)
+    along = (X0 - start.lines[:, 0]) * start.lines[:, 2] + (Y0 - start.lines[:, 1]) * start.lines[:, 3]
+    frac = along / start.heights[None, :]
+    centre = 0.25 * (frac[:-1, :-1] + frac[:-1, 1:] + frac[1:, :-1] + frac[1:, 1:])   # (nj, ni) of the base
+    nj0 = start.nj
+
+    def problem(refinement: int = 1) -> FitProblem:
+        if refinement == 1:
+            lines = start.lines
+        else:
+            lines = _grid_lines(blunt_body_grid(start.body, nj0, start.mach, refinement=refinement, gated=False).grid)
+        heights = nested_heights(start.lines, start.heights, lines, refinement)
+        nj = nj0 * refinement
+        ni = len(lines) - 1
+        fractions = stretched_fraction(line_strength(heights, R)[:, None], np.arange(nj + 1)[None, :], nj)
+        fa = fractions.T
+        s = 0.25 * (fa[:-1, :-1] + fa[1:, :-1] + fa[:-1, 1:] + fa[1:, 1:])              # (nj, ni)
+        initial = np.empty((nj, ni, 4))
+        for i in range(ni):
+            column = i // refinement
+            c = centre[:, column]
+            w = start.captured[:, column]
+            for j in range(nj):
+                jj = 0
+                while jj < nj0 - 2 and c[jj + 1] < s[j, i]:
+                    jj += 1
+                t = min(max((s[j, i] - c[jj]) / (c[jj + 1] - c[jj]), 0.0), 1.0)
+                initial[j, i] = w[jj] + t * (w[jj + 1] - w[jj])
+        return FitProblem(lines[:, 0].copy(), lines[:, 1].copy(), lines[:, 2].copy(), lines[:, 3].copy(), fractions,
+                          heights, nj, R, start.gamma, start.mach, free, None, initial.reshape(-1, 4), "symmetry", 0.0)
+
+    return problem
+
+
+def blunt_fit_problem(asked: Body, mach: float, nj: int = 20, gamma: float = 1.4,
+                      refinement: int = 1) -> FitProblem:
+    """bluntFitProblem (src/analysis/fitted-flow.ts:467-469): the family's
+    problem at `refinement` from a fresh captured start."""
+    return blunt_fit_family(blunt_start(asked, mach, nj, gamma))(refinement)
 
 
 # ---- verified fitted drag -------------------------------------------------------
@@ -544,22 +622,34 @@ def fitted_case_failure(problem: FitProblem, asked_end: float, grid: StructuredG
 def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance: float = 1e-4,
                          max_refinement: int = 8, floor: float = FITTED_DRAG_FLOOR,
                          iterations_per_refinement: int = 200000, on_level=None, on_fallback=None):
-    """verifiedFittedDrag (fitted-flow.ts:1005-1075) for sharp noses, on the
-    GPU fit: grids refined by 2 from 20 cells across until the drag's band
+    """verifiedFittedDrag (fitted-flow.ts:1005-1075) for sharp noses and for
+    blunt ones at the body's scale (one captured start for the family), on
+    the GPU fit: grids refined by 2 from 20 cells across until the drag's band
     (grid convergence index plus `floor`) is within `tolerance`; a grid
     whose fit does not settle, or whose flow fails the checks, stops the run
-    without a value, but a family whose grid fails only the quality gates is
-    solved again with 1.5 times as many columns. Returns a
+    without a value, but a sharp family whose grid fails only the quality
+    gates is solved again with 1.5 times as many columns. Returns a
     verified_drag.VerifiedDrag."""
     from .verification import refine_until_verified
     from .verified_drag import LevelReport, VerifiedDrag
 
     asked_end = body.nose.length + body.cylinder_length
     reports: list = []
+    blunt = None
+    if not math.isfinite(_nose_slopes(body)[0]):
+        # Blunt: one captured start for the whole family (bluntFitFamily).
+        try:
+            blunt = blunt_fit_family(blunt_start(body, mach, FITTED_BASE_NJ, gamma))
+        except ValueError as e:
+            return VerifiedDrag("invalid", None, reports, 1, str(e))
 
     def family(density: float):
         def solve_at(r: int) -> float:
-            p = sharp_fit_problem(body, mach, nj=FITTED_BASE_NJ, refinement=r, gamma=gamma, column_density=density)
+            if blunt is not None:
+                p = blunt(r)
+            else:
+                p = sharp_fit_problem(body, mach, nj=FITTED_BASE_NJ, refinement=r, gamma=gamma,
+                                      column_density=density)
             with CudaFit(p) as g:
                 converged, it, speed, drag = settle(g, iterations_per_refinement * r, check_every=250 * r)
                 if not converged:
@@ -589,6 +679,8 @@ def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance:
         try:
             return VerifiedDrag("solved", family(1.0), reports)
         except GridRefused as e:
+            if blunt is not None:
+                raise
             if on_fallback is not None:
                 on_fallback(e.refinement, str(e))
             reports.clear()

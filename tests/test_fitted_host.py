@@ -187,3 +187,27 @@ def test_fit_create_refuses_a_grid_without_a_shock_side():
                          C.byref(abi.Primitive(p.free.rho, p.free.u, p.free.v, p.free.p)), inflow.ctypes.data_as(dp),
                          0, initial.ctypes.data_as(dp), C.byref(h))
     assert st == abi.BS_INVALID_ARGUMENT and b"jMax" in L.bs_last_error()
+
+
+def test_blunt_grid_families_nest():
+    # tests/analysis/fitted-flow.test.ts:76-114: the refined C grid keeps
+    # every line of the base grid; nested heights keep the base heights on
+    # them, and the node fractions fixed at those heights nest too.
+    from bowshock_b200.fitted import _grid_lines, line_strength, nested_heights, stretched_fraction
+    from bowshock_b200.grid import Body, Nose, NoseShape, blunt_body_grid
+
+    body = Body(Nose(NoseShape("ellipsoid"), 1.5, 0.5), 2.0)
+    coarse = _grid_lines(blunt_body_grid(body, 20, 2.0, gated=False).grid)
+    rng = np.random.default_rng(3)
+    h1 = 0.3 + 0.1 * rng.random(len(coarse))
+    for r in (2, 4):
+        fine = _grid_lines(blunt_body_grid(body, 20, 2.0, refinement=r, gated=False).grid)
+        assert len(fine) - 1 == r * (len(coarse) - 1)
+        assert np.max(np.hypot(*(fine[::r, :2] - coarse[:, :2]).T)) < 1e-13
+        h = nested_heights(coarse, h1, fine, r)
+        assert np.array_equal(h[::r], h1)
+        f1 = stretched_fraction(line_strength(h1, 0.5)[:, None], np.arange(21)[None, :], 20)
+        fr = stretched_fraction(line_strength(h, 0.5)[:, None], np.arange(20 * r + 1)[None, :], 20 * r)
+        assert np.max(np.abs(fr[::r, ::r] - f1)) < 1e-14
+    with pytest.raises(ValueError):
+        nested_heights(coarse, h1, coarse[:-1], 1)

@@ -188,3 +188,22 @@ def test_a_grid_failing_only_the_gates_is_solved_again_with_more_columns():
     assert out.kind == "solved" and out.column_density == FALLBACK_COLUMN_DENSITY
     assert out.reports[0].ni == FALLBACK["columns"]
     assert abs(out.result.levels[0][1] / FALLBACK["value"] - 1) < 3e-7
+
+
+def test_verified_fitted_drag_of_a_blunt_nose():
+    # The hemisphere-cylinder at Mach 2 through the verified procedure: one
+    # captured start for the family, grids of 20 cells across refined by 2,
+    # the nested heights of the refined grids keeping the base heights.
+    from bowshock_b200.fitted import blunt_fit_family, blunt_start, verified_fitted_drag
+    from bowshock_b200.grid import Body, Nose, NoseShape
+
+    b = HEMI["body"]
+    body = Body(Nose(NoseShape(b["shape"]), b["length"], b["base_radius"]), b["cylinder"])
+    family = blunt_fit_family(blunt_start(body, HEMI["mach"], 20))
+    p1, p2 = family(1), family(2)
+    assert np.array_equal(p2.heights[::2], p1.heights) and p2.nj == 40
+    out = verified_fitted_drag(body, HEMI["mach"], tolerance=1e-3, max_refinement=8)
+    assert out.kind == "solved", out.reason
+    v = out.result
+    assert v.verified and v.uncertainty <= 1e-3 and len(v.levels) >= 2
+    assert abs(v.levels[0][1] - out.reports[0].drag) == 0.0
