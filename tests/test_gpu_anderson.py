@@ -121,3 +121,28 @@ def test_accelerated_steps_follow_the_oracle_and_keep_the_drag(mach):
     assert abs(runs[8][2] / runs[0][2] - 1) < 1e-7
     steps_oracle = _oracle_anderson_steps(case)
     assert abs(runs[8][1] - steps_oracle) <= 0.15 * steps_oracle + 20
+
+
+def test_near_mach_one_the_acceleration_takes_fewer_steps():
+    # The regime the reference accelerates (src/analysis/transonic-flow.ts):
+    # the hemisphere-cylinder's C grid at Mach 1.2, where a subsonic region
+    # behind the detached shock converges slowly under plain steps.
+    from bowshock_b200.config import Boundary, free_stream_at, steady_drag_config
+    from bowshock_b200.grid import Body, Nose, NoseShape, blunt_body_grid
+
+    body = Body(Nose(NoseShape("ellipsoid"), 0.5, 0.5), 4.0)
+    grid = blunt_body_grid(body, 20, 1.2, gated=False).grid
+    free = free_stream_at(1.2, 1.4)
+    cfg = steady_drag_config(grid, free.state, boundaries={
+        "iMin": Boundary("wall"), "iMax": Boundary("outflow"), "jMin": Boundary("wall"),
+        "jMax": Boundary("inflow", free.state)})
+    runs = {}
+    for depth in (0, 8):
+        with CudaBatch([cfg], precision=64) as b:
+            b.set_free_stream()
+            b.set_anderson(depth, 30)
+            r = b.solve("lusgs", 1e-8, max_steps=20000, cfl=5.0)[0]
+            runs[depth] = (r.status, r.steps, b.forebody_drag(0, free, 0.5))
+    assert runs[0][0] == 0 and runs[8][0] == 0
+    assert runs[8][1] < 0.8 * runs[0][1]
+    assert abs(runs[8][2] / runs[0][2] - 1) < 1e-7
