@@ -84,19 +84,24 @@ class FittedSolver {
     if (!(cfg.cfl > 0 && cfg.cfl <= 1)) return fail(BS_INVALID_ARGUMENT, "cfl must be in (0, 1]");
     if (first_node != 0 && first_node != 1) return fail(BS_INVALID_ARGUMENT, "first_node is 0 (fixed) or 1 (symmetry)");
     if (!(free.rho > 0 && free.p > 0)) return fail(BS_INVALID_ARGUMENT, "the free stream needs rho > 0 and p > 0");
-    gamma_ = cfg.gamma;
-    integrator_ = cfg.integrator;
-    FIT_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    if (!(cfg.gamma > 1)) return fail(BS_INVALID_ARGUMENT, "gamma must exceed 1");
     const size_t nn = size_t(ni + 1) * (nj + 1), nc = size_t(ni) * nj;
     std::vector<double> line(4 * size_t(ni + 1));
     for (int k = 0; k <= ni; k++) {
       const double len = std::hypot(line_dx[k], line_dy[k]);
       if (!(std::fabs(len - 1) < 1e-12)) return fail(BS_INVALID_ARGUMENT, "the lines' directions must be unit vectors");
+      if (!(heights[k] > 0)) return fail(BS_INVALID_ARGUMENT, "the shock heights must be positive");
       line[4 * k] = line_x[k];
       line[4 * k + 1] = line_y[k];
       line[4 * k + 2] = line_dx[k];
       line[4 * k + 3] = line_dy[k];
     }
+    for (size_t k = 0; k < nn; k++)
+      if (!(fractions[k] >= 0 && fractions[k] <= 1))
+        return fail(BS_INVALID_ARGUMENT, "the node fractions must lie in [0, 1]");
+    gamma_ = cfg.gamma;
+    integrator_ = cfg.integrator;
+    FIT_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     FIT_CUDA(line_.alloc(line.size()));
     FIT_CUDA(line_.upload(line.data(), line.size(), stream_));
     FIT_CUDA(fraction_.alloc(nn));

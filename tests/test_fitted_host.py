@@ -165,10 +165,32 @@ def test_oracle_fit_moves_the_shock_towards_rest_and_the_conical_drag():
     assert abs(p.drag(f.engine.boundary_fluxes("jMin")) / exact - 1) < 3e-3
 
 
-def test_fit_create_refuses_a_grid_without_a_shock_side():
+def _fit_create(p, cfg=None, **change):
+    """bs_fit_create on a fit problem with some inputs changed; returns
+    (status, message). Its argument checks run before any CUDA call."""
     import ctypes as C
 
     from bowshock_b200 import _native, abi
+
+    cfg = cfg or p.config()
+    L = _native.load()
+    dp = C.POINTER(C.c_double)
+    arrays = {k: np.ascontiguousarray(change.get(k, getattr(p, k)), np.float64).reshape(-1)
+              for k in ("line_x", "line_y", "line_dx", "line_dy", "fractions", "heights")}
+    inflow = change.get("inflow", p.inflow)
+    inflow = None if inflow is None else np.ascontiguousarray(inflow, np.float64).reshape(-1)
+    initial = np.ascontiguousarray(p.initial, np.float64).reshape(-1)
+    h = C.c_void_p()
+    st = L.bs_fit_create(C.byref(cfg.to_abi()), *[arrays[k].ctypes.data_as(dp) for k in
+                                                  ("line_x", "line_y", "line_dx", "line_dy", "fractions", "heights")],
+                         C.byref(abi.Primitive(p.free.rho, p.free.u, p.free.v, p.free.p)),
+                         None if inflow is None else inflow.ctypes.data_as(dp), change.get("first_node", 0),
+                         initial.ctypes.data_as(dp), C.byref(h))
+    return st, L.bs_last_error().decode()
+
+
+def test_fit_create_refuses_bad_problems_before_touching_the_gpu():
+    from bowshock_b200 import abi
     from bowshock_b200.config import Boundary
     from bowshock_b200.fitted import sharp_fit_problem
     from bowshock_b200.workloads import cone_body
@@ -176,17 +198,27 @@ def test_fit_create_refuses_a_grid_without_a_shock_side():
     p = sharp_fit_problem(cone_body(20, 4.0), 3.0, nj=10)
     cfg = p.config()
     cfg.boundaries["jMax"] = Boundary("outflow")
-    L = _native.load()
-    dp = C.POINTER(C.c_double)
-    arrays = [np.ascontiguousarray(a, np.float64) for a in (p.line_x, p.line_y, p.line_dx, p.line_dy,
-                                                               p.fractions.reshape(-1), p.heights)]
-    inflow = np.ascontiguousarray(p.inflow, np.float64).reshape(-1)
-    initial = np.ascontiguousarray(p.initial, np.float64).reshape(-1)
-    h = C.c_void_p()
-    st = L.bs_fit_create(C.byref(cfg.to_abi()), *[a.ctypes.data_as(dp) for a in arrays],
-                         C.byref(abi.Primitive(p.free.rho, p.free.u, p.free.v, p.free.p)), inflow.ctypes.data_as(dp),
-                         0, initial.ctypes.data_as(dp), C.byref(h))
-    assert st == abi.BS_INVALID_ARGUMENT and b"jMax" in L.bs_last_error()
+    st, msg = _fit_create(p, cfg)
+    assert st == abi.BS_INVALID_ARGUMENT and "jMax" in msg
+    cfg = p.config()
+    cfg.boundaries["iMin"] = Boundary("outflow")
+    st, msg = _fit_create(p, cfg)
+    assert st == abi.BS_INVALID_ARGUMENT and "iMin" in msg
+    st, msg = _fit_create(p, inflow=None)
+    assert st == abi.BS_INVALID_ARGUMENT and "inflow" in msg
+    st, msg = _fit_create(p, line_dx=p.line_dx + 0.1)
+    assert st == abi.BS_INVALID_ARGUMENT and "unit" in msg
+    st, msg = _fit_create(p, heights=np.where(np.arange(len(p.heights)) == 3, -1.0, p.heights))
+    assert st == abi.BS_INVALID_ARGUMENT and "heights" in msg
+    st, msg = _fit_create(p, fractions=p.fractions * 2)
+    assert st == abi.BS_INVALID_ARGUMENT and "fractions" in msg
+    st, msg = _fit_create(p, first_node=2)
+    assert st == abi.BS_INVALID_ARGUMENT and "first_node" in msg
+    import dataclasses
+
+    cfg = dataclasses.replace(p.config(), time_integrator="forwardEuler")
+    st, msg = _fit_create(p, cfg)
+    assert st == abi.BS_INVALID_ARGUMENT and "SSP-RK" in msg
 
 
 def test_blunt_grid_families_nest():
