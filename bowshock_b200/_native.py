@@ -97,11 +97,14 @@ SIGNATURES: dict[str, list] = {
                              C.c_double, _vp, _dp, _ip],
     "bs_body_grid": [C.POINTER(abi.Body), C.POINTER(abi.BodyGridOptions), C.POINTER(_vp)],
     "bs_blunt_body_grid": [C.POINTER(abi.Body), C.POINTER(abi.BodyGridOptions), C.POINTER(_vp)],
+    "bs_blunt_body_grid_bounded": [C.POINTER(abi.Body), C.POINTER(abi.BodyGridOptions), _dp, _dp, C.c_int32,
+                                   C.POINTER(_vp)],
     "bs_ramp_grid": [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
                      C.c_double, C.POINTER(_vp)],
     "bs_grid_dims": [_vp, _ip, _ip],
     "bs_grid_nodes": [_vp, _dp, _dp],
     "bs_grid_info": [_vp, _ip, _dp],
+    "bs_grid_two_scale": [_vp, _ip],
     "bs_grid_destroy": [_vp],
     "bs_grid_quality_of": [C.c_int32, C.c_int32, _dp, _dp, C.POINTER(abi.GridQuality)],
     "bs_taylor_maccoll": [C.c_double, C.c_double, C.c_double, C.c_double,

@@ -96,8 +96,10 @@ class FittedSolver {
       line[4 * k + 2] = line_dx[k];
       line[4 * k + 3] = line_dy[k];
     }
+    // The fractions of a stretched line end at expm1(b nj / nj) / expm1(b),
+    // which rounds to 1 + 2^-52 for some b: a rounding above 1 is accepted.
     for (size_t k = 0; k < nn; k++)
-      if (!(fractions[k] >= 0 && fractions[k] <= 1))
+      if (!(fractions[k] >= 0 && fractions[k] <= 1 + 1e-12))
         return fail(BS_INVALID_ARGUMENT, "the node fractions must lie in [0, 1]");
     gamma_ = cfg.gamma;
     integrator_ = cfg.integrator;

@@ -52,14 +52,28 @@ bs_status bs_body_grid(const bs_body* body, const bs_body_grid_options* options,
 
 bs_status bs_blunt_body_grid(const bs_body* body, const bs_body_grid_options* options,
                              bs_grid** out) {
+  return bs_blunt_body_grid_bounded(body, options, nullptr, nullptr, 0, out);
+}
+
+bs_status bs_blunt_body_grid_bounded(const bs_body* body, const bs_body_grid_options* options,
+                                     const double* outer_x, const double* outer_y, int32_t n_outer,
+                                     bs_grid** out) {
   if (body == nullptr || options == nullptr || out == nullptr)
     return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  if (n_outer < 0 || (n_outer > 0 && (outer_x == nullptr || outer_y == nullptr)))
+    return bs::fail(BS_INVALID_ARGUMENT, "the outer boundary's points are missing");
+  if (n_outer == 1)
+    return bs::fail(BS_INVALID_ARGUMENT, "the outer boundary needs at least two points, the first on the axis");
   bs::BluntGridOptions o;
   o.nj = options->nj;
   o.refinement = options->refinement <= 0 ? 1 : options->refinement;
   o.ni = options->ni;
   o.mach = options->mach;
   o.gated = (options->flags & BS_GRID_UNGATED) == 0;
+  if (n_outer > 0) {
+    o.outer_x.assign(outer_x, outer_x + n_outer);
+    o.outer_y.assign(outer_y, outer_y + n_outer);
+  }
   auto* g = new (std::nothrow) bs_grid;
   if (g == nullptr) return bs::fail(BS_MEMORY_LIMIT, "out of host memory");
   bool quality = false;
@@ -106,6 +120,12 @@ bs_status bs_grid_info(const bs_grid* grid, int32_t* i_tip, double* outer_angle)
   if (grid == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
   if (i_tip) *i_tip = grid->g.i_tip;
   if (outer_angle) *outer_angle = grid->g.outer_angle;
+  return bs::ok();
+}
+
+bs_status bs_grid_two_scale(const bs_grid* grid, int32_t* two_scale) {
+  if (grid == nullptr || two_scale == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  *two_scale = grid->g.two_scale ? 1 : 0;
   return bs::ok();
 }
 

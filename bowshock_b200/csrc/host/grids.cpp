@@ -432,16 +432,45 @@ std::string blunt_body_grid(const Body& body, const BluntGridOptions& o, Grid* o
                                          : std::max(tip_radius, std::min(R, kTipScaleFactor * tip_scale));
 
   // Outer boundary: an arc ahead of the tip (standoff from Billig's
-  // correlation, billigStandoff, blunt-grid.ts:99-101), then a straight line.
+  // correlation, billigStandoff, blunt-grid.ts:99-101), then a straight line;
+  // or the polyline given, linear between its points and continued by its
+  // last segment beyond them.
   const double outer_angle = (M_PI / 2 + std::asin(1 / o.mach)) / 2;
   const double arc_radius = kArcRadiusFactor * scale;
   const double standoff = kStandoffFactor * 0.143 * std::exp(3.24 / (o.mach * o.mach)) * scale;
   const double centre = arc_radius - standoff;
   const double y_join = arc_radius * std::cos(outer_angle);
   const double x_join = centre - arc_radius * std::sin(outer_angle);
+  const std::vector<double>& cx = o.outer_x;
+  const std::vector<double>& cy = o.outer_y;
+  const bool custom = !cx.empty() || !cy.empty();
+  if (custom) {
+    if (cx.size() != cy.size() || cx.size() < 2 || cy[0] != 0)
+      return "the outer boundary needs at least two points, the first on the axis";
+    for (size_t k = 0; k < cx.size(); k++)
+      if (!std::isfinite(cx[k]) || !std::isfinite(cy[k])) return "the outer boundary must be finite";
+    for (size_t k = 1; k < cy.size(); k++)
+      if (!(cy[k] > cy[k - 1])) return "the outer boundary must be ordered outwards from the axis";
+  }
   auto outer_x = [&](double y) {
-    return y <= y_join ? centre - std::sqrt(arc_radius * arc_radius - y * y)
-                       : x_join + (y - y_join) / std::tan(outer_angle);
+    if (!custom)
+      return y <= y_join ? centre - std::sqrt(arc_radius * arc_radius - y * y)
+                         : x_join + (y - y_join) / std::tan(outer_angle);
+    // The segment holding y (the last one at or beyond the last point; the
+    // first one below the axis, where the lines ahead of the tip look).
+    const size_t n = cy.size() - 1;
+    size_t low = 0;
+    if (y >= cy[n]) {
+      low = n - 1;
+    } else {
+      size_t high = n;
+      while (high - low > 1) {
+        const size_t mid = (low + high) >> 1;
+        if (cy[mid] <= y) low = mid;
+        else high = mid;
+      }
+    }
+    return cx[low] + ((y - cy[low]) / (cy[low + 1] - cy[low])) * (cx[low + 1] - cx[low]);
   };
   bool reaches = false;
   // Distance from the body point at s to the outer boundary along (dx, dy).
@@ -583,6 +612,7 @@ std::string blunt_body_grid(const Body& body, const BluntGridOptions& o, Grid* o
   out->nj = nj;
   out->i_tip = 0;
   out->outer_angle = outer_angle;
+  out->two_scale = sharp || scale < R;
   out->x.assign(size_t(ni + 1) * (nj + 1), 0);
   out->y.assign(size_t(ni + 1) * (nj + 1), 0);
   for (int i = 0; i <= ni; i++) {

@@ -18,6 +18,9 @@ struct Grid {
   std::vector<double> x, y;  // (ni + 1)(nj + 1) nodes, node (i, j) at i + j (ni + 1)
   int i_tip = 0;
   double outer_angle = 0;
+  // A C grid whose boundary is placed at the tip's blunt part, narrower
+  // than the body (BluntGrid.twoScale, src/grid/blunt-grid.ts:553).
+  bool two_scale = false;
 };
 
 struct GridQuality {  // src/grid/quality.ts:6-21
@@ -62,13 +65,17 @@ std::string body_grid(const Body& body, const BodyGridOptions& options, Grid* ou
 // an arc ahead of the tip and a straight line at the angle halfway between
 // the normal shock and the Mach angle. iMin is the axis ahead of the tip,
 // jMin the body, jMax the outer boundary, iMax the outflow plane. `ni` > 0
-// asks for exactly that many columns (refinement 1).
+// asks for exactly that many columns (refinement 1). A given outer boundary
+// (outer_x, outer_y: a polyline from a point on the axis outwards, y
+// strictly increasing) replaces the arc and line (BluntGridOptions
+// .outerBoundary, src/grid/blunt-grid.ts:42, 296-331).
 struct BluntGridOptions {
   int nj = 20;
   int refinement = 1;
   int ni = 0;
   double mach = 2;
   bool gated = true;
+  std::vector<double> outer_x, outer_y;
 };
 std::string blunt_body_grid(const Body& body, const BluntGridOptions& options, Grid* out,
                             bool* quality_error);

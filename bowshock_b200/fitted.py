@@ -305,6 +305,14 @@ class CudaFit:
                    C.byref(it), C.byref(conv), C.byref(s), C.byref(r))
         return bool(conv.value), it.value, s.value, r.value
 
+    def grid(self) -> StructuredGrid:
+        """The fitted grid as it stands: its nodes on the current heights."""
+        p = self.problem
+        x = np.empty((p.ni + 1) * (p.nj + 1))
+        y = np.empty_like(x)
+        self._call("bs_fit_nodes", x.ctypes.data_as(C.POINTER(C.c_double)), y.ctypes.data_as(C.POINTER(C.c_double)))
+        return StructuredGrid(p.ni, p.nj, x, y)
+
     def heights(self) -> np.ndarray:
         out = np.empty(self.problem.ni + 1)
         self._call("bs_fit_heights", out.ctypes.data_as(C.POINTER(C.c_double)))
@@ -395,7 +403,8 @@ def captured_shock_heights(prims: np.ndarray, x: np.ndarray, y: np.ndarray, line
 class BluntStart:
     """What starts a blunt family (BluntStart, fitted-flow.ts:472-490): the
     body solved, the base grid, its lines (x, y, dx, dy), the captured shock's
-    heights along them and the captured solution (nj, ni, 4)."""
+    heights along them and the captured solution (nj, ni, 4); on a two-scale
+    nose the outer boundary (n, 2) the family's grids share."""
 
     body: Body
     asked_end: float
@@ -406,6 +415,7 @@ class BluntStart:
     nj: int
     mach: float
     gamma: float
+    outer_boundary: np.ndarray | None = None
 
 
 def _grid_lines(grid: StructuredGrid) -> np.ndarray:
@@ -417,31 +427,49 @@ def _grid_lines(grid: StructuredGrid) -> np.ndarray:
     return np.stack([X[0], Y[0], ex / length, ey / length], 1)
 
 
-def blunt_start(asked: Body, mach: float, nj: int = 20, gamma: float = 1.4) -> BluntStart:
-    """bluntStart (fitted-flow.ts:498-508) for noses whose blunt grid is at the
-    body's scale (spheres and ellipsoids): the body's cylinder lengthened a
-    caliber at a time until its C grid meets the fitted grids' size-ratio
-    gate (solvedBluntBody, :140-185); 3,000 captured explicit steps from the
-    free stream on it (here on the GPU engine); the captured shock's heights
-    (capturedShockHeights)."""
-    from .engine import CudaEuler2D
-    from .grid import blunt_body_grid, grid_quality
+BOUNDARY_MARGIN = 0.5       # a two-scale boundary's margin over the first captured shock (fitted-flow.ts:951)
+BOUNDARY_CELLS = 3          # ... and at least this many base-grid cells above it (:953)
+BOUNDARY_SMOOTHING = 50     # 1-2-1 passes over that boundary's distances (:955)
 
-    if asked.nose.shape.kind != "ellipsoid":
-        raise ValueError("the blunt fit here takes spheres and ellipsoids (noses whose grid is at the body's scale)")
-    R = asked.nose.base_radius
-    caliber = 2 * R
-    shortest = max(asked.cylinder_length, SOLVED_CYLINDER * caliber)
-    chosen = None
-    for extra in range(MAX_BLUNT_EXTENSION + 1):
-        body = Body(asked.nose, shortest + extra * caliber)
-        grid = blunt_body_grid(body, nj, mach, gated=False).grid
-        if chosen is None:
-            chosen = (body, grid)
-        if grid_quality(grid).max_size_ratio <= FITTED_MAX_SIZE_RATIO:
-            chosen = (body, grid)
-            break
-    body, grid = chosen
+
+def outer_cell_height(h, nj: int, radius: float):
+    """outerCellHeight (src/grid/blunt-grid.ts:571-573): the outermost cell's
+    height on a line of height h with nj cells."""
+    return h * (1 - stretched_fraction(line_strength(h, radius), nj - 1, nj))
+
+
+def two_scale_boundary(lines: np.ndarray, heights: np.ndarray, nj: int, radius: float) -> np.ndarray:
+    """The outer boundary of a two-scale nose's family (secondCapture,
+    fitted-flow.ts:624-672) from the shock captured on the generator's grid:
+    on each line the captured height pushed out by half of itself and by at
+    least three outer cells of the base grid, smoothed by 50 passes of 1-2-1
+    (mirrored at the ends), the last point continuing the segment before it
+    to the last line where that rises. Returns (ni + 1, 2) points."""
+    d = (1 + BOUNDARY_MARGIN) * heights
+    for _ in range(20):
+        d = np.maximum(d, heights + BOUNDARY_CELLS * outer_cell_height(d, nj, radius))
+    for _ in range(BOUNDARY_SMOOTHING):
+        c = d.copy()
+        d[0] = 0.5 * (c[0] + c[1])
+        d[1:-1] = 0.25 * c[:-2] + 0.5 * c[1:-1] + 0.25 * c[2:]
+        d[-1] = 0.5 * (c[-1] + c[-2])
+    pts = np.stack([lines[:, 0] + d * lines[:, 2], lines[:, 1] + d * lines[:, 3]], 1)
+    n = len(pts) - 1
+    if n >= 2:
+        (ax, ay), (bx, by) = pts[n - 2], pts[n - 1]
+        y = by + (lines[n, 0] - bx) * (by - ay) / (bx - ax)
+        if y > by:
+            pts[n] = (lines[n, 0], y)
+    return pts
+
+
+def _capture(body: Body, grid: StructuredGrid, mach: float, gamma: float) -> np.ndarray:
+    """bluntCapture (fitted-flow.ts:572-603): 3,000 explicit steps from the
+    free stream on a C grid (the axis and the body walls, outflow behind,
+    the free stream on the outer boundary), here on the GPU engine; the
+    solution (nj, ni, 4)."""
+    from .engine import CudaEuler2D
+
     free = free_stream_at(mach, gamma).state
     cfg = steady_drag_config(grid, free, gamma, boundaries={
         "iMin": Boundary("wall"), "iMax": Boundary("outflow"), "jMin": Boundary("wall"),
@@ -449,13 +477,54 @@ def blunt_start(asked: Body, mach: float, nj: int = 20, gamma: float = 1.4) -> B
     with CudaEuler2D(cfg) as e:
         e.set_uniform(free)
         e.iterate(CAPTURED_START_STEPS)
-        captured = e.primitives().reshape(grid.nj, grid.ni, 4)
-    lines = _grid_lines(grid)
-    X = grid.x.reshape(nj + 1, grid.ni + 1)
-    Y = grid.y.reshape(nj + 1, grid.ni + 1)
-    heights = captured_shock_heights(captured, X, Y, lines, free)
+        return e.primitives().reshape(grid.nj, grid.ni, 4)
+
+
+def blunt_start(asked: Body, mach: float, nj: int = 20, gamma: float = 1.4) -> BluntStart:
+    """bluntStart (fitted-flow.ts:498-508): the body's cylinder lengthened a
+    caliber at a time until its C grid meets the fitted grids' size-ratio
+    gate (solvedBluntBody, :140-185; a two-scale nose keeps the shortest);
+    3,000 captured explicit steps from the free stream on it (here on the GPU
+    engine) and the captured shock's heights (capturedShockHeights). On a
+    two-scale nose (Haack, power series: the generator's boundary is sized
+    for the tip) a second capture on the grid built on the first captured
+    shock (two_scale_boundary), whose boundary the family then shares."""
+    from .grid import blunt_body_grid, grid_quality
+
+    R = asked.nose.base_radius
+    caliber = 2 * R
+    shortest = max(asked.cylinder_length, SOLVED_CYLINDER * caliber)
+    chosen = None
+    for extra in range(MAX_BLUNT_EXTENSION + 1):
+        body = Body(asked.nose, shortest + extra * caliber)
+        bg = blunt_body_grid(body, nj, mach, gated=False)
+        if chosen is None:
+            chosen = (body, bg)
+        if bg.two_scale:
+            break
+        if grid_quality(bg.grid).max_size_ratio <= FITTED_MAX_SIZE_RATIO:
+            chosen = (body, bg)
+            break
+    body, bg = chosen
+    free = free_stream_at(mach, gamma).state
+
+    def heights_of(grid: StructuredGrid, captured: np.ndarray):
+        lines = _grid_lines(grid)
+        X = grid.x.reshape(nj + 1, grid.ni + 1)
+        Y = grid.y.reshape(nj + 1, grid.ni + 1)
+        return lines, captured_shock_heights(captured, X, Y, lines, free)
+
+    grid = bg.grid
+    captured = _capture(body, grid, mach, gamma)
+    lines, heights = heights_of(grid, captured)
+    boundary = None
+    if bg.two_scale:
+        boundary = two_scale_boundary(lines, heights, nj, R)
+        grid = blunt_body_grid(body, nj, mach, gated=False, outer_boundary=boundary).grid
+        captured = _capture(body, grid, mach, gamma)
+        lines, heights = heights_of(grid, captured)
     return BluntStart(body, asked.nose.length + asked.cylinder_length, grid, lines, heights, captured, nj, mach,
-                      gamma)
+                      gamma, boundary)
 
 
 def nested_heights(base_lines: np.ndarray, base_heights: np.ndarray, fine_lines: np.ndarray,
@@ -503,7 +572,8 @@ def blunt_fit_family(start: BluntStart):
         if refinement == 1:
             lines = start.lines
         else:
-            lines = _grid_lines(blunt_body_grid(start.body, nj0, start.mach, refinement=refinement, gated=False).grid)
+            lines = _grid_lines(blunt_body_grid(start.body, nj0, start.mach, refinement=refinement, gated=False,
+                                                outer_boundary=start.outer_boundary).grid)
         heights = nested_heights(start.lines, start.heights, lines, refinement)
         nj = nj0 * refinement
         ni = len(lines) - 1
@@ -543,6 +613,81 @@ FITTED_NOISE = 1e-7            # the GPU fit's drag settles to this, relative (s
 FITTED_MIN_ANGLE = 12.0        # the fitted grids' quality gates (src/grid/quality.ts:24-38, 64-68), degrees
 FITTED_MIN_WALL_ANGLE = 50.0
 FITTED_MAX_ASPECT = 13.0
+TWO_SCALE_DRAG_FLOOR = 8e-4    # a two-scale family's allowance, relative (src/analysis/verified-drag.ts:159)
+# The Von Karman noses checked against a reference: length in calibers, Mach
+# number (VON_KARMAN_REFERENCES, fitted-flow.ts:890-900).
+VON_KARMAN_REFERENCES = ((1, 1.5), (1, 2), (1, 3), (3, 2), (3, 3), (5, 1.5), (5, 2), (5, 3), (6, 3))
+
+
+def _number(x: float) -> str:
+    """A number as the reference's messages print it (shortest form, no '.0')."""
+    x = float(x)
+    return str(int(x)) if x.is_integer() else repr(x)
+
+
+def inside_outline(points, point, tolerance: float = 1e-9) -> bool:
+    """insideOutline (fitted-flow.ts:903-940): whether `point` lies in the
+    convex hull of `points` (a point, a segment or a polygon) or on it,
+    within `tolerance` after scaling each coordinate by the points' extent in
+    it. The hull by the monotone chain (A. M. Andrew, 1979), counterclockwise,
+    dropping turns within the tolerance."""
+    pts = [(float(a), float(b)) for a, b in points]
+    sx = (max(p[0] for p in pts) - min(p[0] for p in pts)) or 1.0
+    sy = (max(p[1] for p in pts) - min(p[1] for p in pts)) or 1.0
+    scaled = sorted((a / sx, b / sy) for a, b in pts)
+    q = (float(point[0]) / sx, float(point[1]) / sy)
+
+    def cross(o, a, b):
+        return (a[0] - o[0]) * (b[1] - o[1]) - (a[1] - o[1]) * (b[0] - o[0])
+
+    def chain(seq):
+        h: list = []
+        for c in seq:
+            while len(h) >= 2 and cross(h[-2], h[-1], c) <= tolerance:
+                h.pop()
+            h.append(c)
+        return h[:-1]
+
+    hull = chain(scaled) + chain(scaled[::-1])
+    if len(hull) <= 2:
+        a = hull[0] if hull else scaled[0]
+        b = hull[1] if len(hull) > 1 else a
+        dx, dy = b[0] - a[0], b[1] - a[1]
+        n2 = dx * dx + dy * dy
+        t = ((q[0] - a[0]) * dx + (q[1] - a[1]) * dy) / n2 if n2 > 0 else 0.0
+        u = min(max(t, 0.0), 1.0)
+        return math.hypot(q[0] - a[0] - u * dx, q[1] - a[1] - u * dy) <= tolerance
+    return all(cross(hull[k], hull[(k + 1) % len(hull)], q) >= -tolerance for k in range(len(hull)))
+
+
+def blunt_nose_refusal(body: Body, mach: float) -> str | None:
+    """bluntNoseRefusal (fitted-flow.ts:863-876): why a nose the fitted
+    solver could solve is not served, or None. Sharp tips and ellipsoids are
+    served; of the noses with unbounded tip curvature only the Von Karman
+    (LD-Haack, C = 0) nose, inside the outline of the lengths and Mach
+    numbers checked against a reference."""
+    shape = body.nose.shape
+    if math.isfinite(_nose_slopes(body)[0]) or shape.kind == "ellipsoid":
+        return None
+    if not (shape.kind == "haack" and shape.parameter == 0):
+        return ("of the blunt noses whose tip curvature is unbounded, only the Von Karman (LD-Haack) nose has "
+                "been checked against a reference so far")
+    calibers = body.nose.length / (2 * body.nose.base_radius)
+    if inside_outline(VON_KARMAN_REFERENCES, (calibers, mach)):
+        return None
+    checked = ", ".join(f"{_number(c)} at Mach {_number(m)}" for c, m in VON_KARMAN_REFERENCES)
+    unit = "caliber" if calibers == 1 else "calibers"
+    return (f"a Von Karman nose of {_number(calibers)} {unit} at Mach {_number(mach)} lies outside the referenced "
+            f"range (the outline of the noses checked against a reference, in calibers: {checked})")
+
+
+def fitted_drag_floor(floor: float, start: BluntStart | None) -> float:
+    """fittedDragFloor (fitted-flow.ts:964-966): the caller's allowance,
+    raised to TWO_SCALE_DRAG_FLOOR for a two-scale start (one with its own
+    outer boundary)."""
+    if start is not None and start.outer_boundary is not None:
+        return max(floor, TWO_SCALE_DRAG_FLOOR)
+    return floor
 
 
 class FitNotConverged(Exception):
@@ -622,26 +767,34 @@ def fitted_case_failure(problem: FitProblem, asked_end: float, grid: StructuredG
 def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance: float = 1e-4,
                          max_refinement: int = 8, floor: float = FITTED_DRAG_FLOOR,
                          iterations_per_refinement: int = 200000, on_level=None, on_fallback=None):
-    """verifiedFittedDrag (fitted-flow.ts:1005-1075) for sharp noses and for
-    blunt ones at the body's scale (one captured start for the family), on
-    the GPU fit: grids refined by 2 from 20 cells across until the drag's band
-    (grid convergence index plus `floor`) is within `tolerance`; a grid
-    whose fit does not settle, or whose flow fails the checks, stops the run
-    without a value, but a sharp family whose grid fails only the quality
-    gates is solved again with 1.5 times as many columns. Returns a
-    verified_drag.VerifiedDrag."""
+    """verifiedFittedDrag (fitted-flow.ts:1011-1080) for sharp noses and for
+    blunt ones (one captured start for the family; two captures and a shared
+    outer boundary on a two-scale nose), on the GPU fit: noses the reference
+    does not serve refused (blunt_nose_refusal); grids refined by 2 from 20
+    cells across until the drag's band (grid convergence index plus the
+    allowance, `floor` raised to TWO_SCALE_DRAG_FLOOR on a two-scale family)
+    is within `tolerance`; a grid whose fit does not settle, or whose flow
+    fails the checks, stops the run without a value, but a sharp family whose
+    grid fails only the quality gates is solved again with 1.5 times as many
+    columns. Returns a verified_drag.VerifiedDrag."""
     from .verification import refine_until_verified
     from .verified_drag import LevelReport, VerifiedDrag
 
     asked_end = body.nose.length + body.cylinder_length
     reports: list = []
+    refusal = blunt_nose_refusal(body, mach)
+    if refusal is not None:
+        return VerifiedDrag("invalid", None, reports, 1, refusal)
     blunt = None
+    start = None
     if not math.isfinite(_nose_slopes(body)[0]):
         # Blunt: one captured start for the whole family (bluntFitFamily).
         try:
-            blunt = blunt_fit_family(blunt_start(body, mach, FITTED_BASE_NJ, gamma))
+            start = blunt_start(body, mach, FITTED_BASE_NJ, gamma)
+            blunt = blunt_fit_family(start)
         except ValueError as e:
             return VerifiedDrag("invalid", None, reports, 1, str(e))
+    floor = fitted_drag_floor(floor, start)
 
     def family(density: float):
         def solve_at(r: int) -> float:
@@ -655,11 +808,7 @@ def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance:
                 if not converged:
                     raise FitNotConverged(r, f"the fit stopped after {it} iterations with the shock moving at "
                                              f"{speed:.1e} of the sound speed")
-                x = np.empty((p.ni + 1) * (p.nj + 1))
-                y = np.empty_like(x)
-                g._call("bs_fit_nodes", x.ctypes.data_as(C.POINTER(C.c_double)),
-                        y.ctypes.data_as(C.POINTER(C.c_double)))
-                grid = StructuredGrid(p.ni, p.nj, x, y)
+                grid = g.grid()
                 prims = g.primitives().reshape(p.nj, p.ni, 4)
             e = fitted_grid_failure(grid)
             if e is not None:
@@ -677,7 +826,7 @@ def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance:
 
     try:
         try:
-            return VerifiedDrag("solved", family(1.0), reports)
+            return VerifiedDrag("solved", family(1.0), reports, floor=floor)
         except GridRefused as e:
             if blunt is not None:
                 raise
@@ -685,7 +834,7 @@ def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance:
                 on_fallback(e.refinement, str(e))
             reports.clear()
             return VerifiedDrag("solved", family(FALLBACK_COLUMN_DENSITY), reports,
-                                column_density=FALLBACK_COLUMN_DENSITY)
+                                column_density=FALLBACK_COLUMN_DENSITY, floor=floor)
     except FitRefused as e:
         return VerifiedDrag("invalid", None, reports, e.refinement, str(e))
     except FitNotConverged as e:

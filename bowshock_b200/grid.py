@@ -50,6 +50,7 @@ class BodyGrid:
     grid: StructuredGrid
     i_tip: int
     outer_angle: float
+    two_scale: bool = False
 
 
 def _take(handle: C.c_void_p, lib) -> tuple[StructuredGrid, int, float]:
@@ -89,10 +90,12 @@ def body_grid(body: Body, nj: int, mach: float, gamma: float = 1.4, refinement: 
 
 
 def blunt_body_grid(body: Body, nj: int, mach: float, refinement: int = 1, ni: int = 0,
-                    gated: bool = True, lib=None) -> BodyGrid:
+                    gated: bool = True, outer_boundary=None, lib=None) -> BodyGrid:
     """bluntBodyGrid: the C-topology grid of a blunt nose (or of a sharp one
     whose shock detaches); iMin is the axis ahead of the tip. `gated=False`
-    skips the quality gates, as for the reference's two-scale (Haack) noses."""
+    skips the quality gates, as for the reference's two-scale (Haack) noses.
+    `outer_boundary` (n, 2) points (x, y), the first on the axis, y
+    increasing, replaces the generator's arc and line."""
     L = lib or _native.load()
     o = abi.BodyGridOptions()
     o.nj = nj
@@ -103,9 +106,22 @@ def blunt_body_grid(body: Body, nj: int, mach: float, refinement: int = 1, ni: i
     o.gamma = 1.4
     b = body.to_abi()
     h = C.c_void_p()
-    _native.check(L.bs_blunt_body_grid(C.byref(b), C.byref(o), C.byref(h)), L)
+    if outer_boundary is None:
+        ox = oy = np.empty(0)
+    else:
+        pts = np.asarray(outer_boundary, dtype=np.float64).reshape(-1, 2)
+        ox, oy = np.ascontiguousarray(pts[:, 0]), np.ascontiguousarray(pts[:, 1])
+    dp = C.POINTER(C.c_double)
+    _native.check(L.bs_blunt_body_grid_bounded(C.byref(b), C.byref(o), ox.ctypes.data_as(dp),
+                                               oy.ctypes.data_as(dp), len(ox), C.byref(h)), L)
+    two = C.c_int32()
+    try:
+        _native.check(L.bs_grid_two_scale(h, C.byref(two)), L)
+    except BaseException:
+        L.bs_grid_destroy(h)
+        raise
     grid, tip, angle = _take(h, L)
-    return BodyGrid(grid, tip, angle)
+    return BodyGrid(grid, tip, angle, bool(two.value))
 
 
 def ramp_grid(ni: int, nj: int, x_min: float, x_corner: float, x_max: float, height: float,

@@ -67,6 +67,7 @@ class VerifiedDrag:
     refinement: int | None = None
     reason: str | None = None
     column_density: float | None = None   # fitted families solved with more columns than usual
+    floor: float | None = None            # the allowance in a fitted band, relative (fittedDragFloor)
 
 
 def outflow_mach(gamma: float, ni: int, nj: int, cell) -> float:

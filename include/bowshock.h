@@ -428,6 +428,17 @@ BS_API bs_status bs_body_grid(const bs_body *body, const bs_body_grid_options *o
 BS_API bs_status bs_blunt_body_grid(const bs_body *body, const bs_body_grid_options *options,
                                     bs_grid **out);
 
+/* bluntBodyGrid with BluntGridOptions.outerBoundary (src/grid/blunt-grid.ts:42,
+ * 296-331): the outer boundary is the polyline of the n_outer points given
+ * (at least two, the first on the axis, y strictly increasing outwards),
+ * linear between them and continued by its last segment; the lines and
+ * their spacing are placed as for the generator's own boundary. n_outer = 0
+ * is bs_blunt_body_grid. A two-scale nose's fitted family is built on such a
+ * boundary (secondCapture, src/analysis/fitted-flow.ts:624-672). */
+BS_API bs_status bs_blunt_body_grid_bounded(const bs_body *body, const bs_body_grid_options *options,
+                                            const double *outer_x, const double *outer_y,
+                                            int32_t n_outer, bs_grid **out);
+
 /* rampGrid (src/grid/shapes.ts:30-52): a channel whose lower wall turns by
  * `angle` at x_corner. */
 BS_API bs_status bs_ramp_grid(int32_t ni, int32_t nj, double x_min, double x_corner, double x_max,
@@ -438,6 +449,11 @@ BS_API bs_status bs_grid_dims(const bs_grid *grid, int32_t *ni, int32_t *nj);
 BS_API bs_status bs_grid_nodes(const bs_grid *grid, double *x, double *y);
 /* BodyGrid.iTip and outerAngle (src/grid/body-grid.ts:47-54). */
 BS_API bs_status bs_grid_info(const bs_grid *grid, int32_t *i_tip, double *outer_angle);
+/* BluntGrid.twoScale (src/grid/blunt-grid.ts:553): 1 for a C grid whose
+ * generator's boundary is sized for the tip's blunt part, narrower than the
+ * body (Haack and power-series noses, and sharp tips whose shock detaches);
+ * 0 for spheres, ellipsoids and every H grid. */
+BS_API bs_status bs_grid_two_scale(const bs_grid *grid, int32_t *two_scale);
 BS_API bs_status bs_grid_destroy(bs_grid *grid);
 
 /* GridQuality (src/grid/quality.ts:6-21, gridQuality :75-128). */

@@ -160,6 +160,27 @@ def main() -> None:
         "mach": 1.5, "aspect_ratio": float(fb.group(1)), "aspect_limit": int(fb.group(2)),
         "value": float(fv.group(1)), "columns": int(fv.group(2)), "equal_within": 1e-12,
     }
+    # A two-scale family on the CPU engine: the 1-caliber Von Karman nose
+    # with a caliber of body at Mach 2, its fitted drags on nj = 20 and 40.
+    f2 = "tests/analysis/two-scale-fit.test.ts"
+    t2 = (REF / f2).read_text()
+    meas = re.search(r"const MEASURED = \[([0-9.]+), ([0-9.]+)\];", t2)
+    vk = re.search(r"shape: \{ kind: 'haack', parameter: 0 \}, length: ([0-9.]+), baseRadius: ([0-9.]+) \},\s*"
+                   r"cylinderLength: ([0-9.]+),", t2)
+    opts = re.search(r"const familyOptions = \{ mach: ([0-9.]+), gamma, nj: (\d+) \};", t2)
+    out["fitted_von_karman_mach2"] = {
+        "source": f"{f2}:{find_line(t2, 'const MEASURED')}",
+        "body": {"shape": "haack", "parameter": 0, "length": float(vk.group(1)),
+                 "base_radius": float(vk.group(2)), "cylinder": float(vk.group(3))},
+        "mach": float(opts.group(1)), "nj": int(opts.group(2)),
+        "drag_nj20": float(meas.group(1)), "drag_nj40": float(meas.group(2)), "within": 1e-9,
+    }
+    # The two-scale allowance (TWO_SCALE_DRAG_FLOOR).
+    fv2 = "src/analysis/verified-drag.ts"
+    tf = (REF / fv2).read_text()
+    floor = re.search(r"export const TWO_SCALE_DRAG_FLOOR = ([0-9.e-]+);", tf)
+    out["two_scale_drag_floor"] = {"source": f"{fv2}:{find_line(tf, 'export const TWO_SCALE_DRAG_FLOOR')}",
+                                   "value": float(floor.group(1))}
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {OUT}")
 

@@ -4,7 +4,9 @@ behind a fitted shock, the shock compatible with the flow behind it, and
 the Taylor-Maccoll field on rays that starts a fit on a sharp nose."""
 from __future__ import annotations
 
+import json
 import math
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -12,6 +14,8 @@ import pytest
 from bowshock_b200.config import Primitive2D
 from bowshock_b200.fitted import column_positions, compatible_shock, cone_flow_field, shock_state
 from bowshock_b200.grid import normal_shock, oblique_shock
+
+GOLDEN_DIR = Path(__file__).parent / "golden"
 
 GAMMA = 1.4
 DEG = math.pi / 180
@@ -243,3 +247,96 @@ def test_blunt_grid_families_nest():
         assert np.max(np.abs(fr[::r, ::r] - f1)) < 1e-14
     with pytest.raises(ValueError):
         nested_heights(coarse, h1, coarse[:-1], 1)
+
+
+# ---- two-scale noses (no GPU: grids, outline, allowance) ---------------------------
+
+def test_two_scale_family_nests_on_its_outer_boundary():
+    # tests/analysis/fitted-flow.test.ts:179-225: a 3-caliber Haack nose at
+    # Mach 2 is two-scale and keeps its cylinder; every grid of a family on
+    # an outer boundary (here 0.4 of the generator's lines, heights 0.6 of
+    # the base grid's, made up) keeps the base lines, heights and node
+    # fractions at refinements 2, 4 and 8.
+    from bowshock_b200.config import free_stream_at
+    from bowshock_b200.fitted import BluntStart, _grid_lines, blunt_fit_family
+    from bowshock_b200.grid import Body, Nose, NoseShape, blunt_body_grid
+
+    body = Body(Nose(NoseShape("haack", 0.0), 3.0, 0.5), 2.0)
+    first = blunt_body_grid(body, 20, 2.0, gated=False)
+    assert first.two_scale
+    X = first.grid.x.reshape(21, -1)
+    Y = first.grid.y.reshape(21, -1)
+    lines = _grid_lines(first.grid)
+    h = np.hypot(X[20] - X[0], Y[20] - Y[0])
+    boundary = np.stack([lines[:, 0] + 0.4 * h * lines[:, 2], lines[:, 1] + 0.4 * h * lines[:, 3]], 1)
+    base = blunt_body_grid(body, 20, 2.0, gated=False, outer_boundary=boundary).grid
+    bl = _grid_lines(base)
+    Xb = base.x.reshape(21, -1)
+    Yb = base.y.reshape(21, -1)
+    free = free_stream_at(2.0, 1.4).state
+    captured = np.tile([free.rho, free.u, free.v, free.p], (20, base.ni, 1))
+    start = BluntStart(body, 5.0, base, bl, 0.6 * np.hypot(Xb[20] - Xb[0], Yb[20] - Yb[0]), captured, 20, 2.0,
+                       1.4, boundary)
+    family = blunt_fit_family(start)
+    coarse = family(1)
+    assert coarse.ni == base.ni
+    for r in (2, 4, 8):
+        fine = family(r)
+        assert fine.ni == 2 * coarse.ni and fine.nj == 2 * coarse.nj
+        assert np.array_equal(fine.line_x[::2], coarse.line_x) and np.array_equal(fine.line_y[::2], coarse.line_y)
+        assert np.array_equal(fine.heights[::2], coarse.heights)
+        assert np.array_equal(fine.fractions[::2, ::2], coarse.fractions)
+        coarse = fine
+
+
+def test_outer_boundary_refusals_and_the_sphere_is_one_scale():
+    from bowshock_b200._native import BowshockError
+    from bowshock_b200.grid import Body, Nose, NoseShape, blunt_body_grid
+
+    sphere = Body(Nose(NoseShape("ellipsoid"), 0.5, 0.5), 1.0)
+    assert not blunt_body_grid(sphere, 20, 2.0, gated=False).two_scale
+    for bad in ([[-1.0, 0.0]], [[-1.0, 0.1], [0.0, 2.0]], [[-1.0, 0.0], [0.0, 2.0], [1.0, 1.0]]):
+        with pytest.raises(BowshockError, match="outer boundary"):
+            blunt_body_grid(sphere, 20, 2.0, gated=False, outer_boundary=bad)
+
+
+def test_von_karman_outline_and_allowance():
+    # tests/analysis/fitted-flow.test.ts:227-297: ellipsoids and sharp tips
+    # served; Von Karman noses inside the outline of the lengths and Mach
+    # numbers checked; other two-scale noses refused; the allowance raised
+    # on a two-scale start only.
+    from bowshock_b200.fitted import (FITTED_DRAG_FLOOR, TWO_SCALE_DRAG_FLOOR, VON_KARMAN_REFERENCES, BluntStart,
+                                      blunt_nose_refusal, fitted_drag_floor, inside_outline)
+    from bowshock_b200.grid import Body, Nose, NoseShape
+
+    known = json.loads((GOLDEN_DIR / "reference_known_answers.json").read_text())
+    assert TWO_SCALE_DRAG_FLOOR == known["two_scale_drag_floor"]["value"]
+
+    def nose(shape, calibers):
+        return Body(Nose(shape, calibers, 0.5), 1.0)
+
+    vk = NoseShape("haack", 0.0)
+    assert blunt_nose_refusal(nose(NoseShape("ellipsoid"), 6), 1.2) is None
+    for c, m in VON_KARMAN_REFERENCES:
+        assert blunt_nose_refusal(nose(vk, c), m) is None
+    assert "outside the referenced range" in blunt_nose_refusal(nose(vk, 8), 1.2)
+    for c, m in ((5, 3), (6, 3), (4.1, 2.5), (5.6, 2.5), (5.3, 2)):
+        assert blunt_nose_refusal(nose(vk, c), m) is None, (c, m)
+    for c, m in ((5.7, 2.5), (5.4, 2), (6, 2), (6, 1.5), (5.1, 1.5), (6.1, 3)):
+        assert "outside the referenced range" in blunt_nose_refusal(nose(vk, c), m), (c, m)
+    assert "only the Von Karman" in blunt_nose_refusal(nose(NoseShape("haack", 1 / 3), 3), 2)
+    assert "only the Von Karman" in blunt_nose_refusal(nose(NoseShape("power", 0.75), 3), 2)
+    assert blunt_nose_refusal(nose(NoseShape("ogive", 1.0), 1), 1.2) is None
+    assert inside_outline([[3, 2]], [3, 2]) and not inside_outline([[3, 2]], [3, 2.1])
+    assert inside_outline([[1, 2], [3, 2]], [2, 2]) and not inside_outline([[1, 2], [3, 2]], [2, 2.01])
+    quad = [[1, 2], [3, 2], [3, 3], [5, 1.5]]
+    assert all(inside_outline(quad, p) for p in ([3, 2], [4, 2], [5, 1.5]))
+    assert not inside_outline(quad, [5, 2]) and not inside_outline(quad, [1, 1.5])
+    assert not inside_outline(VON_KARMAN_REFERENCES, [6, 1.5]) and not inside_outline(VON_KARMAN_REFERENCES, [6, 2])
+
+    def start(boundary):
+        return BluntStart(None, 0.0, None, None, None, None, 20, 2.0, 1.4, boundary)
+
+    assert fitted_drag_floor(FITTED_DRAG_FLOOR, None) == FITTED_DRAG_FLOOR
+    assert fitted_drag_floor(FITTED_DRAG_FLOOR, start(None)) == FITTED_DRAG_FLOOR
+    assert fitted_drag_floor(FITTED_DRAG_FLOOR, start(np.array([[-1.0, 0.0]]))) == TWO_SCALE_DRAG_FLOOR
