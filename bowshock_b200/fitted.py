@@ -6,6 +6,7 @@ native library.
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 import math
 from dataclasses import dataclass
 
@@ -265,6 +266,7 @@ class CudaFit:
             initial.ctypes.data_as(dp), C.byref(h)), self._lib)
         self._h = h
         self._keep = (arrays, inflow, initial)
+        self.rate = math.nan   # the drag's convergence rate per check, once settled (settle)
 
     def destroy(self) -> None:
         if self._h:
@@ -339,7 +341,7 @@ class CudaFit:
 
 
 def settle(fit: CudaFit, max_iterations: int, noise: float = 1e-7, speed_tolerance: float = 1e-6,
-           check_every: int = 250):
+           check_every: int = 250, known_rate: float = math.nan):
     """The GPU fit's stopping rule (fitShockGpu, src/engine-gpu/shock-fitting-gpu.ts:
     135-170): every `check_every` steps the drag is added to a SettlingValue of
     `noise`; the fit has converged once the drag has settled and the shock
@@ -347,22 +349,56 @@ def settle(fit: CudaFit, max_iterations: int, noise: float = 1e-7, speed_toleran
     the metrics FP32: the shock's speeds settle near 1e-7 (the reference's
     all-FP32 engine: 1e-6 to 4e-6, against its tolerance of 3e-5), and the
     drag at a few 1e-8 on slowly settling fits, hence the noise of 1e-7.
+    `known_rate`: the drag's rate of convergence per check on the grid
+    before, for a fit started from that grid's (it may begin too close to
+    its limit to show its own). Leaves the rate to pass on in fit.rate.
     Returns (converged, iterations, max speed, drag)."""
     from .verification import SettlingValue
 
-    settling = SettlingValue(noise)
+    settling = SettlingValue(noise, known_rate)
     done, speed, drag = 0, math.inf, math.nan
-    while done < max_iterations:
-        n = min(check_every, max_iterations - done)
-        fit.iterate(n)
-        done += n
-        speed, _ = fit.check()
-        drag = fit.drag()
-        if not math.isfinite(drag):
-            break
-        if settling.add(drag) and speed < speed_tolerance:
-            return True, done, speed, drag
-    return False, done, speed, drag
+    try:
+        while done < max_iterations:
+            n = min(check_every, max_iterations - done)
+            fit.iterate(n)
+            done += n
+            speed, _ = fit.check()
+            drag = fit.drag()
+            if not math.isfinite(drag):
+                break
+            if settling.add(drag) and speed < speed_tolerance:
+                return True, done, speed, drag
+        return False, done, speed, drag
+    finally:
+        fit.rate = settling.rate_to_pass_on
+
+
+def started_from(fine: FitProblem, coarse: FitProblem, heights: np.ndarray, cells: np.ndarray) -> FitProblem | None:
+    """startedFrom (src/analysis/gpu-fitted-flow.ts:116-146): the problem on
+    the grid refined by 2, started from the settled fit on `coarse` (its
+    shock heights and its cells (nj, ni, 4)): on nested grids each fine cell
+    lies inside one coarse cell, whose state it takes, and the heights of the
+    new lines are interpolated in x between their neighbours. None where the
+    grids do not nest (a line or node fraction of the coarse grid missing
+    from the fine one, within 1e-12). The settled state does not depend on
+    the start; only the steps to reach it do."""
+    n, nj = coarse.ni, coarse.nj
+    if fine.ni != 2 * n or fine.nj != 2 * nj:
+        return None
+    scale = abs(coarse.line_x[n] - coarse.line_x[0])
+    if not (np.all(np.abs(fine.line_x[::2] - coarse.line_x) <= 1e-12 * scale)
+            and np.all(np.abs(fine.line_y[::2] - coarse.line_y) <= 1e-12 * scale)
+            and np.all(np.abs(fine.fractions[::2, ::2] - coarse.fractions) <= 1e-12)):
+        return None
+    h = np.asarray(heights, np.float64)
+    new = np.empty(fine.ni + 1)
+    new[::2] = h
+    ax, bx = coarse.line_x[:-1], coarse.line_x[1:]
+    t = (fine.line_x[1::2] - ax) / (bx - ax)
+    new[1::2] = h[:-1] * (1 - t) + h[1:] * t
+    c = np.asarray(cells, np.float64).reshape(nj, n, 4)
+    initial = np.repeat(np.repeat(c, 2, axis=0), 2, axis=1)
+    return dataclasses.replace(fine, heights=new, initial=initial.reshape(-1, 4))
 
 
 # ---- the blunt-nose fit problem -------------------------------------------------
@@ -767,16 +803,21 @@ def fitted_case_failure(problem: FitProblem, asked_end: float, grid: StructuredG
 def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance: float = 1e-4,
                          max_refinement: int = 8, floor: float = FITTED_DRAG_FLOOR,
                          iterations_per_refinement: int = 200000, on_level=None, on_fallback=None):
-    """verifiedFittedDrag (fitted-flow.ts:1011-1080) for sharp noses and for
-    blunt ones (one captured start for the family; two captures and a shared
-    outer boundary on a two-scale nose), on the GPU fit: noses the reference
-    does not serve refused (blunt_nose_refusal); grids refined by 2 from 20
-    cells across until the drag's band (grid convergence index plus the
-    allowance, `floor` raised to TWO_SCALE_DRAG_FLOOR on a two-scale family)
-    is within `tolerance`; a grid whose fit does not settle, or whose flow
-    fails the checks, stops the run without a value, but a sharp family whose
-    grid fails only the quality gates is solved again with 1.5 times as many
-    columns. Returns a verified_drag.VerifiedDrag."""
+    """The verified fitted drag as the reference's GPU driver computes it
+    (verifiedFittedDragGpu, src/analysis/gpu-fitted-flow.ts:197-338, the
+    procedure of verifiedFittedDrag, fitted-flow.ts:1011-1080), for sharp
+    noses and for blunt ones (one captured start for the family; two
+    captures and a shared outer boundary on a two-scale nose): noses the
+    reference does not serve refused (blunt_nose_refusal); grids refined by 2
+    from 20 cells across until the drag's band (grid convergence index plus
+    the allowance, `floor` raised to TWO_SCALE_DRAG_FLOOR on a two-scale
+    family) is within `tolerance`, each finer grid started from the settled
+    fit before it (started_from) with that fit's rate of convergence. A
+    first grid whose fit does not settle stops the run without a value; on a
+    finer grid (or one too large for the GPU) the band of the grids before it
+    stands (result.stopped). A flow failing the checks is refused, but a
+    sharp family whose grid fails only the quality gates is solved again with
+    1.5 times as many columns. Returns a verified_drag.VerifiedDrag."""
     from .verification import refine_until_verified
     from .verified_drag import LevelReport, VerifiedDrag
 
@@ -797,32 +838,54 @@ def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance:
     floor = fitted_drag_floor(floor, start)
 
     def family(density: float):
+        # The last grid's problem, its settled fit and its rate, to start the next from.
+        previous: list = []
+
         def solve_at(r: int) -> float:
             if blunt is not None:
-                p = blunt(r)
+                fresh = blunt(r)
             else:
-                p = sharp_fit_problem(body, mach, nj=FITTED_BASE_NJ, refinement=r, gamma=gamma,
-                                      column_density=density)
+                fresh = sharp_fit_problem(body, mach, nj=FITTED_BASE_NJ, refinement=r, gamma=gamma,
+                                          column_density=density)
+            p, rate = fresh, math.nan
+            if previous:
+                coarse, heights, cells, rate = previous[-1]
+                p = started_from(fresh, coarse, heights, cells) or fresh
             with CudaFit(p) as g:
-                converged, it, speed, drag = settle(g, iterations_per_refinement * r, check_every=250 * r)
+                converged, it, speed, drag = settle(g, iterations_per_refinement * r, check_every=250 * r,
+                                                    known_rate=rate)
                 if not converged:
                     raise FitNotConverged(r, f"the fit stopped after {it} iterations with the shock moving at "
-                                             f"{speed:.1e} of the sound speed")
+                                             f"{speed:.1e} of the sound speed or the drag still changing")
                 grid = g.grid()
                 prims = g.primitives().reshape(p.nj, p.ni, 4)
+                settled = (p, g.heights(), prims, g.rate)
             e = fitted_grid_failure(grid)
             if e is not None:
                 raise GridRefused(r, e)
             e = fitted_case_failure(p, asked_end, grid, prims)
             if e is not None:
                 raise FitRefused(r, e)
+            previous[:] = [settled]
             rep = LevelReport(r, p.ni, p.nj, it, drag)
             reports.append(rep)
             if on_level is not None:
                 on_level(rep)
             return drag
 
-        return refine_until_verified(solve_at, tolerance, floor, max_refinement, 0.5, FITTED_NOISE)
+        def stop_on(e: Exception) -> str | None:
+            # A finer grid too large for the GPU, or whose fit does not
+            # settle, leaves the band of the grids before it; a case refused
+            # on any grid stays refused (verifiedFittedDragGpu's stopOn).
+            if isinstance(e, FitRefused):
+                return None
+            if isinstance(e, FitNotConverged):
+                return f"its fit did not converge ({e})"
+            if isinstance(e, _native.BowshockError) and e.status == abi.BS_MEMORY_LIMIT:
+                return str(e)
+            return None
+
+        return refine_until_verified(solve_at, tolerance, floor, max_refinement, 0.5, FITTED_NOISE, stop_on)
 
     try:
         try:

@@ -258,7 +258,7 @@ def test_two_scale_family_nests_on_its_outer_boundary():
     # the base grid's, made up) keeps the base lines, heights and node
     # fractions at refinements 2, 4 and 8.
     from bowshock_b200.config import free_stream_at
-    from bowshock_b200.fitted import BluntStart, _grid_lines, blunt_fit_family
+    from bowshock_b200.fitted import BluntStart, _grid_lines, blunt_fit_family, started_from
     from bowshock_b200.grid import Body, Nose, NoseShape, blunt_body_grid
 
     body = Body(Nose(NoseShape("haack", 0.0), 3.0, 0.5), 2.0)
@@ -286,7 +286,18 @@ def test_two_scale_family_nests_on_its_outer_boundary():
         assert np.array_equal(fine.line_x[::2], coarse.line_x) and np.array_equal(fine.line_y[::2], coarse.line_y)
         assert np.array_equal(fine.heights[::2], coarse.heights)
         assert np.array_equal(fine.fractions[::2, ::2], coarse.fractions)
+        # startedFrom (src/analysis/gpu-fitted-flow.ts:116-146) takes the
+        # nested grid: the coarse heights on the shared lines, each fine cell
+        # the coarse cell it lies in.
+        cells = np.arange(coarse.nj * coarse.ni * 4, dtype=np.float64).reshape(coarse.nj, coarse.ni, 4)
+        moved = 1.01 * coarse.heights
+        s = started_from(fine, coarse, moved, cells)
+        assert s is not None and np.array_equal(s.heights[::2], moved)
+        assert np.all((s.heights[1::2] - moved[:-1]) * (s.heights[1::2] - moved[1:]) <= 0)
+        w = s.initial.reshape(fine.nj, fine.ni, 4)
+        assert np.array_equal(w[1::2, 1::2], cells) and np.array_equal(w[::2, 1::2], cells)
         coarse = fine
+    assert started_from(family(4), family(1), family(1).heights, cells[:20, :base.ni]) is None
 
 
 def test_outer_boundary_refusals_and_the_sphere_is_one_scale():
