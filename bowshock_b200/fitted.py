@@ -184,8 +184,9 @@ def sharp_fit_problem(asked: Body, mach: float, nj: int = 10, refinement: int = 
     try:
         _, _, cone = cone_flow_field(mach, tip_angle, gamma, [tip_angle])
     except _native.BowshockError as e:
-        raise ValueError(f"at Mach {mach} the bow shock cannot stay attached to a tip of "
-                         f"{math.degrees(tip_angle):.1f} deg half-angle") from e
+        raise ValueError(f"at Mach {_number(mach)} the bow shock cannot stay attached to a tip of "
+                         f"{math.degrees(tip_angle):.1f} deg half-angle; this needs a sharper or longer nose, "
+                         "or a higher Mach number") from e
     beta = cone.shock_angle
     enthalpy = gamma / (gamma - 1) + 0.5 * free.u * free.u
     v_max = math.sqrt(2 * enthalpy)
@@ -231,9 +232,20 @@ def sharp_fit_problem(asked: Body, mach: float, nj: int = 10, refinement: int = 
     surface = conical(tip_angle)[0]
     a_s = math.sqrt(gamma * surface[3] / surface[0])
     surface_mach = math.hypot(surface[1], surface[2]) / a_s
-    if not surface[1] / a_s > 1 and (not surface_mach > 1 or base_slope > 0):
-        raise ValueError(f"at Mach {mach} the flow behind a tip of {math.degrees(tip_angle):.1f} deg half-angle "
-                         "crosses the starting plane subsonically")
+    axial_mach = surface[1] / a_s
+    if not axial_mach > 1 and (not surface_mach > 1 or base_slope > 0):
+        degrees = f"{math.degrees(tip_angle):.1f}"
+        if surface_mach > 1:
+            raise ValueError(
+                f"at Mach {_number(mach)} the flow behind a tip of {degrees} deg half-angle crosses the solver's "
+                f"starting plane, normal to the axis, at an axial Mach number of {axial_mach:.2f} at the surface, "
+                "below 1, which this solver handles only where the nose meets the body without a corner: at a "
+                "corner the drag converges too slowly to be verified; this needs a sharper or longer nose, a nose "
+                "tangent to the body, or a higher Mach number")
+        raise ValueError(
+            f"at Mach {_number(mach)} the flow over a tip of {degrees} deg half-angle is subsonic at the surface "
+            f"(Mach {surface_mach:.2f}), so the body behind the tip reaches it, which this solver does not handle "
+            "yet; this needs a sharper or longer nose, or a higher Mach number")
     cx = 0.25 * (X[:-1, :-1] + X[:-1, 1:] + X[1:, :-1] + X[1:, 1:])
     cy = 0.25 * (Y[:-1, :-1] + Y[:-1, 1:] + Y[1:, :-1] + Y[1:, 1:])
     problem.initial = conical(np.arctan2(cy, cx).ravel())
@@ -516,6 +528,29 @@ def _capture(body: Body, grid: StructuredGrid, mach: float, gamma: float) -> np.
         return e.primitives().reshape(grid.nj, grid.ni, 4)
 
 
+def solved_blunt_body(asked: Body, mach: float, nj: int = 20):
+    """solvedBluntBody (fitted-flow.ts:154-222): the body a blunt nose's fit
+    solves and its start grid (ungated). The cylinder is at least a caliber
+    and is lengthened a caliber at a time, by at most seven, until the C
+    grid's neighbouring cells differ in size by no more than the fitted
+    grids' gate allows (1.3); if none passes, the shortest. A two-scale nose
+    keeps the shortest, its family being built on its captured shock.
+    Returns (body, grid.BodyGrid)."""
+    from .grid import blunt_body_grid, grid_quality
+
+    caliber = 2 * asked.nose.base_radius
+    shortest = max(asked.cylinder_length, SOLVED_CYLINDER * caliber)
+    first = None
+    for extra in range(MAX_BLUNT_EXTENSION + 1):
+        body = Body(asked.nose, shortest + extra * caliber)
+        bg = blunt_body_grid(body, nj, mach, gated=False)
+        if bg.two_scale or grid_quality(bg.grid).max_size_ratio <= FITTED_MAX_SIZE_RATIO:
+            return body, bg
+        if first is None:
+            first = (body, bg)
+    return first
+
+
 def blunt_start(asked: Body, mach: float, nj: int = 20, gamma: float = 1.4) -> BluntStart:
     """bluntStart (fitted-flow.ts:498-508): the body's cylinder lengthened a
     caliber at a time until its C grid meets the fitted grids' size-ratio
@@ -525,23 +560,10 @@ def blunt_start(asked: Body, mach: float, nj: int = 20, gamma: float = 1.4) -> B
     two-scale nose (Haack, power series: the generator's boundary is sized
     for the tip) a second capture on the grid built on the first captured
     shock (two_scale_boundary), whose boundary the family then shares."""
-    from .grid import blunt_body_grid, grid_quality
+    from .grid import blunt_body_grid
 
     R = asked.nose.base_radius
-    caliber = 2 * R
-    shortest = max(asked.cylinder_length, SOLVED_CYLINDER * caliber)
-    chosen = None
-    for extra in range(MAX_BLUNT_EXTENSION + 1):
-        body = Body(asked.nose, shortest + extra * caliber)
-        bg = blunt_body_grid(body, nj, mach, gated=False)
-        if chosen is None:
-            chosen = (body, bg)
-        if bg.two_scale:
-            break
-        if grid_quality(bg.grid).max_size_ratio <= FITTED_MAX_SIZE_RATIO:
-            chosen = (body, bg)
-            break
-    body, bg = chosen
+    body, bg = solved_blunt_body(asked, mach, nj)
     free = free_stream_at(mach, gamma).state
 
     def heights_of(grid: StructuredGrid, captured: np.ndarray):

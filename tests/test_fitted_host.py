@@ -351,3 +351,130 @@ def test_von_karman_outline_and_allowance():
     assert fitted_drag_floor(FITTED_DRAG_FLOOR, None) == FITTED_DRAG_FLOOR
     assert fitted_drag_floor(FITTED_DRAG_FLOOR, start(None)) == FITTED_DRAG_FLOOR
     assert fitted_drag_floor(FITTED_DRAG_FLOOR, start(np.array([[-1.0, 0.0]]))) == TWO_SCALE_DRAG_FLOOR
+
+
+# ---- the fitted problems' refusals and bodies (tests/analysis/fitted-flow.test.ts:115-178, 361-488) --------
+
+def _ogive_body(length: float, cylinder: float, parameter: float = 1.0):
+    from bowshock_b200.grid import Body, Nose, NoseShape
+
+    return Body(Nose(NoseShape("ogive", parameter), length, 0.5), cylinder)
+
+
+def _cone(angle_deg: float, cylinder: float):
+    from bowshock_b200.grid import Body, Nose, NoseShape
+
+    return Body(Nose(NoseShape("conical"), 0.5 / math.tan(angle_deg * DEG), 0.5), cylinder)
+
+
+def test_sharp_tips_refused_with_their_angle_and_what_to_change():
+    from bowshock_b200.fitted import sharp_fit_problem
+
+    with pytest.raises(ValueError, match=r"at Mach 1.2 the bow shock cannot stay attached to a tip of 45.0 deg "
+                                         r"half-angle; this needs a sharper or longer nose"):
+        sharp_fit_problem(_cone(45, 2.0), 1.2, nj=20)
+    ogive = _ogive_body(3.0, 2.0)
+    with pytest.raises(ValueError, match=r"at Mach 1.2 the flow over a tip of 18.9 deg half-angle is subsonic at "
+                                         r"the surface \(Mach 0.85\)"):
+        sharp_fit_problem(ogive, 1.2, nj=20)
+    sharp_fit_problem(ogive, 1.5, nj=20)
+    for r in (1, 8):
+        sharp_fit_problem(ogive, 1.35, nj=20, refinement=r)
+    short = _ogive_body(2.0, 2.0)
+    sharp_fit_problem(short, 1.6, nj=20)
+    with pytest.raises(ValueError, match=r"is subsonic at the surface \(Mach 0.99\)"):
+        sharp_fit_problem(short, 1.59, nj=20)
+    for r in (1, 8):
+        with pytest.raises(ValueError, match=r"crosses the solver's starting plane, normal to the axis, at an axial "
+                                             r"Mach number of 0.95 at the surface, below 1, which this solver "
+                                             r"handles only where the nose meets the body without a corner"):
+            sharp_fit_problem(_cone(24, 2.0), 1.5, nj=20, refinement=r)
+
+
+def test_a_36_deg_tip_passes_the_fitted_gates_but_not_the_generated_ones():
+    # The secant ogive (0.5) of 1 caliber at Mach 3: wall cells near 53 deg,
+    # below the generated grids' 60 deg, above the fitted grids' 50.
+    from bowshock_b200.fitted import fitted_grid_failure, sharp_fit_problem
+    from bowshock_b200.grid import grid_quality
+
+    p = sharp_fit_problem(_ogive_body(1.0, 2.0, 0.5), 3.0, nj=20)
+    g = p.grid()
+    q = grid_quality(g)
+    assert 50 * DEG < q.min_wall_angle < 60 * DEG
+    assert fitted_grid_failure(g) is None
+
+
+def test_base_flow_is_tested_at_the_end_of_the_body_asked_for():
+    # A cylinder shorter than the caliber always solved ends inside a column:
+    # the axial Mach number there, interpolated between the columns; a bare
+    # nose ends on a grid line, the column just ahead of it tested.
+    from bowshock_b200.fitted import base_mach, sharp_fit_problem
+
+    g = 1.4
+    cone = _cone(20, 0.3)
+    p = sharp_fit_problem(cone, 3.0, nj=20)
+    end = cone.nose.length + 0.3
+    assert not np.any(np.abs(p.line_x - end) < 1e-9)
+
+    def mach(x):
+        return 0.5 + 0.2 * x
+
+    def flow(problem):
+        xc = 0.5 * (problem.line_x[:-1] + problem.line_x[1:])
+        w = np.zeros((problem.nj, problem.ni, 4))
+        w[..., 0] = 1
+        w[..., 1] = math.sqrt(g) * mach(xc)[None, :]
+        w[..., 3] = 1
+        return w
+
+    assert abs(base_mach(p, end, flow(p)) - mach(end)) < 1e-12
+    bare = _cone(20, 0.0)
+    p0 = sharp_fit_problem(bare, 3.0, nj=20)
+    corner = int(np.nonzero(p0.line_x == bare.nose.length)[0][0])
+    assert corner > 0
+    ahead = mach(0.5 * (p0.line_x[corner - 1] + p0.line_x[corner]))
+    assert abs(base_mach(p0, bare.nose.length, flow(p0)) - ahead) < 1e-12
+
+
+def test_a_blunt_nose_cylinder_is_lengthened_until_its_start_grid_meets_the_size_ratio_gate():
+    # The 1.5-caliber ellipsoid at Mach 1.2 on one caliber of cylinder: its
+    # start grid passes on three; the 3:1 ellipsoid with two calibers at
+    # Mach 2 keeps its cylinder; a bare nose gets the caliber always solved.
+    from bowshock_b200.fitted import FITTED_MAX_SIZE_RATIO, solved_blunt_body
+    from bowshock_b200.grid import Body, Nose, NoseShape, grid_quality
+
+    asked = Body(Nose(NoseShape("ellipsoid"), 1.5, 0.5), 1.0)
+    body, bg = solved_blunt_body(asked, 1.2, 20)
+    assert body.cylinder_length == 3.0 and body.nose == asked.nose
+    assert grid_quality(bg.grid).max_size_ratio <= FITTED_MAX_SIZE_RATIO
+    e3 = Body(Nose(NoseShape("ellipsoid"), 3.0, 0.5), 2.0)
+    assert solved_blunt_body(e3, 2.0, 20)[0].cylinder_length == 2.0
+    assert solved_blunt_body(Body(e3.nose, 0.0), 3.0, 20)[0].cylinder_length == 1.0
+
+
+def test_a_lengthened_blunt_family_nests_at_mach_1_2():
+    # What started_from and nested_heights need, on a family whose cylinder
+    # is lengthened; the start's heights are made up (0.4 of each line).
+    from bowshock_b200.config import free_stream_at
+    from bowshock_b200.fitted import BluntStart, _grid_lines, blunt_fit_family, solved_blunt_body, started_from
+    from bowshock_b200.grid import Body, Nose, NoseShape
+
+    asked = Body(Nose(NoseShape("ellipsoid"), 1.5, 0.5), 1.0)
+    body, bg = solved_blunt_body(asked, 1.2, 20)
+    lines = _grid_lines(bg.grid)
+    X = bg.grid.x.reshape(21, -1)
+    Y = bg.grid.y.reshape(21, -1)
+    free = free_stream_at(1.2, 1.4).state
+    captured = np.tile([free.rho, free.u, free.v, free.p], (20, bg.grid.ni, 1))
+    start = BluntStart(body, 2.5, bg.grid, lines, 0.4 * np.hypot(X[20] - X[0], Y[20] - Y[0]), captured, 20, 1.2, 1.4)
+    family = blunt_fit_family(start)
+    coarse = family(1)
+    assert coarse.line_x[-1] == body.nose.length + body.cylinder_length
+    for r in (2, 4, 8):
+        fine = family(r)
+        assert fine.ni == 2 * coarse.ni and fine.nj == 2 * coarse.nj
+        assert np.array_equal(fine.line_x[::2], coarse.line_x) and np.array_equal(fine.line_y[::2], coarse.line_y)
+        assert np.array_equal(fine.heights[::2], coarse.heights)
+        assert np.array_equal(fine.fractions[::2, ::2], coarse.fractions)
+        assert started_from(fine, coarse, coarse.heights, coarse.initial) is not None
+        coarse = fine

@@ -207,3 +207,31 @@ def test_verified_fitted_drag_of_a_blunt_nose():
     v = out.result
     assert v.verified and v.uncertainty <= 1e-3 and len(v.levels) >= 2
     assert abs(v.levels[0][1] - out.reports[0].drag) == 0.0
+
+
+def test_a_bare_nose_is_solved_with_a_cylinder_only_where_its_base_flow_is_supersonic():
+    # tests/analysis/fitted-flow.test.ts:413-426: the bare 20 deg cone at
+    # Mach 3, solved on a caliber of cylinder, leaves its base at Mach 2; the
+    # same grid with the flow slowed to Mach 0.42 is refused.
+    from bowshock_b200.fitted import base_mach
+    from bowshock_b200.grid import Body, Nose, NoseShape
+
+    bare = Body(Nose(NoseShape("conical"), 0.5 / math.tan(20 * math.pi / 180), 0.5), 0.0)
+    p = sharp_fit_problem(bare, 3.0, nj=20)
+    with CudaFit(p) as g:
+        converged, _, _, _ = settle(g, 20000, check_every=250)
+        prims = g.primitives().reshape(p.nj, p.ni, 4)
+    assert converged
+    assert base_mach(p, bare.nose.length, prims) > 1
+    slow = np.tile([1.0, 0.5, 0.0, 1.0], (p.nj, p.ni, 1))
+    assert base_mach(p, bare.nose.length, slow) < 1
+
+
+def test_verified_fitted_drag_without_convergence_gives_only_the_reason():
+    # tests/analysis/fitted-flow.test.ts:569-588: ten steps per grid.
+    from bowshock_b200.fitted import verified_fitted_drag
+
+    out = verified_fitted_drag(cone_body(20, 1.0), 3.0, tolerance=0.0, floor=0.0, max_refinement=8,
+                               iterations_per_refinement=10)
+    assert out.kind == "not-converged" and out.refinement == 1 and out.result is None
+    assert "the fit stopped after 10 iterations" in out.reason
