@@ -88,6 +88,10 @@ SIGNATURES: dict[str, list] = {
     "bs_batch_set_anderson": [_vp, C.c_int32, C.c_int32],
     "bs_batch_anderson_restarts": [_vp, _ip],
     "bs_engine_set_anderson": [_vp, C.c_int32, C.c_int32],
+    "bs_engine_iterate_accelerated": [_vp, C.c_int32, C.c_double, C.c_double, C.c_double],
+    "bs_engine_anderson_restarts": [_vp, _ip],
+    "bs_engine_set_metric_precision": [_vp, C.c_int32],
+    "bs_batch_set_metric_precision": [_vp, C.c_int32],
     "bs_batch_forebody_drag": [_vp, C.c_int32, C.c_double, C.c_double, C.c_double, _dp],
     "bs_batch_read_primitives": [_vp, C.c_int32, _dp],
     "bs_batch_density_residual_norms": [_vp, _dp],
@@ -105,6 +109,8 @@ SIGNATURES: dict[str, list] = {
     "bs_grid_nodes": [_vp, _dp, _dp],
     "bs_grid_info": [_vp, _ip, _dp],
     "bs_grid_two_scale": [_vp, _ip],
+    "bs_transonic_grid": [C.POINTER(abi.Body), C.POINTER(abi.TransonicGridOptions), C.POINTER(_vp)],
+    "bs_grid_transonic_info": [_vp, _ip, _ip, _dp, _dp, _dp],
     "bs_grid_destroy": [_vp],
     "bs_grid_quality_of": [C.c_int32, C.c_int32, _dp, _dp, C.POINTER(abi.GridQuality)],
     "bs_taylor_maccoll": [C.c_double, C.c_double, C.c_double, C.c_double,

@@ -115,6 +115,21 @@ class BodyGridOptions(C.Structure):
     ]
 
 
+class TransonicGridOptions(C.Structure):
+    _fields_ = [
+        ("refinement", C.c_int32),
+        ("reserved", C.c_int32),
+        ("far_field", C.c_double),
+        ("cylinder", C.c_double),
+        ("wall", C.c_double),
+        ("growth", C.c_double),
+        ("tip", C.c_double),
+        ("shoulder", C.c_double),
+        ("nose", C.c_double),
+        ("nose_growth", C.c_double),
+    ]
+
+
 class GridQuality(C.Structure):
     _fields_ = [
         ("min_angle", C.c_double),

@@ -68,6 +68,10 @@ class CudaBatch:
                    1 if relative else 0, max_steps, check_every, out)
         return list(out)
 
+    def set_metric_precision(self, bits: int) -> None:
+        """64: two-float metrics in the residual; 32: FP32 metrics (default)."""
+        self._call("bs_batch_set_metric_precision", int(bits))
+
     def set_anderson(self, depth: int, plain_steps: int = 30) -> None:
         """Anderson acceleration of later LU-SGS solves: `depth` differences
         kept (0: plain steps), after `plain_steps` plain steps."""

@@ -8,7 +8,9 @@
 //   cells      float2 (volume, planar area) at `cell`;
 //   LU-SGS     per-cell sweep records and corrections in diagonal-major
 //              order, (ni + nj - 1) nj slots at `skew` (skew_slot).
-// Metrics are computed in FP64 on the host and stored as FP32. The state is
+// Metrics are computed in FP64 on the host and stored as FP32; with the
+// two-float metrics on, also each value's FP32 low part (the FP64 value less
+// the FP32 one), which the residual adds back (about 48 bits). The state is
 // stored in the solve's arithmetic type R: double for the steady solves
 // (the residual that decides convergence is evaluated in FP64), float for
 // the reference GPU engine's all-FP32 arithmetic.
@@ -81,7 +83,40 @@ struct MetricsView {
   const float4* iface;  // (nx, ny, area, 0)
   const float4* jface;
   const float2* cell;   // (volume, planar area)
+  // Low parts of the same values, or null (FP32 metrics).
+  const float4* iface_lo = nullptr;
+  const float4* jface_lo = nullptr;
+  const float2* cell_lo = nullptr;
 };
+
+// A face's unit normal and area in the arithmetic R: the FP32 values, plus
+// their low parts where the two-float metrics are on.
+template <class R>
+struct FaceGeom {
+  R nx, ny, area;
+};
+
+template <class R>
+__device__ __forceinline__ FaceGeom<R> face_geom(const float4* hi, const float4* lo, int64_t idx) {
+  const float4 h = hi[idx];
+  if (lo == nullptr) return {R(h.x), R(h.y), R(h.z)};
+  const float4 l = lo[idx];
+  return {R(h.x) + R(l.x), R(h.y) + R(l.y), R(h.z) + R(l.z)};
+}
+
+// A cell's volume and planar area (the axisymmetric source's weight) in R.
+template <class R>
+__device__ __forceinline__ void cell_geom(const MetricsView& m, int64_t k, R* volume, R* planar) {
+  const float2 h = m.cell[k];
+  if (m.cell_lo == nullptr) {
+    *volume = R(h.x);
+    *planar = R(h.y);
+    return;
+  }
+  const float2 l = m.cell_lo[k];
+  *volume = R(h.x) + R(l.x);
+  *planar = R(h.y) + R(l.y);
+}
 
 // The conserved state of cell (i, j) of a case, for i in [-2, ni + 1] with j in
 // range or j in [-2, nj + 1] with i in range: interior cells from `at(k)`,
@@ -97,23 +132,26 @@ __device__ __forceinline__ Cons<R> cell_or_ghost(const CaseDev& cd, const Metric
   const int ni = cd.ni, nj = cd.nj;
   if (i >= 0 && i < ni && j >= 0 && j < nj) return at(cd.cell + i + int64_t(j) * ni);
   int side, mi, mj, wi, wj, ii, ij;
-  float4 f;
+  // The boundary face's metrics: array, low parts and index.
+  const float4* fa;
+  const float4* fl;
+  int64_t fk;
   if (i < 0) {
     side = BS_IMIN;
     mi = -1 - i; mj = j; wi = i + ni; wj = j; ii = 0; ij = j;
-    f = m.iface[cd.iface + int64_t(j) * (ni + 1)];
+    fa = m.iface; fl = m.iface_lo; fk = cd.iface + int64_t(j) * (ni + 1);
   } else if (i >= ni) {
     side = BS_IMAX;
     mi = 2 * ni - 1 - i; mj = j; wi = i - ni; wj = j; ii = ni - 1; ij = j;
-    f = m.iface[cd.iface + ni + int64_t(j) * (ni + 1)];
+    fa = m.iface; fl = m.iface_lo; fk = cd.iface + ni + int64_t(j) * (ni + 1);
   } else if (j < 0) {
     side = BS_JMIN;
     mi = i; mj = -1 - j; wi = i; wj = j + nj; ii = i; ij = 0;
-    f = m.jface[cd.jface + i];
+    fa = m.jface; fl = m.jface_lo; fk = cd.jface + i;
   } else {
     side = BS_JMAX;
     mi = i; mj = 2 * nj - 1 - j; wi = i; wj = j - nj; ii = i; ij = nj - 1;
-    f = m.jface[cd.jface + i + int64_t(nj) * ni];
+    fa = m.jface; fl = m.jface_lo; fk = cd.jface + i + int64_t(nj) * ni;
   }
   const int kind = cd.bc[side];
   if (kind == BS_BC_FACE_STATES) {
@@ -135,12 +173,14 @@ __device__ __forceinline__ Cons<R> cell_or_ghost(const CaseDev& cd, const Metric
     const double* s = cd.inflow_prim[side];
     const Prim<R> fr{R(s[0]), R(s[1]), R(s[2]), R(s[3])};
     const R sgn = (side == BS_IMIN || side == BS_JMIN) ? R(-1) : R(1);
-    return to_cons(far_field_state(inside, fr, sgn * R(f.x), sgn * R(f.y), gamma), gamma);
+    const FaceGeom<R> f = face_geom<R>(fa, fl, fk);
+    return to_cons(far_field_state(inside, fr, sgn * f.nx, sgn * f.ny, gamma), gamma);
   }
   if (kind == BS_BC_PERIODIC) return at(cd.cell + wi + int64_t(wj) * ni);
   Cons<R> c = at(cd.cell + mi + int64_t(mj) * ni);
   if (kind == BS_BC_WALL) {
-    const R nx = R(f.x), ny = R(f.y);
+    const FaceGeom<R> f = face_geom<R>(fa, fl, fk);
+    const R nx = f.nx, ny = f.ny;
     const R mn = c.mu * nx + c.mv * ny;
     c.mu = c.mu - R(2) * mn * nx;
     c.mv = c.mv - R(2) * mn * ny;

@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(TILE_THREADS, kMinBlocks) tile_kernel(const Ti
     if (f < nfi) {
       const int fl = f % (ti + 1), fr = f / (ti + 1);
       const int gi = i0 + fl, gj = j0 + fr;
-      const float4 fm = A.m.iface[cd.iface + gi + int64_t(gj) * (ni + 1)];
+      const FaceGeom<R> fm = face_geom<R>(A.m.iface, A.m.iface_lo, cd.iface + gi + int64_t(gj) * (ni + 1));
       const int sj = fr + 2, si = fl + 2;
       const double* imposed = (gi == 0 || gi == ni) ? cd.face_flux[gi == 0 ? BS_IMIN : BS_IMAX] : nullptr;
       if (imposed != nullptr) {
@@ -132,18 +132,18 @@ __global__ void __launch_bounds__(TILE_THREADS, kMinBlocks) tile_kernel(const Ti
         for (int v = 0; v < 4; v++) flux[v] = R(imposed[4 * gj + v]);
       } else {
         face_states(cd.recon, cd.limiter, Wat(sj, si - 2), Wat(sj, si - 1), Wat(sj, si),
-                    Wat(sj, si + 1), gamma, wall_side(cd, gi, ni, BS_IMIN, BS_IMAX), R(fm.x),
-                    R(fm.y), left, right);
-        face_flux(cd.flux, left, right, R(fm.x), R(fm.y), gamma, flux);
+                    Wat(sj, si + 1), gamma, wall_side(cd, gi, ni, BS_IMIN, BS_IMAX), fm.nx, fm.ny,
+                    left, right);
+        face_flux(cd.flux, left, right, fm.nx, fm.ny, gamma, flux);
       }
-      const R area = R(fm.z);
+      const R area = fm.area;
 #pragma unroll
       for (int v = 0; v < 4; v++) Fi[v][fr][fl] = flux[v] * area;
     } else {
       const int f2 = f - nfi;
       const int fl = f2 % ti, fr = f2 / ti;
       const int gi = i0 + fl, gj = j0 + fr;
-      const float4 fm = A.m.jface[cd.jface + gi + int64_t(gj) * ni];
+      const FaceGeom<R> fm = face_geom<R>(A.m.jface, A.m.jface_lo, cd.jface + gi + int64_t(gj) * ni);
       const int sj = fr + 2, si = fl + 2;
       const double* imposed = (gj == 0 || gj == nj) ? cd.face_flux[gj == 0 ? BS_JMIN : BS_JMAX] : nullptr;
       if (imposed != nullptr) {
@@ -151,11 +151,11 @@ __global__ void __launch_bounds__(TILE_THREADS, kMinBlocks) tile_kernel(const Ti
         for (int v = 0; v < 4; v++) flux[v] = R(imposed[4 * gi + v]);
       } else {
         face_states(cd.recon, cd.limiter, Wat(sj - 2, si), Wat(sj - 1, si), Wat(sj, si),
-                    Wat(sj + 1, si), gamma, wall_side(cd, gj, nj, BS_JMIN, BS_JMAX), R(fm.x),
-                    R(fm.y), left, right);
-        face_flux(cd.flux, left, right, R(fm.x), R(fm.y), gamma, flux);
+                    Wat(sj + 1, si), gamma, wall_side(cd, gj, nj, BS_JMIN, BS_JMAX), fm.nx, fm.ny,
+                    left, right);
+        face_flux(cd.flux, left, right, fm.nx, fm.ny, gamma, flux);
       }
-      const R area = R(fm.z);
+      const R area = fm.area;
 #pragma unroll
       for (int v = 0; v < 4; v++) Fj[v][fr][fl] = flux[v] * area;
     }
@@ -171,8 +171,9 @@ __global__ void __launch_bounds__(TILE_THREADS, kMinBlocks) tile_kernel(const Ti
     for (int v = 0; v < 4; v++)
       res[v] = ((Fi[v][lj][li] - Fi[v][lj][li + 1]) + Fj[v][lj][li]) - Fj[v][lj + 1][li];
     const float2 cm = A.m.cell[k];
-    if (cd.axisym) res[2] = res[2] + pressure_of(qs.rho, qs.mu, qs.mv, qs.e, gamma) * R(cm.y);
-    const R V = R(cm.x);
+    R V, planar;
+    cell_geom<R>(A.m, k, &V, &planar);
+    if (cd.axisym) res[2] = res[2] + pressure_of(qs.rho, qs.mu, qs.mv, qs.e, gamma) * planar;
     if (A.norm != nullptr) {
       const R r = res[0] / V;
       nsq = double(r) * double(r);

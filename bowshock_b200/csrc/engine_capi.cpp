@@ -239,6 +239,26 @@ bs_status bs_engine_solve(bs_engine* engine, int32_t method, double cfl, double 
   });
 }
 
+bs_status bs_engine_iterate_accelerated(bs_engine* engine, int32_t steps, double cfl_max, double omega,
+                                        double growth) {
+  BS_ENGINE_CALL(engine, { return engine->solver->iterate_accelerated(steps, cfl_max, omega, growth); });
+}
+
+bs_status bs_engine_set_metric_precision(bs_engine* engine, int32_t bits) {
+  BS_ENGINE_CALL(engine, { return engine->solver->set_metric_precision(bits); });
+}
+
+bs_status bs_engine_anderson_restarts(bs_engine* engine, int32_t* restarts) {
+  BS_ENGINE_CALL(engine, {
+    if (restarts == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+    int r = 0;
+    const bs_status s = engine->solver->anderson_restarts(&r);
+    if (s != BS_OK) return s;
+    *restarts = int32_t(r);
+    return BS_OK;
+  });
+}
+
 bs_status bs_engine_set_anderson(bs_engine* engine, int32_t depth, int32_t plain_steps) {
   BS_ENGINE_CALL(engine, { return engine->solver->set_anderson(depth, plain_steps); });
 }
@@ -366,6 +386,10 @@ bs_status bs_batch_solve(bs_batch* batch, int32_t method, double cfl, double ome
 
 bs_status bs_batch_set_anderson(bs_batch* batch, int32_t depth, int32_t plain_steps) {
   BS_BATCH_CALL(batch, { return batch->solver->set_anderson(depth, plain_steps); });
+}
+
+bs_status bs_batch_set_metric_precision(bs_batch* batch, int32_t bits) {
+  BS_BATCH_CALL(batch, { return batch->solver->set_metric_precision(bits); });
 }
 
 bs_status bs_batch_anderson_restarts(bs_batch* batch, int32_t* restarts) {

@@ -11,6 +11,8 @@
 
 struct bs_grid {
   bs::Grid g;
+  bool transonic = false;
+  bs::TransonicGridInfo info;
 };
 
 namespace {
@@ -120,6 +122,44 @@ bs_status bs_grid_info(const bs_grid* grid, int32_t* i_tip, double* outer_angle)
   if (grid == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
   if (i_tip) *i_tip = grid->g.i_tip;
   if (outer_angle) *outer_angle = grid->g.outer_angle;
+  return bs::ok();
+}
+
+bs_status bs_transonic_grid(const bs_body* body, const bs_transonic_grid_options* options, bs_grid** out) {
+  if (body == nullptr || options == nullptr || out == nullptr)
+    return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  bs::TransonicGridOptions o;
+  o.refinement = options->refinement;
+  o.far_field = options->far_field;
+  o.cylinder = options->cylinder;
+  // A spacing of 0 takes the default.
+  const double given[6] = {options->wall, options->growth, options->tip, options->shoulder, options->nose,
+                           options->nose_growth};
+  double* fields[6] = {&o.spacing.wall, &o.spacing.growth, &o.spacing.tip, &o.spacing.shoulder,
+                       &o.spacing.nose, &o.spacing.nose_growth};
+  for (int k = 0; k < 6; k++)
+    if (given[k] != 0) *fields[k] = given[k];
+  auto* g = new (std::nothrow) bs_grid;
+  if (g == nullptr) return bs::fail(BS_MEMORY_LIMIT, "out of host memory");
+  const std::string e = bs::transonic_grid(to_body(*body), o, &g->g, &g->info);
+  if (!e.empty()) {
+    delete g;
+    return bs::fail(BS_INVALID_ARGUMENT, e);
+  }
+  g->transonic = true;
+  *out = g;
+  return bs::ok();
+}
+
+bs_status bs_grid_transonic_info(const bs_grid* grid, int32_t* i_shoulder, int32_t* base_nj, double* far_radius,
+                                 double* x_upstream, double* x_end) {
+  if (grid == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+  if (!grid->transonic) return bs::fail(BS_INVALID_ARGUMENT, "not a transonic grid");
+  if (i_shoulder) *i_shoulder = grid->info.i_shoulder;
+  if (base_nj) *base_nj = grid->info.base_nj;
+  if (far_radius) *far_radius = grid->info.far_radius;
+  if (x_upstream) *x_upstream = grid->info.x_upstream;
+  if (x_end) *x_end = grid->info.x_end;
   return bs::ok();
 }
 

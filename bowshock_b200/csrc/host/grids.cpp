@@ -655,6 +655,76 @@ std::vector<double> sharp_fit_columns(const Body& body, double beta, double x0, 
   return column_positions(bp, [&](double x) { return density / spacing(x); }, refinement, 0);
 }
 
+std::string transonic_grid(const Body& body, const TransonicGridOptions& o, Grid* out,
+                           TransonicGridInfo* info) {
+  std::string e = validate_body(body);
+  if (!e.empty()) return e;
+  const int refinement = o.refinement;
+  if (!(refinement >= 1 && (refinement & (refinement - 1)) == 0))
+    return "the refinement must be 1, 2, 4, 8, ...";
+  const double R = body.nose.base_radius, L = body.nose.length;
+  if (!(o.cylinder > 0)) return "the transonic domain needs a cylinder";
+  if (!(o.far_field * R > 4 * std::max(R, L))) return "the far boundaries must lie beyond four nose lengths";
+  const TransonicSpacing& s = o.spacing;
+  if (!(s.wall > 0 && s.growth > 0 && s.tip > 0 && s.shoulder > 0 && s.nose > 0 && s.nose_growth > 0))
+    return "the transonic grid's spacings must be positive";
+  if (!std::isfinite(nose_tip_slope(body.nose)))
+    return "the transonic grid is built for sharp noses only here (the C grids of blunt noses are not)";
+  const double wall = s.wall * R, growth = s.growth;
+  // Cells across on the base grid: geometric growth from the wall spacing
+  // reaches the far radius in this many cells.
+  const int base_nj = int(std::ceil(std::log1p(growth * o.far_field * R / wall) / growth - 1e-9));
+  const double far_radius = (wall / growth) * std::expm1(growth * base_nj);
+  const double x_upstream = -far_radius;
+  const double x_end = L + 2 * R * o.cylinder;
+  const int nj = base_nj * refinement;
+  // Column spacing along x: growing geometrically from the tip and from the
+  // shoulder, at most s.nose along the nose.
+  const double tip = s.tip * R, shoulder = s.shoulder * R;
+  auto spacing = [&](double x) {
+    if (x <= 0) return tip + growth * -x;
+    if (x >= L) return shoulder + growth * (x - L);
+    return std::min(std::min(tip + s.nose_growth * x, shoulder + s.nose_growth * (L - x)), s.nose * R);
+  };
+  const std::vector<double> xs = column_positions(
+      {x_upstream, 0.0, L, x_end}, [&](double x) { return refinement / spacing(x); }, refinement, 0);
+  const int ni = int(xs.size()) - 1;
+  int i_tip = -1, i_shoulder = -1;
+  for (int i = 0; i <= ni; i++) {
+    if (i_tip < 0 && xs[i] == 0) i_tip = i;
+    if (i_shoulder < 0 && xs[i] == L) i_shoulder = i;
+  }
+  // Across each line from the wall to the far radius at f = expm1(b j / nj)
+  // / expm1(b) of the way, b = growth base_nj; the lines lean, by f^2 of the
+  // way, to points evenly spaced along the far boundary.
+  const double b = growth * base_nj;
+  out->ni = ni;
+  out->nj = nj;
+  out->i_tip = i_tip;
+  out->outer_angle = 0;
+  out->two_scale = false;
+  out->x.assign(size_t(ni + 1) * (nj + 1), 0);
+  out->y.assign(size_t(ni + 1) * (nj + 1), 0);
+  for (int j = 0; j <= nj; j++) {
+    const double f = std::expm1((b * j) / nj) / std::expm1(b);
+    for (int i = 0; i <= ni; i++) {
+      const double x = xs[i];
+      const double r = body_radius(body, x);
+      const double x_far = x_upstream + ((x_end - x_upstream) * i) / ni;
+      const size_t k = i + size_t(j) * (ni + 1);
+      out->x[k] = x + (x_far - x) * f * f;
+      out->y[k] = r + (far_radius - r) * f;
+    }
+  }
+  info->i_tip = i_tip;
+  info->i_shoulder = i_shoulder;
+  info->base_nj = base_nj;
+  info->far_radius = far_radius;
+  info->x_upstream = x_upstream;
+  info->x_end = x_end;
+  return "";
+}
+
 std::string ramp_grid(int ni, int nj, double x_min, double x_corner, double x_max, double height,
                       double angle, Grid* out) {
   if (!(x_min < x_corner && x_corner < x_max)) return "the corner must lie inside";

@@ -89,6 +89,38 @@ std::string blunt_body_grid(const Body& body, const BluntGridOptions& options, G
 std::vector<double> sharp_fit_columns(const Body& body, double beta, double x0, int nj, int refinement,
                                       double aspect, double density);
 
+// The base grid's spacings of the transonic grids, in body radii
+// (TRANSONIC_SPACING, src/grid/transonic-grid.ts:119-126).
+struct TransonicSpacing {
+  double wall = 0.05;         // cell height at the wall
+  double growth = 0.2;        // e^growth: cell growth away from the body and along the axis
+  double tip = 0.05;          // column spacing at the tip
+  double shoulder = 0.02;     // column spacing at the shoulder (the end of the nose)
+  double nose = 0.2;          // largest column spacing along the nose
+  double nose_growth = 0.1;   // growth of the column spacing along the nose
+};
+
+struct TransonicGridOptions {
+  int refinement = 1;
+  double far_field = 100;   // far boundaries at least this many body radii out
+  double cylinder = 10;     // calibers of cylinder solved behind the nose
+  TransonicSpacing spacing;
+};
+
+struct TransonicGridInfo {
+  int i_tip = 0, i_shoulder = 0, base_nj = 0;
+  double far_radius = 0, x_upstream = 0, x_end = 0;
+};
+
+// transonicGrid (src/grid/transonic-grid.ts:128-189) for sharp noses: the
+// H grid of a nose and a long cylinder in a domain reaching far upstream,
+// sideways and downstream (jMin the axis ahead of the tip and the body,
+// jMax the far radius, iMin the far boundary upstream, iMax the plane
+// ending the cylinder); cells growing geometrically away from the wall and
+// from the tip and shoulder along the axis; refined grids nest.
+std::string transonic_grid(const Body& body, const TransonicGridOptions& options, Grid* out,
+                           TransonicGridInfo* info);
+
 // rampGrid (src/grid/shapes.ts:30-52).
 std::string ramp_grid(int ni, int nj, double x_min, double x_corner, double x_max, double height,
                       double angle, Grid* out);

@@ -219,6 +219,8 @@ class Solver final : public SolverBase {
     BS_CUDA(iface_.alloc(ifc));
     BS_CUDA(jface_.alloc(jfc));
     BS_CUDA(cellm_.alloc(total_cells_));
+    total_iface_ = ifc;
+    total_jface_ = jfc;
     BS_CUDA(norm_.alloc(n_));
     BS_CUDA(status_.alloc(n_));
     BS_CUDA(dtmin_.alloc(n_));
@@ -392,6 +394,7 @@ class Solver final : public SolverBase {
     BS_CUDA(cudaMemcpyAsync(status_.p + c, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, stream_));
     BS_CUDA(cudaStreamSynchronize(stream_));
     steps_[c] = 0;
+    anderson_stale_ = true;
     return BS_OK;
   }
 
@@ -593,6 +596,78 @@ class Solver final : public SolverBase {
     return check_status();
   }
 
+  // LU-SGS steps with the Anderson settings of set_anderson applied, the
+  // acceleration's history kept from one call to the next: plain steps until
+  // anderson_plain_ steps have been taken since the history was last reset
+  // (by setting the state or the settings), accelerated ones after, as
+  // solveTransonic steps (src/analysis/transonic-flow.ts:151-245).
+  bs_status iterate_accelerated(int steps, double cfl_max, double omega, double growth) override {
+    if (steps < 0) return fail(BS_INVALID_ARGUMENT, "steps must be non-negative");
+    if (!(cfl_max > 0 && omega >= 1 && growth >= 1))
+      return fail(BS_INVALID_ARGUMENT, "implicit steps need cfl > 0, omega >= 1 and growth >= 1");
+    BS_TRY(ensure_implicit());
+    BS_TRY(set_implicit_params(cfl_max, omega, growth));
+    if (anderson_depth_ == 0) {
+      BS_TRY(run_steps(kMethodImplicit, steps, false));
+    } else {
+      if (anderson_stale_) {
+        BS_TRY(reset_anderson());
+        anderson_stale_ = false;
+        accelerated_steps_ = 0;
+      }
+      const int plain =
+          int(std::max<int64_t>(0, std::min<int64_t>(steps, anderson_plain_ - accelerated_steps_)));
+      if (plain > 0) BS_TRY(run_steps(kMethodImplicit, plain, false));
+      if (steps > plain) BS_TRY(run_steps(kMethodAnderson, steps - plain, false));
+      accelerated_steps_ += steps;
+    }
+    count_steps(steps);
+    return check_status();
+  }
+
+  // Two-float metrics (bits 64): the FP32 low part of every face normal,
+  // area, cell volume and planar area, which the residual and the ghost cells
+  // add to the FP32 values, as the reference's two-float engine stores its
+  // metrics (src/engine-gpu/euler2d-two-float.ts:584-605); the LU-SGS
+  // operator and the time steps keep the FP32 values. Bits 32: FP32 metrics.
+  bs_status set_metric_precision(int bits) override {
+    if (bits != 32 && bits != 64) return fail(BS_INVALID_ARGUMENT, "metric precision is 32 or 64 bits");
+    if (bits == 64 && sizeof(R) != sizeof(double))
+      return fail(BS_INVALID_ARGUMENT, "the all-FP32 engine keeps FP32 metrics");
+    const bool on = bits == 64;
+    if (on == metrics_lo_) return BS_OK;
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    if (on && iface_lo_.p == nullptr) {
+      BS_CUDA(iface_lo_.alloc(total_iface_));
+      BS_CUDA(jface_lo_.alloc(total_jface_));
+      BS_CUDA(cellm_lo_.alloc(total_cells_));
+      auto lo = [](double v) { return float(v - double(float(v))); };
+      std::vector<float4> fi, fj;
+      std::vector<float2> cm;
+      for (int c = 0; c < n_; c++) {
+        const Metrics64& m = cases_[c].m;
+        fi.resize(m.inx.size());
+        for (size_t k = 0; k < fi.size(); k++) fi[k] = make_float4(lo(m.inx[k]), lo(m.iny[k]), lo(m.iarea[k]), 0.f);
+        fj.resize(m.jnx.size());
+        for (size_t k = 0; k < fj.size(); k++) fj[k] = make_float4(lo(m.jnx[k]), lo(m.jny[k]), lo(m.jarea[k]), 0.f);
+        cm.resize(m.volume.size());
+        for (size_t k = 0; k < cm.size(); k++) cm[k] = make_float2(lo(m.volume[k]), lo(m.planar[k]));
+        BS_CUDA(cudaMemcpy(iface_lo_.p + hc_[c].iface, fi.data(), fi.size() * sizeof(float4),
+                           cudaMemcpyHostToDevice));
+        BS_CUDA(cudaMemcpy(jface_lo_.p + hc_[c].jface, fj.data(), fj.size() * sizeof(float4),
+                           cudaMemcpyHostToDevice));
+        BS_CUDA(cudaMemcpy(cellm_lo_.p + hc_[c].cell, cm.data(), cm.size() * sizeof(float2),
+                           cudaMemcpyHostToDevice));
+      }
+    }
+    metrics_lo_ = on;
+    // Captured graphs hold the old metric views.
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+    graph_launches_.clear();
+    return BS_OK;
+  }
+
   bs_status residual_norms(double* norms) override {
     BS_CUDA(cudaMemsetAsync(norm_.p, 0, n_ * sizeof(double), stream_));
     BS_TRY(launch_tile<bsd::MODE_RESIDUAL>(q_view(), q_view(), q_view(), 0, 1, false, norm_.p,
@@ -707,6 +782,7 @@ class Solver final : public SolverBase {
       return fail(BS_INVALID_ARGUMENT, "Anderson acceleration keeps 0 to 16 differences after plain_steps >= 0");
     anderson_depth_ = depth;
     anderson_plain_ = plain_steps;
+    anderson_stale_ = true;
     return BS_OK;
   }
 
@@ -733,6 +809,8 @@ class Solver final : public SolverBase {
       BS_TRY(set_implicit_params(cfl, omega, 1.0));
       BS_TRY(set_implicit_cfl(cfl));
       if (anderson_depth_ > 0) BS_TRY(reset_anderson());
+      // A later iterate_accelerated starts its own history.
+      anderson_stale_ = true;
     } else {
       BS_TRY(ensure_explicit());
     }
@@ -832,7 +910,15 @@ class Solver final : public SolverBase {
   bsd::StateView<R> q_view() const { return {q_[0].p, q_[1].p, q_[2].p, q_[3].p}; }
   bsd::StateView<R> s1_view() const { return {s1_[0].p, s1_[1].p, s1_[2].p, s1_[3].p}; }
   bsd::StateView<R> s2_view() const { return {s2_[0].p, s2_[1].p, s2_[2].p, s2_[3].p}; }
-  bsd::MetricsView metrics() const { return {iface_.p, jface_.p, cellm_.p}; }
+  bsd::MetricsView metrics() const {
+    bsd::MetricsView m{iface_.p, jface_.p, cellm_.p};
+    if (metrics_lo_) {
+      m.iface_lo = iface_lo_.p;
+      m.jface_lo = jface_lo_.p;
+      m.cell_lo = cellm_lo_.p;
+    }
+    return m;
+  }
 
   bs_status ensure_explicit() {
     if (s1_[0].p != nullptr) return BS_OK;
@@ -1208,6 +1294,11 @@ class Solver final : public SolverBase {
   DevBuf<float> dt_, cfl_, cflmax_, growth_, omega_;
   DevBuf<float4> iface_, jface_, rec_, dq_;
   DevBuf<float2> cellm_;
+  // The two-float metrics' low parts, allocated when first switched on.
+  DevBuf<float4> iface_lo_, jface_lo_;
+  DevBuf<float2> cellm_lo_;
+  bool metrics_lo_ = false;
+  int64_t total_iface_ = 0, total_jface_ = 0;
   DevBuf<double> norm_, bgeom_, bflux_, force_, res_out_;
   DevBuf<unsigned> status_, dtmin_;
   cudaStream_t stream_ = nullptr;
@@ -1232,6 +1323,10 @@ class Solver final : public SolverBase {
   int64_t last_solve_launches_ = 0;
   // Anderson acceleration: settings and its per-case history.
   int anderson_depth_ = 0, anderson_plain_ = 30, anderson_alloc_depth_ = 0;
+  // iterate_accelerated's history: reset before its next step when stale,
+  // and the steps it has taken since.
+  bool anderson_stale_ = true;
+  int64_t accelerated_steps_ = 0;
   DevBuf<float4> adx_, adf_, alastf_;
   DevBuf<R> alastx_[4];
   DevBuf<bsd::AndersonCase> ac_;

@@ -45,6 +45,13 @@ class SolverBase {
   virtual bs_status set_primitives(int c, const double* prim) = 0;
   virtual bs_status iterate(int steps) = 0;
   virtual bs_status iterate_implicit(int steps, double cfl_max, double omega, double growth) = 0;
+  // As iterate_implicit with the Anderson settings applied and the
+  // acceleration's history kept between calls (reset when the state or the
+  // settings change).
+  virtual bs_status iterate_accelerated(int steps, double cfl_max, double omega, double growth) = 0;
+  // 64: two-float metrics in the residual (FP32 values and their FP32 low
+  // parts); 32: FP32 metrics (the default).
+  virtual bs_status set_metric_precision(int bits) = 0;
   virtual bs_status set_implicit_cfl(double cfl) = 0;
   virtual bs_status residual_norms(double* norms) = 0;
   virtual bs_status residual(int c, double* out) = 0;

@@ -178,6 +178,26 @@ class CudaEuler2D:
             self.set_implicit_cfl(cfl)
         self._call("bs_engine_iterate_implicit", int(count), float(cfl), float(omega), float(growth))
 
+    def iterate_accelerated(self, count: int, cfl: float, omega: float = 1.5, growth: float = 1.0) -> None:
+        """LU-SGS steps with the Anderson acceleration of set_anderson, its
+        history kept from call to call (solveTransonic's steps,
+        src/analysis/transonic-flow.ts:151-245): plain steps until
+        `plain_steps` have been taken since the state or the settings were set,
+        accelerated ones after. The CFL number grows by `growth` per step up to
+        `cfl` from its current value (set_implicit_cfl)."""
+        self._call("bs_engine_iterate_accelerated", int(count), float(cfl), float(omega), float(growth))
+
+    def set_metric_precision(self, bits: int) -> None:
+        """64: two-float metrics in the residual (FP32 values plus their FP32
+        low parts, as the reference's two-float engine); 32: FP32 metrics."""
+        self._call("bs_engine_set_metric_precision", int(bits))
+
+    def anderson_restarts(self) -> int:
+        """The times the acceleration forgot its history since its last reset."""
+        r = C.c_int32()
+        self._call("bs_engine_anderson_restarts", C.byref(r))
+        return r.value
+
     def set_anderson(self, depth: int, plain_steps: int = 30) -> None:
         """Anderson acceleration of later LU-SGS solves (AndersonMixing,
         src/solver/anderson.ts): `depth` differences kept, 0 for plain steps,

@@ -124,6 +124,53 @@ def blunt_body_grid(body: Body, nj: int, mach: float, refinement: int = 1, ni: i
     return BodyGrid(grid, tip, angle, bool(two.value))
 
 
+@dataclass(frozen=True)
+class TransonicGrid:
+    """TransonicGrid (src/grid/transonic-grid.ts:84-101)."""
+
+    grid: StructuredGrid
+    i_tip: int
+    i_shoulder: int
+    far_radius: float
+    x_upstream: float
+    x_end: float
+    base_nj: int
+    topology: str = "H"
+
+
+def transonic_grid(body: Body, refinement: int = 1, far_field: float = 100.0, cylinder: float = 10.0,
+                   spacing: dict | None = None, lib=None) -> TransonicGrid:
+    """transonicGrid (src/grid/transonic-grid.ts:128-189) for sharp noses:
+    the H grid of the nose and `cylinder` calibers of cylinder, its far
+    boundaries `far_field` body radii out (rounded up to whole base cells);
+    `spacing` overrides TRANSONIC_SPACING's entries (wall, growth, tip,
+    shoulder, nose, nose_growth)."""
+    L = lib or _native.load()
+    o = abi.TransonicGridOptions()
+    o.refinement = refinement
+    o.far_field = far_field
+    o.cylinder = cylinder
+    for k, v in (spacing or {}).items():
+        if k not in ("wall", "growth", "tip", "shoulder", "nose", "nose_growth"):
+            raise ValueError(f"unknown transonic spacing {k!r}")
+        if not v > 0:
+            raise ValueError("the transonic grid's spacings must be positive")
+        setattr(o, k, float(v))
+    b = body.to_abi()
+    h = C.c_void_p()
+    _native.check(L.bs_transonic_grid(C.byref(b), C.byref(o), C.byref(h)), L)
+    shoulder, base_nj = C.c_int32(), C.c_int32()
+    far, up, end = C.c_double(), C.c_double(), C.c_double()
+    try:
+        _native.check(L.bs_grid_transonic_info(h, C.byref(shoulder), C.byref(base_nj), C.byref(far), C.byref(up),
+                                               C.byref(end)), L)
+    except BaseException:
+        L.bs_grid_destroy(h)
+        raise
+    grid, tip, _ = _take(h, L)
+    return TransonicGrid(grid, tip, shoulder.value, far.value, up.value, end.value, base_nj.value)
+
+
 def ramp_grid(ni: int, nj: int, x_min: float, x_corner: float, x_max: float, height: float,
               angle: float, lib=None) -> StructuredGrid:
     L = lib or _native.load()

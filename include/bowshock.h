@@ -264,8 +264,34 @@ BS_API bs_status bs_engine_steps(bs_engine *engine, int64_t *steps);
 BS_API bs_status bs_engine_solve(bs_engine *engine, int32_t method, double cfl, double omega,
                           double tolerance, int32_t relative, int32_t max_steps,
                           int32_t check_every, bs_solve_result *result);
-/* As bs_batch_set_anderson, for the engine's later bs_engine_solve calls. */
+/* As bs_batch_set_anderson, for the engine's later bs_engine_solve and
+ * bs_engine_iterate_accelerated calls. */
 BS_API bs_status bs_engine_set_anderson(bs_engine *engine, int32_t depth, int32_t plain_steps);
+
+/* LU-SGS steps as bs_engine_iterate_implicit (the CFL number growing by
+ * `growth` up to `cfl_max` from its current value), with the Anderson
+ * acceleration of bs_engine_set_anderson and its history kept from one call
+ * to the next: plain steps until plain_steps have been taken since the state
+ * or the settings were last set, accelerated ones after (solveTransonic's
+ * steps, src/analysis/transonic-flow.ts:151-245: the history forgotten when
+ * |f|^2 exceeds 100 times its least value, a non-physical accelerated state
+ * replaced by the plain step). Without acceleration (depth 0) it is
+ * bs_engine_iterate_implicit. */
+BS_API bs_status bs_engine_iterate_accelerated(bs_engine *engine, int32_t steps, double cfl_max,
+                                               double omega, double growth);
+/* The times the acceleration forgot its history since it was last reset. */
+BS_API bs_status bs_engine_anderson_restarts(bs_engine *engine, int32_t *restarts);
+
+/* The metrics the residual reads: 32 (FP32, the default) or 64 (two-float:
+ * each face normal, face area, cell volume and planar area as its FP32 value
+ * plus the FP32 low part of the FP64 value, about 48 bits, as the reference's
+ * two-float engine holds them, src/engine-gpu/euler2d-two-float.ts:1-8,
+ * 584-605). The steady state is then that of the FP64 residual to about
+ * 1e-12 instead of FP32 metric rounding (a drag error near 1e-6 of its value
+ * on the far-field domains of transonic flow); the LU-SGS operator and the
+ * time steps keep FP32 metrics. Costs 24 more bytes per cell of device
+ * memory and of residual traffic. Engines of precision 32 refuse 64. */
+BS_API bs_status bs_engine_set_metric_precision(bs_engine *engine, int32_t bits);
 
 /* ---- an LU-SGS step that allocates nothing -------------------------------- */
 
@@ -350,6 +376,8 @@ BS_API bs_status bs_batch_solve(bs_batch *batch, int32_t method, double cfl, dou
  * default) keeps plain steps; at most 16. The steady state, and the residual
  * test that stops a case, are those of the plain steps. */
 BS_API bs_status bs_batch_set_anderson(bs_batch *batch, int32_t depth, int32_t plain_steps);
+/* As bs_engine_set_metric_precision, for every case of the batch. */
+BS_API bs_status bs_batch_set_metric_precision(bs_batch *batch, int32_t bits);
 /* Per case, the times the last solve's acceleration forgot its history. */
 BS_API bs_status bs_batch_anderson_restarts(bs_batch *batch, int32_t *restarts);
 
@@ -438,6 +466,35 @@ BS_API bs_status bs_blunt_body_grid(const bs_body *body, const bs_body_grid_opti
 BS_API bs_status bs_blunt_body_grid_bounded(const bs_body *body, const bs_body_grid_options *options,
                                             const double *outer_x, const double *outer_y,
                                             int32_t n_outer, bs_grid **out);
+
+/* transonicGrid's options (TransonicGridOptions and TRANSONIC_SPACING,
+ * src/grid/transonic-grid.ts:39-126): the refinement (1, 2, 4, ...), the far
+ * boundaries' distance in body radii (rounded up to whole base cells), the
+ * cylinder solved behind the nose in calibers, and the base grid's spacings
+ * in body radii, each 0 for the default (wall 0.05, growth 0.2, tip 0.05,
+ * shoulder 0.02, nose 0.2, nose_growth 0.1). */
+typedef struct bs_transonic_grid_options {
+  int32_t refinement;
+  int32_t reserved;
+  double far_field;
+  double cylinder;
+  double wall, growth, tip, shoulder, nose, nose_growth;
+} bs_transonic_grid_options;
+
+/* transonicGrid (src/grid/transonic-grid.ts:128-189), sharp noses: the H grid
+ * of the nose and a long cylinder for flow from Mach 1 to about 1.2 (jMin the
+ * axis ahead of the tip and the body, jMax the far radius, iMin the far
+ * boundary upstream, iMax the plane ending the cylinder: give the far sides a
+ * far-field condition); every base cell divides into refinement^2 cells of
+ * the refined grid. Blunt noses' C grids are refused. */
+BS_API bs_status bs_transonic_grid(const bs_body *body, const bs_transonic_grid_options *options,
+                                   bs_grid **out);
+/* TransonicGrid's fields (src/grid/transonic-grid.ts:84-101) of a grid from
+ * bs_transonic_grid: the shoulder's column, the base grid's cells across, the
+ * far radius, the upstream boundary's x and the end of the cylinder; the
+ * tip's column is bs_grid_info's i_tip. */
+BS_API bs_status bs_grid_transonic_info(const bs_grid *grid, int32_t *i_shoulder, int32_t *base_nj,
+                                        double *far_radius, double *x_upstream, double *x_end);
 
 /* rampGrid (src/grid/shapes.ts:30-52): a channel whose lower wall turns by
  * `angle` at x_corner. */

@@ -175,6 +175,27 @@ def main() -> None:
         "mach": float(opts.group(1)), "nj": int(opts.group(2)),
         "drag_nj20": float(meas.group(1)), "drag_nj40": float(meas.group(2)), "within": 1e-9,
     }
+    # Transonic flow: the 7 deg cone of NACA TN 4233 at Mach 1.2 on its
+    # transonic grids, the drags measured on the base grid and the next two.
+    f3 = "tests/analysis/transonic-flow.test.ts"
+    t3 = (REF / f3).read_text()
+    tn = (REF / "src/validation/cone-cylinder-tn4233.ts").read_text()
+    half = re.search(r"TN4233_CONE_HALF_ANGLE = \(\(([0-9]+) \+ ([0-9]+) / 60\) \* Math\.PI\) / 180;", tn)
+    m3 = re.search(r"Measured when\s*//\s*written: ([0-9.]+) on the base grid \(\+([0-9.]+)%\), ([0-9.]+) and\s*//\s*"
+                   r"([0-9.]+) on the next two", t3)
+    po = re.search(r"mach: ([0-9.]+),\s*gamma,\s*refinement: 1,\s*farField: ([0-9]+),\s*cylinder: ([0-9]+),", t3)
+    so = re.search(r"noise: ([0-9e.-]+),\s*maxSteps: ([0-9]+),\s*checkEvery: ([0-9]+),\s*cfl: ([0-9]+),\s*"
+                   r"depth: ([0-9]+),\s*plainSteps: ([0-9]+),", t3)
+    within = re.search(r"toBeLessThan\(([0-9e.-]+)\);", t3)
+    out["transonic_cone_tn4233_mach1_2"] = {
+        "source": f"{f3}:{find_line(t3, 'Measured when')}",
+        "cone_half_angle_deg": int(half.group(1)) + int(half.group(2)) / 60, "base_radius": 1.0,
+        "mach": float(po.group(1)), "far_field": float(po.group(2)), "cylinder": float(po.group(3)),
+        "solve": {"noise": float(so.group(1)), "max_steps": int(so.group(2)), "check_every": int(so.group(3)),
+                  "cfl": float(so.group(4)), "depth": int(so.group(5)), "plain_steps": int(so.group(6))},
+        "drags": [float(m3.group(1)), float(m3.group(3)), float(m3.group(4))],
+        "base_rel_vs_taylor_maccoll": float(m3.group(2)) / 100, "within_taylor_maccoll": float(within.group(1)),
+    }
     # The two-scale allowance (TWO_SCALE_DRAG_FLOOR).
     fv2 = "src/analysis/verified-drag.ts"
     tf = (REF / fv2).read_text()
