@@ -47,9 +47,12 @@ struct AndersonCase {
   double best;     // smallest |f|^2 since the last restart (+inf at first)
 };
 
-// Per case, `acc` holds 1 + 2 depth sums of the current step: |f|^2, the new
-// column's dot products with the columns by slot, and each column's dot
-// product with f by slot.
+// Per tile, `part` holds 1 + 2 depth sums over the tile's cells for the
+// current step (the tile's row at its case's tile_base plus its index):
+// |f|^2, the new column's dot products with the columns by slot, and each
+// column's dot product with f by slot. The solve kernel adds the rows of a
+// case in a fixed order, so a step's result does not depend on the order in
+// which the tiles ran.
 template <class R>
 struct AndersonArgs {
   const CaseDev* cases;
@@ -66,7 +69,7 @@ struct AndersonArgs {
   int64_t total;          // cells of the batch
   int depth;
   AndersonCase* ac;
-  double* acc;            // (1 + 2 depth) per case
+  double* part;           // (1 + 2 depth) per tile
   double* gram;           // depth x depth per case, by slot
   double* gamma;          // depth per case, by slot (0 for a dropped column)
   unsigned* status;
@@ -80,53 +83,38 @@ __device__ __forceinline__ bool anderson_cell(const CaseDev& cd, int2 tile, int 
   return tid < TI * TJ && *i < cd.ni && *j < cd.nj;
 }
 
-// Adds per-thread values over the CTA and then to global sums with one FP64
-// atomic per value: va[p] to out[p] and vb[p] to out[n + p] for p < n
-// (n <= K, the same for every thread; vb is read only when `pairs`).
+// Adds per-thread values over the CTA in a fixed order and stores them to
+// out[0 .. 1 + 2 n): the sum of vf, then those of va[p], then those of
+// vb[p], p < n (n <= K, the same for every thread of the CTA).
 template <int K>
-__device__ __forceinline__ void cta_add(const double (&va)[K], const double (&vb)[K], int n, bool pairs,
-                                        double* out) {
-  __shared__ double part[TILE_THREADS / 32][2 * kMaxAndersonDepth];
+__device__ __forceinline__ void cta_store(double vf, const double (&va)[K], const double (&vb)[K], int n,
+                                          double* out) {
+  __shared__ double part[TILE_THREADS / 32][1 + 2 * K];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double sf = warp_sum(vf);
+  if (lane == 0) part[warp][0] = sf;
 #pragma unroll
   for (int p = 0; p < K; p++) {
     if (p < n) {
       const double sa = warp_sum(va[p]);
-      const double sb = pairs ? warp_sum(vb[p]) : 0.0;
+      const double sb = warp_sum(vb[p]);
       if (lane == 0) {
-        part[warp][p] = sa;
-        part[warp][K + p] = sb;
+        part[warp][1 + p] = sa;
+        part[warp][1 + n + p] = sb;
       }
     }
   }
   __syncthreads();
   const int t = threadIdx.x;
-  const int total = pairs ? 2 * n : n;
-  if (t < total) {
-    const int col = t < n ? t : K + (t - n);
+  if (t < 1 + 2 * n) {
     double s = 0;
-    for (int w = 0; w < TILE_THREADS / 32; w++) s += part[w][col];
-    if (s != 0.0) atomicAdd(&out[t], s);
+    for (int w = 0; w < TILE_THREADS / 32; w++) s += part[w][t];
+    out[t] = s;
   }
 }
 
 __device__ __forceinline__ double dot4(float4 a, float4 b) {
   return double(a.x) * b.x + double(a.y) * b.y + double(a.z) * b.z + double(a.w) * b.w;
-}
-
-template <class R>
-__global__ void __launch_bounds__(TILE_THREADS) anderson_fnorm_kernel(const AndersonArgs<R> A) {
-  const int2 tile = A.tiles[blockIdx.x];
-  const int c = tile.x;
-  if (A.active != nullptr && A.active[c] == 0) return;
-  const CaseDev& cd = A.cases[c];
-  int i, j;
-  double v[1] = {0.0};
-  if (anderson_cell(cd, tile, threadIdx.x, &i, &j)) {
-    const float4 f = A.dq[cd.skew + skew_slot(i, j, cd.nj)];
-    v[0] = dot4(f, f);
-  }
-  cta_add<1>(v, v, 1, false, A.acc + int64_t(c) * (1 + 2 * A.depth));
 }
 
 // Whether this step forgets the history: the previous accelerated state was
@@ -137,6 +125,9 @@ __device__ __forceinline__ bool anderson_reset(const AndersonCase& a, double fno
   return a.bad != 0 || fnorm > 100.0 * a.best;
 }
 
+// |f|^2 and the push of the new difference columns. The column is pushed
+// unless the previous accelerated state was rejected; if this step's |f|^2
+// makes the solve kernel forget the history, the column goes with the rest.
 template <class R>
 __global__ void __launch_bounds__(TILE_THREADS) anderson_push_kernel(const AndersonArgs<R> A) {
   const int2 tile = A.tiles[blockIdx.x];
@@ -144,8 +135,7 @@ __global__ void __launch_bounds__(TILE_THREADS) anderson_push_kernel(const Ander
   if (A.active != nullptr && A.active[c] == 0) return;
   const CaseDev& cd = A.cases[c];
   const AndersonCase a = A.ac[c];
-  double* acc = A.acc + int64_t(c) * (1 + 2 * A.depth);
-  const bool push = a.have_last && !anderson_reset(a, acc[0]);
+  const bool push = a.have_last && a.bad == 0;
   const int slot = a.count < A.depth ? a.count : a.head;
   const int ncols = push ? min(a.count + 1, A.depth) : 0;
   int i, j;
@@ -166,8 +156,7 @@ __global__ void __launch_bounds__(TILE_THREADS) anderson_push_kernel(const Ander
     A.last_x.store(k, x);
     A.last_f[k] = f;
   }
-  if (ncols == 0) return;  // the same for every thread of the CTA
-  // acc[1 .. 1 + ncols): new column . column p; acc[1 + ncols .. 1 + 2 ncols):
+  // The tile's row: |f|^2, then new column . column p for p < ncols, then
   // column p . f (the solve kernel reads them with this packing).
   double vg[kMaxAndersonDepth], vb[kMaxAndersonDepth];
 #pragma unroll
@@ -180,19 +169,32 @@ __global__ void __launch_bounds__(TILE_THREADS) anderson_push_kernel(const Ander
       vb[p] = dot4(col, f);
     }
   }
-  cta_add<kMaxAndersonDepth>(vg, vb, ncols, true, acc + 1);
+  cta_store<kMaxAndersonDepth>(mine ? dot4(f, f) : 0.0, vg, vb, ncols,
+                               A.part + (cd.tile_base + tile.y) * (1 + 2 * A.depth));
 }
 
-// One thread per case of the lane.
+// One warp per case of the lane: the case's tile rows added in a fixed order
+// (lane l takes tiles l, l + 32, ..., then a fixed shuffle tree), then lane 0
+// updates the history and solves for the mixing coefficients.
 template <class R>
-__global__ void anderson_solve_kernel(const AndersonArgs<R> A) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= A.n_cases) return;
-  const int c = A.case_list[idx];
+__global__ void __launch_bounds__(32) anderson_solve_kernel(const AndersonArgs<R> A) {
+  const int c = A.case_list[blockIdx.x];
   if (A.active != nullptr && A.active[c] == 0) return;
   const int m = A.depth;
+  const CaseDev& cd = A.cases[c];
   AndersonCase a = A.ac[c];
-  double* acc = A.acc + int64_t(c) * (1 + 2 * m);
+  const int width = 1 + 2 * m;
+  const int pushed = a.have_last && a.bad == 0 ? min(a.count + 1, m) : 0;
+  const int nv = 1 + 2 * pushed;
+  const int ntiles = ((cd.ni + TI - 1) / TI) * ((cd.nj + TJ - 1) / TJ);
+  const double* rows = A.part + cd.tile_base * width;
+  double acc[1 + 2 * kMaxAndersonDepth];
+  for (int v = 0; v < nv; v++) {
+    double s = 0;
+    for (int t = int(threadIdx.x); t < ntiles; t += 32) s += rows[int64_t(t) * width + v];
+    acc[v] = warp_sum(s);
+  }
+  if (threadIdx.x != 0) return;
   double* G = A.gram + int64_t(c) * m * m;
   double* gam = A.gamma + int64_t(c) * m;
   const double fnorm = acc[0];
@@ -261,7 +263,6 @@ __global__ void anderson_solve_kernel(const AndersonArgs<R> A) {
     }
     break;
   }
-  for (int p = 0; p < 1 + 2 * m; p++) acc[p] = 0.0;
   A.ac[c] = a;
 }
 

@@ -165,6 +165,7 @@ class Solver final : public SolverBase {
       d.iface = ifc;
       d.jface = jfc;
       d.skew = skw;
+      d.tile_base = int64_t(tiles.size());
       skw += int64_t(cfg.ni + cfg.nj - 1) * cfg.nj;
       for (int s = 0; s < 4; s++) d.bc[s] = cfg.boundaries[s].kind;
       d.flux = cfg.flux;
@@ -946,7 +947,7 @@ class Solver final : public SolverBase {
       BS_CUDA(alastf_.alloc(total_cells_));
       for (int v = 0; v < 4; v++) BS_CUDA(alastx_[v].alloc(total_cells_));
       BS_CUDA(ac_.alloc(n_));
-      BS_CUDA(aacc_.alloc(size_t(n_) * (1 + 2 * m)));
+      BS_CUDA(aacc_.alloc(size_t(n_tiles_) * (1 + 2 * m)));
       BS_CUDA(agram_.alloc(size_t(n_) * m * m));
       BS_CUDA(agamma_.alloc(size_t(n_) * m));
       anderson_alloc_depth_ = m;
@@ -965,7 +966,6 @@ class Solver final : public SolverBase {
     fresh.best = HUGE_VAL;
     std::vector<bsd::AndersonCase> h(n_, fresh);
     BS_CUDA(cudaMemcpyAsync(ac_.p, h.data(), n_ * sizeof(bsd::AndersonCase), cudaMemcpyHostToDevice, stream_));
-    BS_CUDA(cudaMemsetAsync(aacc_.p, 0, size_t(n_) * (1 + 2 * m) * sizeof(double), stream_));
     BS_CUDA(cudaMemsetAsync(agram_.p, 0, size_t(n_) * m * m * sizeof(double), stream_));
     BS_CUDA(cudaMemsetAsync(agamma_.p, 0, size_t(n_) * m * sizeof(double), stream_));
     BS_CUDA(cudaStreamSynchronize(stream_));
@@ -1115,16 +1115,15 @@ class Solver final : public SolverBase {
     A.total = total_cells_;
     A.depth = anderson_depth_;
     A.ac = ac_.p;
-    A.acc = aacc_.p;
+    A.part = aacc_.p;
     A.gram = agram_.p;
     A.gamma = agamma_.p;
     A.status = status_.p;
-    bsd::anderson_fnorm_kernel<R><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
     bsd::anderson_push_kernel<R><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
-    bsd::anderson_solve_kernel<R><<<(lane.n_cases + 63) / 64, 64, 0, lane.stream>>>(A);
+    bsd::anderson_solve_kernel<R><<<lane.n_cases, 32, 0, lane.stream>>>(A);
     bsd::anderson_apply_kernel<R><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
     bsd::anderson_fallback_kernel<R><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
-    launches_ += 5;
+    launches_ += 4;
     BS_CUDA(cudaGetLastError());
     return BS_OK;
   }

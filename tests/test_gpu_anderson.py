@@ -146,3 +146,19 @@ def test_near_mach_one_the_acceleration_takes_fewer_steps():
     assert runs[0][0] == 0 and runs[8][0] == 0
     assert runs[8][1] < 0.8 * runs[0][1]
     assert abs(runs[8][2] / runs[0][2] - 1) < 1e-7
+
+
+def test_accelerated_solves_are_reproducible():
+    # The acceleration's sums are added per tile and then in a fixed order,
+    # so the same solve gives the same steps and the same state bit for bit
+    # (the Mach 2.5 ogive's accelerated path is sensitive to the last bit).
+    case = ogive_case(2.5, 80, 40)
+    runs = []
+    for _ in range(2):
+        with CudaBatch([case.config], precision=64) as b:
+            b.set_free_stream()
+            b.set_anderson(8, 30)
+            r = b.solve("lusgs", 1e-8, max_steps=4000, cfl=5.0)[0]
+            runs.append((r.status, r.steps, b.primitives(0)))
+    assert runs[0][0] == runs[1][0] == 0 and runs[0][1] == runs[1][1]
+    assert np.array_equal(runs[0][2], runs[1][2])
