@@ -804,6 +804,70 @@ def run_stencil(args) -> None:
     print(json.dumps(out), flush=True)
 
 
+def run_transonic(args) -> None:
+    """Transonic flow (bowshock_b200.transonic): the 7 deg cone of NACA TN 4233
+    (half-angle 6 deg 59 min) at Mach 1.2 in its far-field domain (100 radii,
+    10 calibers of cylinder), LU-SGS at a CFL number ramped to 1000 with
+    Anderson acceleration (depth 8 after 200 plain steps) and two-float
+    metrics, on the base grid and two refinements, each finer grid started
+    from the coarser solution, until the drag settles within 1e-7; `value`
+    counts settled grids per second of wall time on the GPU. Beside it the
+    oracle's FP64 restatement of the same steps on the base grid, one host
+    thread."""
+    import math
+
+    import torch
+
+    from bowshock_b200.grid import Body, Nose, NoseShape, taylor_maccoll
+    from bowshock_b200.transonic import solve_transonic, transonic_problem
+
+    torch.cuda.set_device(0)
+    half = (6 + 59 / 60) * math.pi / 180
+    cone = Body(Nose(NoseShape("conical"), 1 / math.tan(half), 1.0), 0.0)
+    # The reference's FP64 CPU engine (tests/analysis/transonic-flow.test.ts:16-19).
+    measured = (0.0832184, 0.0830547, 0.0830207)
+    exact = taylor_maccoll(1.2, half, 1.4).surface_pressure_coefficient
+    problems = [transonic_problem(cone, 1.2, refinement=r) for r in (1, 2, 4)]
+
+    def family():
+        rows, previous = [], None
+        for k, p in enumerate(problems):
+            t1 = time.perf_counter()
+            out = solve_transonic(p, max_steps=4000 * p.refinement,
+                                  known_rate=previous[1].rate if previous else math.nan,
+                                  start=(previous[0], previous[1].primitives) if previous else None)
+            rows.append({"refinement": p.refinement, "cells": p.grid.grid.ni * p.grid.grid.nj, "steps": out.steps,
+                         "converged": out.converged, "wall_s": time.perf_counter() - t1, "drag": out.drag,
+                         "reference_drag": measured[k], "abs_diff_vs_reference": out.drag - measured[k]})
+            previous = (p, out)
+        return rows
+
+    family()      # warm-up: the library and each grid size's first use
+    clocks = Clocks(0)
+    clocks.start()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rows = family()
+    wall = time.perf_counter() - t0
+    clock_info = clocks.stop()
+    from oracle.transonic import solve_transonic as oracle_solve
+
+    t1 = time.perf_counter()
+    ora = oracle_solve(problems[0])
+    cpu_s = time.perf_counter() - t1
+    print(json.dumps({
+        "metric": "transonic solves/s (drag settled within 1e-7)", "value": len(problems) / wall, "unit": "solves/s",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "7 deg cone (TN 4233) at Mach 1.2, far field 100 radii, 10 calibers of cylinder; "
+                               "transonic H grids refined 1, 2, 4; LU-SGS CFL 1 x1.2 to 1000, Anderson depth 8 "
+                               "after 200 plain steps; two-float metrics"},
+        "wall_s": wall, "grids": rows, "taylor_maccoll": exact, "clocks": clock_info,
+        "cpu_baseline": {"value": 1 / cpu_s, "unit": "solves/s", "cores": 1, "kind": "port",
+                         "sample": f"the base grid solved by oracle/transonic.py (FP64, Python-driven): "
+                                   f"{ora.steps} steps in {cpu_s:.2f} s, drag {ora.drag:.10f}",
+                         "gpu_base_grid_s": rows[0]["wall_s"]}}), flush=True)
+
+
 def run_verified(args) -> None:
     """Verified forebody drag (the reference's banded answer) for several
     bodies and Mach numbers at once: grid families nj = 20 .. 160, each grid
@@ -851,7 +915,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--probe", type=int, default=0,
                     help="run this many LU-SGS steps of the batch with per-kernel timing and exit")
-    ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart", "stream", "fitted", "gemm", "stencil", "verified"], default="drag-curve")
+    ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart", "stream", "fitted", "gemm", "stencil", "verified",
+                                                  "transonic"], default="drag-curve")
     ap.add_argument("--train-cases", type=int, default=4096, help="warm start: training seeds")
     ap.add_argument("--eval-cases", type=int, default=512, help="warm start: held-out seeds")
     ap.add_argument("--train-steps", type=int, default=3000, help="warm start: Adam steps")
@@ -895,6 +960,9 @@ def main() -> None:
         return
     if args.workload == "stencil":
         run_stencil(args)
+        return
+    if args.workload == "transonic":
+        run_transonic(args)
         return
     if args.workload == "verified":
         run_verified(args)
