@@ -47,10 +47,18 @@ struct FitArgs {
   float4* iface;
   float4* jface;
   float2* cellm;
+  // The metrics' FP32 low parts (the FP64 value less the FP32 one): the
+  // residual reads two-float metrics, its steady state that of FP64 metrics.
+  float4* iface_lo;
+  float4* jface_lo;
+  float2* cellm_lo;
   double* bgeom;             // boundary faces iMin, iMax, jMin, jMax: (nx, ny, area)
   StateView<double> q;       // the state at the start of a step, and after the remap
   StateView<double> q_old;   // the state after the step's last stage, on the grid before the move
 };
+
+// The FP32 low part of an FP64 value: v less its FP32 rounding.
+__device__ __forceinline__ float low_part(double v) { return float(v - double(float(v))); }
 
 __device__ __forceinline__ void fit_shock_state(const FitArgs& A, double mach, double nx, double ny, double w[4],
                                                 double* speed, double* un) {
@@ -230,6 +238,7 @@ __global__ void fit_regrid_kernel(const FitArgs A, int remap) {
       const int i = int(m % (ni + 1)), j = int(m / (ni + 1));
       face(i, j, i, j + 1, &fx, &fy, &fa);
       A.iface[m] = make_float4(float(fx), float(fy), float(fa), 0.f);
+      A.iface_lo[m] = make_float4(low_part(fx), low_part(fy), low_part(fa), 0.f);
       if (i == 0 || i == ni) {
         double* g = A.bgeom + 3 * ((i == 0 ? 0 : nj) + j);
         g[0] = fx;
@@ -241,6 +250,7 @@ __global__ void fit_regrid_kernel(const FitArgs A, int remap) {
       const int i = int(m % ni), j = int(m / ni);
       face(i + 1, j, i, j, &fx, &fy, &fa);
       A.jface[m] = make_float4(float(fx), float(fy), float(fa), 0.f);
+      A.jface_lo[m] = make_float4(low_part(fx), low_part(fy), low_part(fa), 0.f);
       if (j == 0 || j == nj) {
         double* g = A.bgeom + 3 * (2 * nj + (j == 0 ? 0 : ni) + i);
         g[0] = fx;
@@ -264,7 +274,9 @@ __global__ void fit_regrid_kernel(const FitArgs A, int remap) {
       }
       area *= 0.5;
       const double ycen = sy / (6 * area);
-      A.cellm[m] = make_float2(float(A.axisym ? area * ycen : area), float(area));
+      const double volume = A.axisym ? area * ycen : area;
+      A.cellm[m] = make_float2(float(volume), float(area));
+      A.cellm_lo[m] = make_float2(low_part(volume), low_part(area));
     } else {
       const int64_t m = k - nn - nif - njf - nc;
       const int i = int(m % ni), j = int(m / ni);

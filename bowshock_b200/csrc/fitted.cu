@@ -123,6 +123,9 @@ class FittedSolver {
     FIT_CUDA(iface_.alloc(size_t(ni + 1) * nj));
     FIT_CUDA(jface_.alloc(size_t(ni) * (nj + 1)));
     FIT_CUDA(cellm_.alloc(nc));
+    FIT_CUDA(iface_lo_.alloc(size_t(ni + 1) * nj));
+    FIT_CUDA(jface_lo_.alloc(size_t(ni) * (nj + 1)));
+    FIT_CUDA(cellm_lo_.alloc(nc));
     FIT_CUDA(bgeom_.alloc(3 * size_t(2 * (ni + nj))));
     FIT_CUDA(top_state_.alloc(4 * size_t(ni)));
     FIT_CUDA(top_flux_.alloc(4 * size_t(ni)));
@@ -209,6 +212,9 @@ class FittedSolver {
     A_.iface = iface_.p;
     A_.jface = jface_.p;
     A_.cellm = cellm_.p;
+    A_.iface_lo = iface_lo_.p;
+    A_.jface_lo = jface_lo_.p;
+    A_.cellm_lo = cellm_lo_.p;
     A_.bgeom = bgeom_.p;
     A_.q = q_view();
     A_.q_old = {old_[0].p, old_[1].p, old_[2].p, old_[3].p};
@@ -344,13 +350,23 @@ class FittedSolver {
     return BS_OK;
   }
 
+  // The metrics the residual and the wall fluxes read: two-float (FP32
+  // values and low parts, both written by every regrid).
+  bsd::MetricsView metrics() const {
+    bsd::MetricsView m{iface_.p, jface_.p, cellm_.p};
+    m.iface_lo = iface_lo_.p;
+    m.jface_lo = jface_lo_.p;
+    m.cell_lo = cellm_lo_.p;
+    return m;
+  }
+
   // Wall fluxes of jMin (FP64, as bs_engine_boundary_fluxes) and the drag.
   bs_status wall(double p_inf, double* flux_out, double* force) {
     bsd::BoundaryArgs<double> B{};
     B.cases = case_.p;
     B.case_index = 0;
     B.q = q_view();
-    B.m = {iface_.p, jface_.p, cellm_.p};
+    B.m = metrics();
     B.side = BS_JMIN;
     B.geom = bgeom_.p + 3 * size_t(2 * nj_);
     B.gamma_eval = gamma_;
@@ -425,7 +441,7 @@ class FittedSolver {
     T.src = src;
     T.u0 = q_view();
     T.out = out;
-    T.m = {iface_.p, jface_.p, cellm_.p};
+    T.m = metrics();
     T.dt = dt_.p;
     T.dt_global = nullptr;
     T.norm = norm;
@@ -480,8 +496,8 @@ class FittedSolver {
   Buf<double> line_, fraction_, heights_, heights_old_, heights_next_, x_, y_;
   Buf<double> q_[4], s1_[4], s2_[4], old_[4];
   Buf<float> dt_;
-  Buf<float4> iface_, jface_;
-  Buf<float2> cellm_;
+  Buf<float4> iface_, jface_, iface_lo_, jface_lo_;
+  Buf<float2> cellm_, cellm_lo_;
   Buf<double> bgeom_, top_state_, top_flux_, in_state_, speed_, words_, bflux_;
   Buf<unsigned> status_;
 };

@@ -357,11 +357,15 @@ def settle(fit: CudaFit, max_iterations: int, noise: float = 1e-7, speed_toleran
     """The GPU fit's stopping rule (fitShockGpu, src/engine-gpu/shock-fitting-gpu.ts:
     135-170): every `check_every` steps the drag is added to a SettlingValue of
     `noise`; the fit has converged once the drag has settled and the shock
-    moves slower than `speed_tolerance` times a_inf. Here the state is FP64 and
-    the metrics FP32: the shock's speeds settle near 1e-7 (the reference's
-    all-FP32 engine: 1e-6 to 4e-6, against its tolerance of 3e-5), and the
-    drag at a few 1e-8 on slowly settling fits, hence the noise of 1e-7.
-    `known_rate`: the drag's rate of convergence per check on the grid
+    moves slower than `speed_tolerance` times a_inf. The reference's all-FP32
+    GPU fit settles its shock speeds at 1e-6 to 4e-6 (tolerance 3e-5) and its
+    drag with a noise of 2e-6; here the state is FP64 and the residual reads
+    two-float metrics, so a fit goes on converging to the FP64 floor (shock
+    speeds near 1e-11 a_inf, relative residuals 1e-13, the drag within 1e-11
+    of the reference's FP64 engine): the default noise of 1e-7 stops it
+    where the drag is settled far below the digits the verified band keeps;
+    noise 1e-11 with speed_tolerance 1e-10 settles it to the CPU engine's
+    own limits. `known_rate`: the drag's rate of convergence per check on the grid
     before, for a fit started from that grid's (it may begin too close to
     its limit to show its own). Leaves the rate to pass on in fit.rate.
     Returns (converged, iterations, max speed, drag)."""
@@ -667,7 +671,7 @@ def blunt_fit_problem(asked: Body, mach: float, nj: int = 20, gamma: float = 1.4
 FITTED_BASE_NJ = 20            # base grid cells across (fitted-flow.ts:1003)
 FALLBACK_COLUMN_DENSITY = 1.5  # a sharp family whose grid fails only the gates, solved again (:70)
 FITTED_DRAG_FLOOR = 7e-5       # systematic error of the fitted drag, relative (src/analysis/verified-drag.ts:132)
-FITTED_NOISE = 1e-7            # the GPU fit's drag settles to this, relative (settle)
+FITTED_NOISE = 1e-7            # the verified fitted drag's settling noise by default, relative (settle)
 FITTED_MIN_ANGLE = 12.0        # the fitted grids' quality gates (src/grid/quality.ts:24-38, 64-68), degrees
 FITTED_MIN_WALL_ANGLE = 50.0
 FITTED_MAX_ASPECT = 13.0
@@ -824,7 +828,8 @@ def fitted_case_failure(problem: FitProblem, asked_end: float, grid: StructuredG
 
 def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance: float = 1e-4,
                          max_refinement: int = 8, floor: float = FITTED_DRAG_FLOOR,
-                         iterations_per_refinement: int = 200000, on_level=None, on_fallback=None):
+                         iterations_per_refinement: int = 200000, on_level=None, on_fallback=None,
+                         noise: float = FITTED_NOISE, speed_tolerance: float = 1e-6):
     """The verified fitted drag as the reference's GPU driver computes it
     (verifiedFittedDragGpu, src/analysis/gpu-fitted-flow.ts:197-338, the
     procedure of verifiedFittedDrag, fitted-flow.ts:1011-1080), for sharp
@@ -839,7 +844,10 @@ def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance:
     finer grid (or one too large for the GPU) the band of the grids before it
     stands (result.stopped). A flow failing the checks is refused, but a
     sharp family whose grid fails only the quality gates is solved again with
-    1.5 times as many columns. Returns a verified_drag.VerifiedDrag."""
+    1.5 times as many columns. Each fit settles when its drag changes by less
+    than `noise` (relative) and its shock by less than `speed_tolerance`
+    a_inf; the same noise is the band's. Returns a
+    verified_drag.VerifiedDrag."""
     from .verification import refine_until_verified
     from .verified_drag import LevelReport, VerifiedDrag
 
@@ -874,7 +882,8 @@ def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance:
                 coarse, heights, cells, rate = previous[-1]
                 p = started_from(fresh, coarse, heights, cells) or fresh
             with CudaFit(p) as g:
-                converged, it, speed, drag = settle(g, iterations_per_refinement * r, check_every=250 * r,
+                converged, it, speed, drag = settle(g, iterations_per_refinement * r, noise=noise,
+                                                    speed_tolerance=speed_tolerance, check_every=250 * r,
                                                     known_rate=rate)
                 if not converged:
                     raise FitNotConverged(r, f"the fit stopped after {it} iterations with the shock moving at "
@@ -907,7 +916,7 @@ def verified_fitted_drag(body: Body, mach: float, gamma: float = 1.4, tolerance:
                 return str(e)
             return None
 
-        return refine_until_verified(solve_at, tolerance, floor, max_refinement, 0.5, FITTED_NOISE, stop_on)
+        return refine_until_verified(solve_at, tolerance, floor, max_refinement, 0.5, noise, stop_on)
 
     try:
         try:

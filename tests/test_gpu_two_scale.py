@@ -28,9 +28,10 @@ def _body() -> Body:
     return Body(Nose(NoseShape(b["shape"], float(b["parameter"])), b["length"], b["base_radius"]), b["cylinder"])
 
 
-def _settled(p, cap: int, r: int):
+def _settled(p, cap: int, r: int, noise: float = 1e-7, speed_tolerance: float = 1e-6):
     with CudaFit(p) as g:
-        converged, it, speed, drag = settle(g, cap, check_every=250 * r)
+        converged, it, speed, drag = settle(g, cap, noise=noise, speed_tolerance=speed_tolerance,
+                                            check_every=250 * r)
         return converged, it, speed, drag, g.grid(), g.primitives().reshape(p.nj, p.ni, 4)
 
 
@@ -69,8 +70,10 @@ def test_two_scale_start_follows_the_oracle(monkeypatch):
 def test_von_karman_fitted_drags_are_the_measured_ones():
     # nj = 20 and its refinement, each settled from the family's shock-layer
     # start (the reference starts the finer from the coarser fit: the same
-    # fixed point). The reference's FP64 fits agree with its measured drags
-    # to 1e-9; the GPU fit's FP32 metrics leave a few 1e-8.
+    # fixed point) until the drag changes by less than 1e-11 and the shock by
+    # less than 1e-10 a_inf. The reference's FP64 fits agree with its measured
+    # drags to 1e-9; so does the GPU fit, whose residual reads two-float
+    # metrics (about 1e-11 here).
     t0 = time.perf_counter()
     start = blunt_start(_body(), VK["mach"], VK["nj"])
     t_start = time.perf_counter() - t0
@@ -80,13 +83,13 @@ def test_von_karman_fitted_drags_are_the_measured_ones():
     for r, want in ((1, VK["drag_nj20"]), (2, VK["drag_nj40"])):
         p = family(r)
         t0 = time.perf_counter()
-        converged, it, speed, drag, grid, prims = _settled(p, 40000 * r, r)
+        converged, it, speed, drag, grid, prims = _settled(p, 40000 * r, r, noise=1e-11, speed_tolerance=1e-10)
         print(f"two-scale r={r}: {p.ni} x {p.nj} cells, {it} steps, {time.perf_counter() - t0:.2f} s "
               f"(start {t_start:.2f} s), speed {speed:.1e}, drag {drag:.12f}, rel {drag / want - 1:+.2e}")
         assert converged
         assert fitted_grid_failure(grid) is None
         assert fitted_case_failure(p, asked_end, grid, prims) is None
-        assert abs(drag / want - 1) < 3e-7
+        assert abs(drag / want - 1) < VK["within"]
 
 
 def test_verified_fitted_drag_of_a_von_karman_nose_carries_the_two_scale_allowance():
