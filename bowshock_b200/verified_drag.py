@@ -147,11 +147,13 @@ def verified_forebody_drag(body: Body, mach: float, gamma: float = 1.4, toleranc
 def verified_forebody_drags(cases: list[tuple[Body, float]], gamma: float = 1.4, tolerance: float = 1e-4,
                             max_refinement: int = 8, noise: float = ENGINE_NOISE,
                             floor: float = DRAG_FLOOR, order_tolerance: float = ORDER_TOLERANCE,
-                            precision: int = 64) -> list[VerifiedDrag]:
+                            precision: int = 64, metric_bits: int = 32) -> list[VerifiedDrag]:
     """The same procedure for many (body, Mach) cases: each refinement level
     of every case not yet verified is one GPU batch, iterated in checks of
     500 r steps; a case whose drag has settled is frozen while the others go
-    on. The outcome of every case is the one verified_forebody_drag gives."""
+    on. The outcome of every case is the one verified_forebody_drag gives.
+    `metric_bits` 64 makes the residual read two-float metrics (the steady
+    state of the FP64 CPU engine, at 24 more bytes per cell)."""
     from .batch import CudaBatch
 
     n = len(cases)
@@ -167,6 +169,8 @@ def verified_forebody_drags(cases: list[tuple[Body, float]], gamma: float = 1.4,
         grids = [body_grid(cases[k][0], BASE_NJ, cases[k][1], gamma, refinement=r).grid for k in todo]
         batch = CudaBatch([steady_drag_config(g, frees[k].state, gamma) for g, k in zip(grids, todo)],
                           precision=precision)
+        if metric_bits != 32:
+            batch.set_metric_precision(metric_bits)
         try:
             batch.set_free_stream()
             settle = [SettlingValue(noise) for _ in todo]

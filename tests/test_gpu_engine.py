@@ -171,6 +171,28 @@ def test_verified_drag_pin_on_the_gpu():
         engine.destroy()
 
 
+def test_verified_drag_pin_with_two_float_metrics_is_the_cpu_engines():
+    # The same steady state with two-float metrics in the residual: the GPU
+    # drag meets the reference CPU engine's 0.283146976102 as the FP64
+    # oracle does (4.2e-9), where the FP32 metrics leave it near 1e-7.
+    body = cone_body(20, 4.0)
+    free = free_stream_at(3.0, GAMMA)
+    bg = body_grid(body, 20, 3.0, GAMMA)
+    cfg = steady_drag_config(bg.grid, free.state)
+    drags = {}
+    for bits in (32, 64):
+        with CudaEuler2D(cfg) as e:
+            e.set_metric_precision(bits)
+            e.set_uniform(free.state)
+            e.iterate(1500)
+            assert e.density_residual_norm() < 1e-11
+            drags[bits] = forebody_pressure_drag(e.boundary_fluxes("jMin"), free, 0.5)
+    print(f"cone pin: FP32 metrics {drags[32] / 0.283146976102 - 1:+.2e}, "
+          f"two-float {drags[64] / 0.283146976102 - 1:+.2e}")
+    assert abs(drags[64] / 0.283146976102 - 1) < 1e-8
+    assert abs(drags[32] / 0.283146976102 - 1) < 2e-6
+
+
 def test_lusgs_reaches_the_explicit_steady_state():
     # tests/engine-cpu/implicit.test.ts:201-240: LU-SGS from CFL 1 up to 1000
     # reaches the explicit scheme's drag; the GPU's FP32 operator changes only
