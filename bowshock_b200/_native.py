@@ -110,7 +110,7 @@ SIGNATURES: dict[str, list] = {
     "bs_grid_info": [_vp, _ip, _dp],
     "bs_grid_two_scale": [_vp, _ip],
     "bs_transonic_grid": [C.POINTER(abi.Body), C.POINTER(abi.TransonicGridOptions), C.POINTER(_vp)],
-    "bs_grid_transonic_info": [_vp, _ip, _ip, _dp, _dp, _dp],
+    "bs_grid_transonic_info": [_vp, _ip, _ip, _dp, _dp, _dp, _ip],
     "bs_grid_destroy": [_vp],
     "bs_grid_quality_of": [C.c_int32, C.c_int32, _dp, _dp, C.POINTER(abi.GridQuality)],
     "bs_taylor_maccoll": [C.c_double, C.c_double, C.c_double, C.c_double,

@@ -118,7 +118,7 @@ class BodyGridOptions(C.Structure):
 class TransonicGridOptions(C.Structure):
     _fields_ = [
         ("refinement", C.c_int32),
-        ("reserved", C.c_int32),
+        ("nested", C.c_int32),
         ("far_field", C.c_double),
         ("cylinder", C.c_double),
         ("wall", C.c_double),
@@ -127,6 +127,8 @@ class TransonicGridOptions(C.Structure):
         ("shoulder", C.c_double),
         ("nose", C.c_double),
         ("nose_growth", C.c_double),
+        ("nested_far_field", C.c_double),
+        ("nested_cylinder", C.c_double),
     ]
 
 

@@ -132,6 +132,12 @@ bs_status bs_transonic_grid(const bs_body* body, const bs_transonic_grid_options
   o.refinement = options->refinement;
   o.far_field = options->far_field;
   o.cylinder = options->cylinder;
+  o.nested = options->nested != 0;
+  o.nested_far_field = options->nested_far_field;
+  o.nested_cylinder = options->nested_cylinder;
+  if (!(std::isfinite(o.nested_far_field) && std::isfinite(o.nested_cylinder) && o.nested_far_field >= 0 &&
+        o.nested_cylinder >= 0))
+    return bs::fail(BS_INVALID_ARGUMENT, "the nested domain's far field and cylinder must be 0 or positive");
   // A spacing of 0 takes the default.
   const double given[6] = {options->wall, options->growth, options->tip, options->shoulder, options->nose,
                            options->nose_growth};
@@ -152,7 +158,7 @@ bs_status bs_transonic_grid(const bs_body* body, const bs_transonic_grid_options
 }
 
 bs_status bs_grid_transonic_info(const bs_grid* grid, int32_t* i_shoulder, int32_t* base_nj, double* far_radius,
-                                 double* x_upstream, double* x_end) {
+                                 double* x_upstream, double* x_end, int32_t* c_topology) {
   if (grid == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
   if (!grid->transonic) return bs::fail(BS_INVALID_ARGUMENT, "not a transonic grid");
   if (i_shoulder) *i_shoulder = grid->info.i_shoulder;
@@ -160,6 +166,7 @@ bs_status bs_grid_transonic_info(const bs_grid* grid, int32_t* i_shoulder, int32
   if (far_radius) *far_radius = grid->info.far_radius;
   if (x_upstream) *x_upstream = grid->info.x_upstream;
   if (x_end) *x_end = grid->info.x_end;
+  if (c_topology) *c_topology = grid->info.c_topology ? 1 : 0;
   return bs::ok();
 }
 

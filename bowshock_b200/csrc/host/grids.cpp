@@ -655,6 +655,147 @@ std::vector<double> sharp_fit_columns(const Body& body, double beta, double x0, 
   return column_positions(bp, [&](double x) { return density / spacing(x); }, refinement, 0);
 }
 
+namespace {
+
+// bluntGrid (src/grid/transonic-grid.ts:319-460): the C grid of a blunt nose
+// on the spacings of the sharp noses' grid: columns by arc length along the
+// body (s.tip at the stagnation point, s.shoulder at the shoulder, at most
+// s.nose apart, growing by s.growth along the cylinder), rows by the same
+// geometric growth out to a far boundary that is a quarter circle of the far
+// radius about the stagnation point continued at the far radius. Each line
+// leaves its body point P along the body normal averaged over a window and
+// bends to its point Q on the far boundary (Q evenly spaced along it):
+// node = P + d (f (1 - f) n + f^2 u), d = |Q - P|, u = (Q - P) / d.
+std::string transonic_c_grid(const Body& body, const TransonicSpacing& s, int refinement, int base_nj,
+                             double far_radius, double x_end, Grid* out, int* i_shoulder_out) {
+  constexpr int kProfileSamples = 20000;
+  constexpr double kSmoothing = 0.25, kMaxWidthSlope = 0.5;
+  constexpr int kWindowSamples = 64;
+  const Nose& nose = body.nose;
+  const double L = nose.length, R = nose.base_radius;
+  auto profile_x = [&](double u) { return L * u * u; };
+  auto profile_r = [&](double u) { return nose_radius(nose, profile_x(u)); };
+  std::vector<double> u_of(kProfileSamples + 1, 0.0), s_of(kProfileSamples + 1, 0.0);
+  for (int k = 1; k <= kProfileSamples; k++) {
+    const double u0 = double(k - 1) / kProfileSamples, u1 = double(k) / kProfileSamples;
+    u_of[k] = u1;
+    s_of[k] = s_of[k - 1] + std::hypot(profile_x(u1) - profile_x(u0), profile_r(u1) - profile_r(u0));
+  }
+  const double s_nose = s_of[kProfileSamples];
+  const double s_end = s_nose + (x_end - L);
+  auto u_at = [&](double arc) {
+    int low = 0, high = kProfileSamples;
+    while (high - low > 1) {
+      const int mid = (low + high) >> 1;
+      if (s_of[mid] <= arc) low = mid;
+      else high = mid;
+    }
+    const double f = (arc - s_of[low]) / (s_of[high] - s_of[low]);
+    return u_of[low] + std::min(std::max(f, 0.0), 1.0) / kProfileSamples;
+  };
+  struct P {
+    double x, y, nx, ny;
+  };
+  auto surface = [&](double arc) -> P {
+    if (arc >= s_nose) return {L + (arc - s_nose), R, 0, 1};
+    const double u = u_at(arc);
+    if (u == 0) return {0, 0, -1, 0};
+    const double e = 1e-7;
+    const double ua = std::max(u - e, 0.0), ub = std::min(u + e, 1.0);
+    const double tx = profile_x(ub) - profile_x(ua), ty = profile_r(ub) - profile_r(ua);
+    const double t = std::hypot(tx, ty);
+    return {profile_x(u), profile_r(u), -ty / t, tx / t};
+  };
+  if (!(std::abs(surface(s_nose * (1 - 1e-9)).nx) < 1e-3))
+    return "blunt noses that do not meet the body tangentially are not supported by the transonic grid yet";
+  auto spacing = [&](double arc) {
+    return arc >= s_nose ? s.shoulder * R + s.growth * (arc - s_nose)
+                         : std::min(std::min(s.tip * R + s.nose_growth * arc,
+                                             s.shoulder * R + s.nose_growth * (s_nose - arc)),
+                                    s.nose * R);
+  };
+  const std::vector<double> arcs = column_positions(
+      {0.0, s_nose, s_end}, [&](double arc) { return refinement / spacing(arc); }, refinement, 0);
+  const int ni = int(arcs.size()) - 1;
+  int i_shoulder = -1;
+  for (int i = 0; i <= ni && i_shoulder < 0; i++)
+    if (arcs[i] == s_nose) i_shoulder = i;
+  std::vector<P> points(ni + 1);
+  for (int i = 0; i <= ni; i++) points[i] = surface(arcs[i]);
+  const double quarter = (M_PI / 2) * far_radius;
+  const double far_length = quarter + x_end;
+  auto far = [&](double t, double* qx, double* qy) {
+    if (t <= quarter) {
+      *qx = -far_radius * std::cos(t / far_radius);
+      *qy = far_radius * std::sin(t / far_radius);
+    } else {
+      *qx = t - quarter;
+      *qy = far_radius;
+    }
+  };
+  // Angle of the body normal to the upstream axis, odd about the stagnation
+  // point, pi / 2 from the shoulder on.
+  std::function<double(double)> normal_angle = [&](double arc) -> double {
+    if (arc < 0) return -normal_angle(-arc);
+    if (arc >= s_nose) return M_PI / 2;
+    const P p = surface(arc);
+    return std::atan2(p.ny, -p.nx);
+  };
+  // The normal averaged over a window of half-width the harmonic
+  // combination of kSmoothing h and kMaxWidthSlope times the distance to
+  // the end of the body.
+  auto direction = [&](double arc, double h, double* dx, double* dy) {
+    const double a = kSmoothing * h;
+    const double c = kMaxWidthSlope * (s_end - arc);
+    const double w = a + c > 0 ? (a * c) / (a + c) : 0;
+    double angle;
+    if (arc == 0 || w == 0) {
+      angle = normal_angle(arc);
+    } else {
+      double sum = 0;
+      for (int k = 0; k < kWindowSamples; k++)
+        sum += normal_angle(arc - w + (2 * w * (k + 0.5)) / kWindowSamples);
+      angle = sum / kWindowSamples;
+    }
+    *dx = -std::cos(angle);
+    *dy = std::sin(angle);
+  };
+  const int nj = base_nj * refinement;
+  const double b = s.growth * base_nj;
+  out->ni = ni;
+  out->nj = nj;
+  out->i_tip = 0;
+  out->outer_angle = 0;
+  out->two_scale = false;
+  out->x.assign(size_t(ni + 1) * (nj + 1), 0);
+  out->y.assign(size_t(ni + 1) * (nj + 1), 0);
+  for (int i = 0; i <= ni; i++) {
+    const P& p = points[i];
+    double qx, qy;
+    if (i == ni) {
+      qx = x_end;
+      qy = far_radius;
+    } else {
+      far((far_length * i) / ni, &qx, &qy);
+    }
+    const double d = std::hypot(qx - p.x, qy - p.y);
+    const double ux = (qx - p.x) / d, uy = (qy - p.y) / d;
+    for (int j = 0; j <= nj; j++) {
+      const double f = std::expm1((b * j) / nj) / std::expm1(b);
+      const double along = f * (1 - f);
+      double nx, ny;
+      direction(arcs[i], d * f, &nx, &ny);
+      const size_t k = i + size_t(j) * (ni + 1);
+      out->x[k] = p.x + d * (along * nx + f * f * ux);
+      out->y[k] = p.y + d * (along * ny + f * f * uy);
+    }
+  }
+  *i_shoulder_out = i_shoulder;
+  return "";
+}
+
+}  // namespace
+
 std::string transonic_grid(const Body& body, const TransonicGridOptions& o, Grid* out,
                            TransonicGridInfo* info) {
   std::string e = validate_body(body);
@@ -668,8 +809,7 @@ std::string transonic_grid(const Body& body, const TransonicGridOptions& o, Grid
   const TransonicSpacing& s = o.spacing;
   if (!(s.wall > 0 && s.growth > 0 && s.tip > 0 && s.shoulder > 0 && s.nose > 0 && s.nose_growth > 0))
     return "the transonic grid's spacings must be positive";
-  if (!std::isfinite(nose_tip_slope(body.nose)))
-    return "the transonic grid is built for sharp noses only here (the C grids of blunt noses are not)";
+  const bool blunt = !std::isfinite(nose_tip_slope(body.nose));
   const double wall = s.wall * R, growth = s.growth;
   // Cells across on the base grid: geometric growth from the wall spacing
   // reaches the far radius in this many cells.
@@ -678,6 +818,18 @@ std::string transonic_grid(const Body& body, const TransonicGridOptions& o, Grid
   const double x_upstream = -far_radius;
   const double x_end = L + 2 * R * o.cylinder;
   const int nj = base_nj * refinement;
+  if (blunt) {
+    if (o.nested) return "nested domains are not available on the C grids of blunt noses yet";
+    e = transonic_c_grid(body, s, refinement, base_nj, far_radius, x_end, out, &info->i_shoulder);
+    if (!e.empty()) return e;
+    info->i_tip = 0;
+    info->base_nj = base_nj;
+    info->far_radius = far_radius;
+    info->x_upstream = x_upstream;
+    info->x_end = x_end;
+    info->c_topology = true;
+    return "";
+  }
   // Column spacing along x: growing geometrically from the tip and from the
   // shoulder, at most s.nose along the nose.
   const double tip = s.tip * R, shoulder = s.shoulder * R;
@@ -698,30 +850,118 @@ std::string transonic_grid(const Body& body, const TransonicGridOptions& o, Grid
   // / expm1(b) of the way, b = growth base_nj; the lines lean, by f^2 of the
   // way, to points evenly spaced along the far boundary.
   const double b = growth * base_nj;
-  out->ni = ni;
-  out->nj = nj;
-  out->i_tip = i_tip;
+  auto node = [&](int i, int j, double* x_out, double* y_out) {
+    const double x = xs[i];
+    const double r = body_radius(body, x);
+    const double f = std::expm1((b * j) / nj) / std::expm1(b);
+    const double x_far = x_upstream + ((x_end - x_upstream) * i) / ni;
+    *x_out = x + (x_far - x) * f * f;
+    *y_out = r + (far_radius - r) * f;
+  };
   out->outer_angle = 0;
   out->two_scale = false;
-  out->x.assign(size_t(ni + 1) * (nj + 1), 0);
-  out->y.assign(size_t(ni + 1) * (nj + 1), 0);
-  for (int j = 0; j <= nj; j++) {
-    const double f = std::expm1((b * j) / nj) / std::expm1(b);
-    for (int i = 0; i <= ni; i++) {
-      const double x = xs[i];
-      const double r = body_radius(body, x);
-      const double x_far = x_upstream + ((x_end - x_upstream) * i) / ni;
-      const size_t k = i + size_t(j) * (ni + 1);
-      out->x[k] = x + (x_far - x) * f * f;
-      out->y[k] = r + (far_radius - r) * f;
-    }
+  info->c_topology = false;
+  if (!o.nested) {
+    out->ni = ni;
+    out->nj = nj;
+    out->i_tip = i_tip;
+    out->x.assign(size_t(ni + 1) * (nj + 1), 0);
+    out->y.assign(size_t(ni + 1) * (nj + 1), 0);
+    for (int j = 0; j <= nj; j++)
+      for (int i = 0; i <= ni; i++) {
+        const size_t k = i + size_t(j) * (ni + 1);
+        node(i, j, &out->x[k], &out->y[k]);
+      }
+    info->i_tip = i_tip;
+    info->i_shoulder = i_shoulder;
+    info->base_nj = base_nj;
+    info->far_radius = far_radius;
+    info->x_upstream = x_upstream;
+    info->x_end = x_end;
+    return "";
   }
-  info->i_tip = i_tip;
-  info->i_shoulder = i_shoulder;
-  info->base_nj = base_nj;
-  info->far_radius = far_radius;
-  info->x_upstream = x_upstream;
-  info->x_end = x_end;
+
+  // nestedGrid (:191-303): the grid cut back or continued to the nested far
+  // boundaries and cylinder in whole base cells, every node the two domains
+  // share the same. Beyond the grid's own columns the spacing grows on
+  // geometrically as inside, as vertical lines; beyond its far radius the
+  // rows grow on as on the axis, as horizontal lines.
+  const double g = growth;
+  const double far = (o.nested_far_field == 0 || o.nested_far_field == o.far_field) ? far_radius
+                                                                                       : o.nested_far_field * R;
+  const double cylinder_end = L + 2 * R * (o.nested_cylinder != 0 ? o.nested_cylinder : o.cylinder);
+  if (!(far > 4 * std::max(R, L))) return "the far boundaries must lie beyond four nose lengths";
+  if (!(cylinder_end > L)) return "the transonic domain needs a cylinder";
+  auto row = [&](double j) { return (wall / g) * std::expm1((g * j) / refinement); };
+  const double upstream_step = std::log1p((g * -x_upstream) / tip) / g / (double(i_tip) / refinement);
+  const double downstream_step =
+      std::log1p((g * (x_end - L)) / shoulder) / g / (double(ni - i_shoulder) / refinement);
+  auto x_before = [&](double k) { return -((tip + g * -x_upstream) * std::exp(g * k * upstream_step) - tip) / g; };
+  auto x_beyond = [&](double k) {
+    return L + ((shoulder + g * (x_end - L)) * std::exp(g * k * downstream_step) - shoulder) / g;
+  };
+  auto x_at = [&](int i) {
+    return i < 0 ? x_before(double(-i) / refinement) : i > ni ? x_beyond(double(i - ni) / refinement) : xs[i];
+  };
+  int j_hi = nj, i_lo = 0;
+  if (far < far_radius) {
+    int jb = 1;
+    while (row(jb * refinement) < far) jb++;
+    j_hi = jb * refinement;
+    int m = 0;
+    while (xs[(m + 1) * refinement] <= -far) m++;
+    i_lo = m * refinement;
+  } else if (far > far_radius) {
+    j_hi = refinement * int(std::ceil(std::log1p((g * far) / wall) / g - 1e-9));
+    int k = 1;
+    while (x_before(k) > -far) k++;
+    i_lo = -k * refinement;
+  }
+  int i_hi = ni;
+  if (cylinder_end < x_end) {
+    int m = i_shoulder / refinement + 1;
+    while (xs[m * refinement] < cylinder_end) m++;
+    i_hi = m * refinement;
+  } else if (cylinder_end > x_end) {
+    int k = 1;
+    while (x_beyond(k) < cylinder_end) k++;
+    i_hi = ni + k * refinement;
+  }
+  auto x_far = [&](int i) { return x_upstream + ((x_end - x_upstream) * i) / ni; };
+  const int nni = i_hi - i_lo;
+  out->ni = nni;
+  out->nj = j_hi;
+  out->i_tip = i_tip - i_lo;
+  out->x.assign(size_t(nni + 1) * (j_hi + 1), 0);
+  out->y.assign(size_t(nni + 1) * (j_hi + 1), 0);
+  for (int j = 0; j <= j_hi; j++)
+    for (int ii = 0; ii <= nni; ii++) {
+      const int i = ii + i_lo;
+      const size_t k = ii + size_t(j) * (nni + 1);
+      double x, y;
+      if (i >= 0 && i <= ni && j <= nj) {
+        node(i, j, &x, &y);
+      } else if (j > nj) {
+        x = (i < 0 || i > ni) ? x_at(i) : x_far(i);
+        y = row(j);
+      } else if (i < 0) {
+        x = x_at(i);
+        y = row(j);
+      } else {
+        // Beyond the end along x: vertical lines with the end column's rows.
+        const double f = std::expm1((g * j) / refinement) / std::expm1((g * nj) / refinement);
+        x = x_at(i);
+        y = R + (far_radius - R) * f;
+      }
+      out->x[k] = x;
+      out->y[k] = y;
+    }
+  info->i_tip = i_tip - i_lo;
+  info->i_shoulder = i_shoulder - i_lo;
+  info->base_nj = j_hi / refinement;
+  info->far_radius = row(j_hi);
+  info->x_upstream = x_at(i_lo);
+  info->x_end = x_at(i_hi);
   return "";
 }
 

@@ -105,19 +105,28 @@ struct TransonicGridOptions {
   double far_field = 100;   // far boundaries at least this many body radii out
   double cylinder = 10;     // calibers of cylinder solved behind the nose
   TransonicSpacing spacing;
+  // The grid cut back or continued, node for node, to these far boundaries
+  // and cylinder (0: the grid's own), for sharp noses (nestedGrid).
+  bool nested = false;
+  double nested_far_field = 0, nested_cylinder = 0;
 };
 
 struct TransonicGridInfo {
   int i_tip = 0, i_shoulder = 0, base_nj = 0;
   double far_radius = 0, x_upstream = 0, x_end = 0;
+  bool c_topology = false;  // C grid of a blunt nose (else H)
 };
 
-// transonicGrid (src/grid/transonic-grid.ts:128-189) for sharp noses: the
-// H grid of a nose and a long cylinder in a domain reaching far upstream,
+// transonicGrid (src/grid/transonic-grid.ts:128-189): for sharp noses the H
+// grid of a nose and a long cylinder in a domain reaching far upstream,
 // sideways and downstream (jMin the axis ahead of the tip and the body,
 // jMax the far radius, iMin the far boundary upstream, iMax the plane
-// ending the cylinder); cells growing geometrically away from the wall and
-// from the tip and shoulder along the axis; refined grids nest.
+// ending the cylinder), optionally cut back or continued to a nested domain
+// (nestedGrid, :191-303); for blunt noses the C grid (bluntGrid, :319-460:
+// jMin the body from the stagnation point, iMin the axis ahead of it, jMax a
+// quarter circle about the stagnation point continued at the far radius).
+// Cells grow geometrically away from the wall and from the tip and shoulder
+// along the body; refined grids nest.
 std::string transonic_grid(const Body& body, const TransonicGridOptions& options, Grid* out,
                            TransonicGridInfo* info);
 

@@ -139,17 +139,26 @@ class TransonicGrid:
 
 
 def transonic_grid(body: Body, refinement: int = 1, far_field: float = 100.0, cylinder: float = 10.0,
-                   spacing: dict | None = None, lib=None) -> TransonicGrid:
-    """transonicGrid (src/grid/transonic-grid.ts:128-189) for sharp noses:
-    the H grid of the nose and `cylinder` calibers of cylinder, its far
-    boundaries `far_field` body radii out (rounded up to whole base cells);
-    `spacing` overrides TRANSONIC_SPACING's entries (wall, growth, tip,
-    shoulder, nose, nose_growth)."""
+                   spacing: dict | None = None, nested: dict | None = None, lib=None) -> TransonicGrid:
+    """transonicGrid (src/grid/transonic-grid.ts:128-460): the H grid of a
+    sharp nose (the C grid of a blunt one) and `cylinder` calibers of
+    cylinder, its far boundaries `far_field` body radii out (rounded up to
+    whole base cells); `spacing` overrides TRANSONIC_SPACING's entries (wall,
+    growth, tip, shoulder, nose, nose_growth); `nested` ({"far_field": ...,
+    "cylinder": ...}) cuts the H grid back or continues it to that domain,
+    every shared node the same."""
     L = lib or _native.load()
     o = abi.TransonicGridOptions()
     o.refinement = refinement
     o.far_field = far_field
     o.cylinder = cylinder
+    if nested is not None:
+        unknown = set(nested) - {"far_field", "cylinder"}
+        if unknown:
+            raise ValueError(f"unknown nested-domain entries {sorted(unknown)}")
+        o.nested = 1
+        o.nested_far_field = float(nested.get("far_field", 0.0))
+        o.nested_cylinder = float(nested.get("cylinder", 0.0))
     for k, v in (spacing or {}).items():
         if k not in ("wall", "growth", "tip", "shoulder", "nose", "nose_growth"):
             raise ValueError(f"unknown transonic spacing {k!r}")
@@ -159,16 +168,17 @@ def transonic_grid(body: Body, refinement: int = 1, far_field: float = 100.0, cy
     b = body.to_abi()
     h = C.c_void_p()
     _native.check(L.bs_transonic_grid(C.byref(b), C.byref(o), C.byref(h)), L)
-    shoulder, base_nj = C.c_int32(), C.c_int32()
+    shoulder, base_nj, c_grid = C.c_int32(), C.c_int32(), C.c_int32()
     far, up, end = C.c_double(), C.c_double(), C.c_double()
     try:
         _native.check(L.bs_grid_transonic_info(h, C.byref(shoulder), C.byref(base_nj), C.byref(far), C.byref(up),
-                                               C.byref(end)), L)
+                                               C.byref(end), C.byref(c_grid)), L)
     except BaseException:
         L.bs_grid_destroy(h)
         raise
     grid, tip, _ = _take(h, L)
-    return TransonicGrid(grid, tip, shoulder.value, far.value, up.value, end.value, base_nj.value)
+    return TransonicGrid(grid, tip, shoulder.value, far.value, up.value, end.value, base_nj.value,
+                         "C" if c_grid.value else "H")
 
 
 def ramp_grid(ni: int, nj: int, x_min: float, x_corner: float, x_max: float, height: float,

@@ -42,18 +42,21 @@ class TransonicProblem:
 
 
 def transonic_problem(body: Body, mach: float, gamma: float = 1.4, refinement: int = 1, far_field: float = 100.0,
-                      cylinder: float = 10.0, spacing: dict | None = None) -> TransonicProblem:
-    """transonicProblem (transonic-flow.ts:59-90): the transonic H grid, far
-    fields upstream, outside and downstream, the body (and the axis ahead of
-    it) a wall; HLLC, van Albada with the scaled shared factor,
-    axisymmetric."""
-    grid = transonic_grid(body, refinement, far_field, cylinder, spacing)
+                      cylinder: float = 10.0, spacing: dict | None = None,
+                      nested: dict | None = None) -> TransonicProblem:
+    """transonicProblem (transonic-flow.ts:59-90): the transonic grid, far
+    fields around it, the body (and the axis ahead of it) a wall: on the H
+    grid of a sharp nose iMin is a far boundary upstream, on the C grid of a
+    blunt one the axis ahead of the stagnation point; HLLC, van Albada with
+    the scaled shared factor, axisymmetric."""
+    grid = transonic_grid(body, refinement, far_field, cylinder, spacing, nested)
     free = free_stream_at(mach, gamma)
     far = Boundary("farField", free.state)
     config = Euler2DConfig(
         grid=grid.grid, geometry="axisymmetric", gamma=gamma, flux="hllc", limiter="vanAlbada",
         reconstruction="sharedScaled", time_integrator="ssprk2", cfl=0.8, time_stepping="local",
-        boundaries={"iMin": far, "iMax": far, "jMin": Boundary("wall"), "jMax": far})
+        boundaries={"iMin": far if grid.topology == "H" else Boundary("wall"), "iMax": far,
+                    "jMin": Boundary("wall"), "jMax": far})
     return TransonicProblem(body, mach, gamma, refinement, far_field, cylinder, grid, config, free)
 
 

@@ -475,26 +475,35 @@ BS_API bs_status bs_blunt_body_grid_bounded(const bs_body *body, const bs_body_g
  * shoulder 0.02, nose 0.2, nose_growth 0.1). */
 typedef struct bs_transonic_grid_options {
   int32_t refinement;
-  int32_t reserved;
+  int32_t nested;  /* 1: cut back or continue the grid to nested_far_field / nested_cylinder */
   double far_field;
   double cylinder;
   double wall, growth, tip, shoulder, nose, nose_growth;
+  /* The nested domain (TransonicGridOptions.nested): far boundaries and
+   * cylinder, 0 for the grid's own; every node it shares with the grid is
+   * the same. Sharp noses only. */
+  double nested_far_field, nested_cylinder;
 } bs_transonic_grid_options;
 
-/* transonicGrid (src/grid/transonic-grid.ts:128-189), sharp noses: the H grid
- * of the nose and a long cylinder for flow from Mach 1 to about 1.2 (jMin the
- * axis ahead of the tip and the body, jMax the far radius, iMin the far
- * boundary upstream, iMax the plane ending the cylinder: give the far sides a
- * far-field condition); every base cell divides into refinement^2 cells of
- * the refined grid. Blunt noses' C grids are refused. */
+/* transonicGrid (src/grid/transonic-grid.ts:128-460): for flow from Mach 1 to
+ * about 1.2, the H grid of a sharp nose and a long cylinder (jMin the axis
+ * ahead of the tip and the body, jMax the far radius, iMin the far boundary
+ * upstream, iMax the plane ending the cylinder: give the far sides a
+ * far-field condition), optionally cut back or continued to a nested domain;
+ * or the C grid of a blunt nose meeting the body tangentially (jMin the body
+ * from the stagnation point, iMin the axis ahead of it: a wall, jMax a
+ * quarter circle about the stagnation point continued at the far radius,
+ * iMax the plane ending the cylinder). Every base cell divides into
+ * refinement^2 cells of the refined grid. */
 BS_API bs_status bs_transonic_grid(const bs_body *body, const bs_transonic_grid_options *options,
                                    bs_grid **out);
 /* TransonicGrid's fields (src/grid/transonic-grid.ts:84-101) of a grid from
  * bs_transonic_grid: the shoulder's column, the base grid's cells across, the
- * far radius, the upstream boundary's x and the end of the cylinder; the
- * tip's column is bs_grid_info's i_tip. */
+ * far radius, the upstream boundary's x, the end of the cylinder and the
+ * topology (1: C, 0: H); the tip's column is bs_grid_info's i_tip. */
 BS_API bs_status bs_grid_transonic_info(const bs_grid *grid, int32_t *i_shoulder, int32_t *base_nj,
-                                        double *far_radius, double *x_upstream, double *x_end);
+                                        double *far_radius, double *x_upstream, double *x_end,
+                                        int32_t *c_topology);
 
 /* rampGrid (src/grid/shapes.ts:30-52): a channel whose lower wall turns by
  * `angle` at x_corner. */

@@ -80,3 +80,21 @@ def test_two_float_metrics_put_the_steady_state_on_the_oracle():
                                s["plain_steps"])
     assert settled_gpu.converged and settled_ora.converged
     assert abs(settled_gpu.drag / settled_ora.drag - 1) < 2e-7
+
+
+def test_blunt_nose_on_its_c_grid_follows_the_oracle():
+    # A 2:1 ellipsoid at Mach 1.1 on its transonic C grid (the axis ahead of
+    # the stagnation point a wall): 2,000 accelerated steps on the GPU with
+    # two-float metrics and on the FP64 oracle give the same drag.
+    from oracle.transonic import solve_transonic as oracle_solve
+
+    body = Body(Nose(NoseShape("ellipsoid"), 2.0, 1.0), 0.0)
+    p = transonic_problem(body, 1.1)
+    assert p.grid.topology == "C" and p.config.boundaries["iMin"].kind == "wall"
+    deep = dict(noise=1e-15, max_steps=2000, check_every=50, cfl=1000.0, depth=8, plain_steps=200)
+    gpu = solve_transonic(p, **deep)
+    ora = oracle_solve(p, **deep)
+    print(f"ellipsoid M1.1: {p.grid.grid.ni} x {p.grid.grid.nj} cells, oracle {ora.drag:.12f}, "
+          f"GPU {gpu.drag:.12f} ({gpu.drag / ora.drag - 1:+.1e})")
+    assert math.isfinite(gpu.drag) and gpu.drag > 0
+    assert abs(gpu.drag / ora.drag - 1) < 1e-8

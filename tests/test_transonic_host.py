@@ -62,10 +62,127 @@ def test_transonic_grid_refusals():
         transonic_grid(body, 1, 20, 10)
     with pytest.raises(BowshockError, match="refinement"):
         transonic_grid(body, 3, 100, 10)
-    with pytest.raises(BowshockError, match="sharp noses"):
-        transonic_grid(Body(Nose(NoseShape("ellipsoid"), 1.0, 1.0), 0.0), 1, 100, 10)
     with pytest.raises(ValueError, match="positive"):
         transonic_grid(body, 1, 100, 10, spacing={"wall": -1})
+    # tests/grid/transonic-grid.test.ts:239-251: a blunt nose meeting the
+    # cylinder at an angle; nested domains on a blunt nose (:150-176).
+    corner = Body(Nose(NoseShape("power", 0.5), 2.0, 1.0), 0.0)
+    with pytest.raises(BowshockError, match="tangentially"):
+        transonic_grid(corner, 1, 100, 10)
+    with pytest.raises(BowshockError, match="blunt"):
+        transonic_grid(Body(Nose(NoseShape("ellipsoid"), 2.0, 1.0), 0.0), 1, 100, 10, nested={"far_field": 200})
+
+
+# ---- tests/grid/transonic-grid.test.ts ---------------------------------------------
+
+DEG = math.pi / 180
+CONE7 = Body(Nose(NoseShape("conical"), 1 / math.tan(7 * DEG), 1.0), 0.0)
+OGIVE6 = Body(Nose(NoseShape("ogive", 1.0), 6.0, 1.0), 0.0)
+
+
+def _nodes(tg):
+    g = tg.grid
+    return g.x.reshape(g.nj + 1, g.ni + 1), g.y.reshape(g.nj + 1, g.ni + 1)
+
+
+def _radius(body, x):
+    from bowshock_b200.fitted import _body_radius
+
+    return _body_radius(body, np.asarray(x, np.float64))
+
+
+@pytest.mark.parametrize("body", [CONE7, OGIVE6], ids=["cone", "ogive"])
+def test_sharp_grids_reach_the_far_boundaries_with_tip_and_shoulder_on_lines(body):
+    from bowshock_b200.grid import grid_quality
+
+    tg = transonic_grid(body, 1, 100, 10)
+    X, Y = _nodes(tg)
+    assert 100 <= tg.far_radius < 125 and tg.x_upstream == -tg.far_radius and tg.topology == "H"
+    assert tg.x_end == pytest.approx(body.nose.length + 20, abs=1e-12)
+    assert X[0, tg.i_tip] == 0 and X[0, tg.i_shoulder] == body.nose.length
+    assert np.allclose(Y[0], _radius(body, X[0]), rtol=0, atol=1e-12)
+    assert np.allclose(Y[-1], tg.far_radius, rtol=0, atol=1e-9)
+    q = grid_quality(tg.grid)
+    assert q.min_area > 0
+    assert q.min_wall_angle > 60 * DEG and q.min_angle > 30 * DEG and q.max_size_ratio < 1.4
+
+
+def test_sharp_grids_keep_the_near_body_rows_when_the_far_boundaries_move():
+    near, far = transonic_grid(CONE7, 1, 50, 10), transonic_grid(CONE7, 1, 400, 10)
+    assert far.grid.nj > near.grid.nj
+    Yn, Yf = _nodes(near)[1], _nodes(far)[1]
+    for j in range(1, 6):
+        assert abs(Yf[j, far.i_shoulder] / Yn[j, near.i_shoulder] - 1) < 0.05
+
+
+@pytest.mark.parametrize("nested", [{"far_field": 50}, {"far_field": 200}, {"cylinder": 5}, {"cylinder": 20}],
+                         ids=["far-50", "far-200", "cylinder-5", "cylinder-20"])
+def test_nested_domains_share_every_node_and_nest_under_refinement(nested):
+    from bowshock_b200.grid import grid_quality
+
+    for r in (1, 2):
+        plain = transonic_grid(CONE7, r, 100, 10)
+        g = transonic_grid(CONE7, r, 100, 10, nested=nested)
+        far = nested.get("far_field", 100)
+        assert g.far_radius >= far and -g.x_upstream >= far
+        assert g.x_end >= CONE7.nose.length + 2 * nested.get("cylinder", 10)
+        assert g.grid.nj % r == 0 and g.i_tip % r == 0
+        Xg, Yg = _nodes(g)
+        Xp, Yp = _nodes(plain)
+        assert Xg[0, g.i_tip] == 0
+        off = plain.i_tip - g.i_tip
+        nj = min(plain.grid.nj, g.grid.nj)
+        lo, hi = max(0, -off), min(g.grid.ni, plain.grid.ni - off)
+        assert np.array_equal(Xg[: nj + 1, lo: hi + 1], Xp[: nj + 1, lo + off: hi + off + 1])
+        assert np.array_equal(Yg[: nj + 1, lo: hi + 1], Yp[: nj + 1, lo + off: hi + off + 1])
+        assert hi - lo + 1 == min(plain.grid.ni, g.grid.ni) + 1
+        q = grid_quality(g.grid)
+        assert q.min_area > 0 and q.min_wall_angle > 60 * DEG and q.min_angle > 30 * DEG
+    c = transonic_grid(CONE7, 1, 100, 10, nested=nested)
+    f = transonic_grid(CONE7, 2, 100, 10, nested=nested)
+    assert f.grid.ni == 2 * c.grid.ni and f.grid.nj == 2 * c.grid.nj
+    Xc, Yc = _nodes(c)
+    Xf, Yf = _nodes(f)
+    assert max(np.abs(Xf[::2, ::2] - Xc).max(), np.abs(Yf[::2, ::2] - Yc).max()) < 1e-9
+
+
+def test_a_nested_domain_equal_to_the_grids_own_is_the_grid():
+    plain = transonic_grid(CONE7, 1, 100, 10)
+    same = transonic_grid(CONE7, 1, 100, 10, nested={"far_field": 100, "cylinder": 10})
+    assert np.array_equal(same.grid.x, plain.grid.x) and np.array_equal(same.grid.y, plain.grid.y)
+    assert same.far_radius == plain.far_radius
+
+
+@pytest.mark.parametrize("length", [1.0, 2.0, 3.0])
+def test_blunt_noses_get_a_c_grid_from_the_axis_ahead_to_the_end_of_the_cylinder(length):
+    from bowshock_b200.grid import grid_quality
+
+    body = Body(Nose(NoseShape("ellipsoid"), length, 1.0), 0.0)
+    tg = transonic_grid(body, 1, 100, 10)
+    X, Y = _nodes(tg)
+    assert tg.topology == "C" and tg.i_tip == 0
+    assert X[0, tg.i_shoulder] == pytest.approx(length, abs=1e-12)
+    assert np.allclose(Y[0], _radius(body, X[0]), rtol=0, atol=1e-9)
+    xf, yf = X[-1], Y[-1]
+    assert np.allclose(np.where(xf <= 0, np.hypot(xf, yf), yf), tg.far_radius, rtol=0, atol=1e-9)
+    assert np.all(Y[:, 0] == 0) and np.all(X[:, 0] <= 0)
+    assert np.allclose(X[:, -1], tg.x_end, rtol=0, atol=1e-12)
+    assert X[-1, 0] == pytest.approx(-tg.far_radius, abs=1e-9)
+    # The reference measured wall cells at 85.3 deg or more, corners at 51 deg
+    # or more, neighbours within 1.92 (hemisphere) and 1.43 in size.
+    q = grid_quality(tg.grid)
+    assert q.min_area > 0
+    assert q.min_wall_angle > 80 * DEG and q.min_angle > 45 * DEG
+    assert q.max_size_ratio < (2 if length == 1 else 1.5)
+
+
+def test_blunt_c_grids_nest():
+    body = Body(Nose(NoseShape("ellipsoid"), 2.0, 1.0), 0.0)
+    c, f = transonic_grid(body, 1, 100, 10), transonic_grid(body, 2, 100, 10)
+    assert f.grid.ni == 2 * c.grid.ni and f.grid.nj == 2 * c.grid.nj
+    Xc, Yc = _nodes(c)
+    Xf, Yf = _nodes(f)
+    assert max(np.abs(Xf[::2, ::2] - Xc).max(), np.abs(Yf[::2, ::2] - Yc).max()) < 1e-9
 
 
 def test_geometric_remaining():
