@@ -8,15 +8,16 @@
 //
 // (Walker and Ni's type II, undamped). A step on the GPU, after the residual
 // pass and the sweeps have left f in the diagonal-major dQ array:
-//   anderson_fnorm_kernel  |f|^2 per case (the restart rule needs it first);
 //   anderson_push_kernel   the new differences into the case's ring of
-//                          columns, and in the same pass their dot products
-//                          with every stored column and with f;
-//   anderson_solve_kernel  one thread per case: the Gram matrix of dF kept up
-//                          to date, its Cholesky factor (the R of a Gram-
-//                          Schmidt of dF) with the oldest columns dropped
-//                          while a column keeps less than 1e-6 of its norm,
-//                          and gamma;
+//                          columns, and in the same pass |f|^2 and their dot
+//                          products with every stored column and with f,
+//                          each tile's sums stored in a fixed order;
+//   anderson_solve_kernel  one warp per case: the tiles' sums added in a
+//                          fixed order, then in shared memory the Gram matrix
+//                          of dF kept up to date, its Cholesky factor (the R
+//                          of a Gram-Schmidt of dF) with the oldest columns
+//                          dropped while a column keeps less than 1e-6 of its
+//                          norm, and gamma (lane 0);
 //   anderson_apply_kernel  x + f - (dX + dF) gamma, flagging a case whose new
 //                          state is not physical;
 //   anderson_fallback_kernel  for a flagged case, the plain LU-SGS update of
@@ -194,13 +195,20 @@ __global__ void __launch_bounds__(32) anderson_solve_kernel(const AndersonArgs<R
     for (int t = int(threadIdx.x); t < ntiles; t += 32) s += rows[int64_t(t) * width + v];
     acc[v] = warp_sum(s);
   }
-  if (threadIdx.x != 0) return;
+  // The Gram matrix into shared memory (loaded by the warp), where lane 0
+  // updates it and factors it; the factor and the vectors of the solve too.
+  __shared__ double Gs[kMaxAndersonDepth * kMaxAndersonDepth];
+  __shared__ double Rm[kMaxAndersonDepth][kMaxAndersonDepth];
+  __shared__ double b[kMaxAndersonDepth], z[kMaxAndersonDepth], gs[kMaxAndersonDepth];
+  __shared__ int ord[kMaxAndersonDepth];
   double* G = A.gram + int64_t(c) * m * m;
+  for (int k = int(threadIdx.x); k < m * m; k += 32) Gs[k] = G[k];
+  __syncwarp();
+  if (threadIdx.x != 0) return;
   double* gam = A.gamma + int64_t(c) * m;
   const double fnorm = acc[0];
   const bool reset = anderson_reset(a, fnorm);
   const bool push = a.have_last && !reset;
-  double b[kMaxAndersonDepth];
   if (reset) {
     if (a.bad || fnorm > 100.0 * a.best) a.restarts++;
     if (fnorm > 100.0 * a.best) a.best = fnorm;
@@ -210,6 +218,8 @@ __global__ void __launch_bounds__(32) anderson_solve_kernel(const AndersonArgs<R
     const int slot = a.count < m ? a.count : a.head;
     const int ncols = min(a.count + 1, m);
     for (int p = 0; p < ncols; p++) {
+      Gs[slot * m + p] = acc[1 + p];
+      Gs[p * m + slot] = acc[1 + p];
       G[slot * m + p] = acc[1 + p];
       G[p * m + slot] = acc[1 + p];
       b[p] = acc[1 + ncols + p];
@@ -223,25 +233,22 @@ __global__ void __launch_bounds__(32) anderson_solve_kernel(const AndersonArgs<R
   a.best = fmin(a.best, fnorm);
   a.have_last = 1;
   a.bad = 0;
-  for (int p = 0; p < m; p++) gam[p] = 0.0;
+  for (int p = 0; p < m; p++) gs[p] = 0.0;
   const int n = push ? a.count : 0;
   // Columns oldest first; drop the oldest while the factor is not well
   // conditioned (anderson.ts:78-114 on the Gram matrix).
-  int ord[kMaxAndersonDepth];
   for (int t = 0; t < n; t++) ord[t] = a.count < m ? t : (a.head + t) % m;
-  double Rm[kMaxAndersonDepth][kMaxAndersonDepth];
-  double z[kMaxAndersonDepth];
   for (int first = 0; first < n; first++) {
     const int cols = n - first;
     bool ok = true;
     for (int cc = 0; cc < cols && ok; cc++) {
       const int sc = ord[first + cc];
       for (int p = 0; p < cc; p++) {
-        double s = G[ord[first + p] * m + sc];
+        double s = Gs[ord[first + p] * m + sc];
         for (int r = 0; r < p; r++) s -= Rm[r][p] * Rm[r][cc];
         Rm[p][cc] = s / Rm[p][p];
       }
-      double d = G[sc * m + sc];
+      double d = Gs[sc * m + sc];
       const double g0 = d;
       for (int p = 0; p < cc; p++) d -= Rm[p][cc] * Rm[p][cc];
       if (!(g0 > 0.0) || !(d > 1e-12 * g0)) {
@@ -258,11 +265,12 @@ __global__ void __launch_bounds__(32) anderson_solve_kernel(const AndersonArgs<R
     }
     for (int cc = cols - 1; cc >= 0; cc--) {
       double s = z[cc];
-      for (int p = cc + 1; p < cols; p++) s -= Rm[cc][p] * gam[ord[first + p]];
-      gam[ord[first + cc]] = s / Rm[cc][cc];
+      for (int p = cc + 1; p < cols; p++) s -= Rm[cc][p] * gs[ord[first + p]];
+      gs[ord[first + cc]] = s / Rm[cc][cc];
     }
     break;
   }
+  for (int p = 0; p < m; p++) gam[p] = gs[p];
   A.ac[c] = a;
 }
 
