@@ -51,7 +51,6 @@ struct CaseDev {
   int64_t iface;  // offset of its i-face arrays
   int64_t jface;  // offset of its j-face arrays
   int64_t skew;   // offset of its diagonal-major LU-SGS arrays, (ni + nj - 1) nj slots
-  int64_t tile_base;  // index of its first tile in the batch's tile order
   int32_t bc[4];  // bs_bc_kind per side
   int32_t flux, limiter, recon, axisym;
   int32_t integrator, local_dt;
@@ -63,6 +62,7 @@ struct CaseDev {
   // FP64), and the flux per unit area imposed on each face or null.
   const double* face_state[4] = {};
   const double* face_flux[4] = {};
+  int64_t tile_base = 0;  // index of its first tile in the batch's tile order
 };
 
 template <class R>

@@ -36,7 +36,6 @@ struct SweepArgs {
   const CaseDev* cases;
   const int* case_list;   // blockIdx.x -> case
   const int* active;      // per case (may be null)
-  MetricsView m;
   const float4* rec;      // sweep records, diagonal-major (5 float4 per slot, pass A)
   float4* dq;             // diagonal-major: forward result dQ*, then the final dQ
   float* cfl;             // per case current CFL number (ramped after the sweep)

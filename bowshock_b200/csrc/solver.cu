@@ -1136,7 +1136,6 @@ class Solver final : public SolverBase {
     S.cases = d_cases_.p;
     S.case_list = lane.case_list;
     S.active = d_active_.p;
-    S.m = metrics();
     S.rec = rec_.p;
     S.dq = dq_.p;
     S.cfl = cfl_.p;

@@ -199,7 +199,6 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
     bsd::SweepArgs S{};
     S.cases = d_case;
     S.case_list = &d_words->case_list;
-    S.m = m;
     S.rec = d_rec;
     S.dq = d_dq;
     S.cfl = &d_words->cfl;
