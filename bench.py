@@ -720,6 +720,21 @@ def run_fitted(args) -> None:
                                "extrapolated": v.estimate.extrapolated, "order": v.estimate.order,
                                "levels": [{"refinement": rep.refinement, "cells": rep.ni * rep.nj,
                                            "steps": rep.iterations, "drag": rep.drag} for rep in vb.reports]})
+    # A two-scale nose: the 1-caliber Von Karman nose with a caliber of body at
+    # Mach 2 (the reference measured its fitted drags 0.42909806331 on nj = 20
+    # and 0.42869653926 on nj = 40, tests/analysis/two-scale-fit.test.ts:29).
+    t0 = time.perf_counter()
+    vk = verified_fitted_drag(Body(Nose(NoseShape("haack", 0.0), 1.0, 0.5), 1.0), 2.0, tolerance=1e-3,
+                              max_refinement=8)
+    verified_two_scale = {"case": "Von Karman nose 1 caliber + 1 caliber of body, Mach 2, base nj 20",
+                          "kind": vk.kind, "wall_s": time.perf_counter() - t0, "allowance": vk.floor,
+                          "reference_drags_nj20_nj40": [0.42909806331220435, 0.42869653925562817]}
+    if vk.result is not None:
+        v = vk.result
+        verified_two_scale.update({"value": v.estimate.value, "band": v.uncertainty, "verified": v.verified,
+                                   "extrapolated": v.estimate.extrapolated, "order": v.estimate.order,
+                                   "levels": [{"refinement": rep.refinement, "cells": rep.ni * rep.nj,
+                                               "steps": rep.iterations, "drag": rep.drag} for rep in vk.reports]})
     cpu = None
     if not args.no_cpu_baseline:
         from oracle.shock_fitting import fit_shock
@@ -741,6 +756,7 @@ def run_fitted(args) -> None:
                                "hemisphere-cylinder Mach 2 at nj = 20; SSP-RK2 CFL 0.8 local steps, HLLC, "
                                "van Albada (shared scaled), axisymmetric"},
         "fits": rows, "observed_order": order, "verified_fitted_drag": verified, "verified_fitted_drag_blunt": verified_blunt,
+        "verified_fitted_drag_two_scale": verified_two_scale,
         "fitted_drag_curve": curve,
         "extrapolated_rel_err": errors[2] - (errors[1] - errors[2]) / 3,
         "cpu_baseline": cpu,

@@ -478,3 +478,36 @@ def test_a_lengthened_blunt_family_nests_at_mach_1_2():
         assert np.array_equal(fine.fractions[::2, ::2], coarse.fractions)
         assert started_from(fine, coarse, coarse.heights, coarse.initial) is not None
         coarse = fine
+
+
+def test_two_scale_boundary_keeps_its_margin_and_continues_the_last_segment():
+    # secondCapture's boundary (fitted-flow.ts:624-672) on made-up lines: at
+    # least 1.5 times the captured height and three outer cells above it
+    # before smoothing, smoothed by 50 passes of 1-2-1, its first point on the
+    # axis, and the last point continuing the segment before it where that
+    # rises.
+    from bowshock_b200.fitted import (BOUNDARY_CELLS, BOUNDARY_MARGIN, BOUNDARY_SMOOTHING, outer_cell_height,
+                                      two_scale_boundary)
+
+    n = 40
+    s = np.linspace(0, 1, n + 1)
+    angle = 0.5 * math.pi * np.minimum(s / 0.5, 1.0)
+    lines = np.stack([2.0 * s, 0.5 * np.sin(angle), -np.cos(angle), np.sin(angle)], 1)
+    lines[0, 1] = 0.0
+    heights = 0.2 + 0.3 * s
+    pts = two_scale_boundary(lines, heights, 20, 0.5)
+    assert pts.shape == (n + 1, 2) and pts[0, 1] == 0.0
+    d = (1 + BOUNDARY_MARGIN) * heights
+    for _ in range(20):
+        d = np.maximum(d, heights + BOUNDARY_CELLS * outer_cell_height(d, 20, 0.5))
+    assert np.all(d >= 1.5 * heights)
+    for _ in range(BOUNDARY_SMOOTHING):
+        c = d.copy()
+        d[0], d[-1] = 0.5 * (c[0] + c[1]), 0.5 * (c[-1] + c[-2])
+        d[1:-1] = 0.25 * c[:-2] + 0.5 * c[1:-1] + 0.25 * c[2:]
+    expected = lines[:, :2] + d[:, None] * lines[:, 2:]
+    assert np.array_equal(pts[:-1], expected[:-1])
+    (ax, ay), (bx, by) = expected[-3], expected[-2]
+    y = by + (lines[-1, 0] - bx) * (by - ay) / (bx - ax)
+    assert (pts[-1] == (lines[-1, 0], y)).all() if y > by else np.array_equal(pts[-1], expected[-1])
+    assert np.all(np.diff(pts[:, 1]) > 0)
