@@ -175,8 +175,8 @@ __global__ void __launch_bounds__(TILE_THREADS) anderson_push_kernel(const Ander
 }
 
 // One warp per case of the lane: the case's tile rows added in a fixed order
-// (lane l takes tiles l, l + 32, ..., then a fixed shuffle tree), then lane 0
-// updates the history and solves for the mixing coefficients.
+// (lane v adds value v over the tiles in order, every value at once), then
+// lane 0 updates the history and solves for the mixing coefficients.
 template <class R>
 __global__ void __launch_bounds__(32) anderson_solve_kernel(const AndersonArgs<R> A) {
   const int c = A.case_list[blockIdx.x];
@@ -189,11 +189,11 @@ __global__ void __launch_bounds__(32) anderson_solve_kernel(const AndersonArgs<R
   const int nv = 1 + 2 * pushed;
   const int ntiles = ((cd.ni + TI - 1) / TI) * ((cd.nj + TJ - 1) / TJ);
   const double* rows = A.part + cd.tile_base * width;
-  double acc[1 + 2 * kMaxAndersonDepth];
-  for (int v = 0; v < nv; v++) {
+  __shared__ double acc[1 + 2 * kMaxAndersonDepth];
+  for (int v = int(threadIdx.x); v < nv; v += 32) {
     double s = 0;
-    for (int t = int(threadIdx.x); t < ntiles; t += 32) s += rows[int64_t(t) * width + v];
-    acc[v] = warp_sum(s);
+    for (int t = 0; t < ntiles; t++) s += rows[int64_t(t) * width + v];
+    acc[v] = s;
   }
   // The Gram matrix into shared memory (loaded by the warp), where lane 0
   // updates it and factors it; the factor and the vectors of the solve too.
