@@ -306,3 +306,34 @@ def test_autotune_keeps_the_state_and_the_answer():
         results.append([b.forebody_drag(k, c.free, 0.5) for k, c in enumerate(cases)])
         b.destroy()
     assert np.allclose(results[0], results[1], rtol=1e-6, atol=0)
+
+
+def test_metric_precision_and_accelerated_steps_refuse_and_reduce_as_documented():
+    # bs_engine_set_metric_precision takes 32 or 64 bits, and 64 only on the
+    # FP64 engine; bs_engine_iterate_accelerated without acceleration (depth
+    # 0) is bs_engine_iterate_implicit, state for state.
+    from bowshock_b200._native import BowshockError
+
+    body = cone_body(20, 4.0)
+    free = free_stream_at(3.0, GAMMA)
+    cfg = steady_drag_config(body_grid(body, 10, 3.0, GAMMA).grid, free.state)
+    with CudaEuler2D(cfg) as e:
+        with pytest.raises(BowshockError, match="32 or 64"):
+            e.set_metric_precision(48)
+        e.set_metric_precision(64)
+        e.set_metric_precision(32)
+    with CudaEuler2D(cfg, precision=32) as e:
+        with pytest.raises(BowshockError, match="FP32 metrics"):
+            e.set_metric_precision(64)
+    states = []
+    for accelerated in (False, True):
+        with CudaEuler2D(cfg) as e:
+            e.set_uniform(free.state)
+            e.set_implicit_cfl(1.0)
+            if accelerated:
+                e.set_anderson(0)
+                e.iterate_accelerated(40, 50.0, 1.5, 1.2)
+            else:
+                e.iterate_implicit(40, 50.0, 1.5, 1.2)
+            states.append(e.primitives())
+    assert np.array_equal(states[0], states[1])
