@@ -794,7 +794,8 @@ def run_stencil(args) -> None:
     """HBM throughput of the stencil kernels on a batch larger than L2:
     `--cases` copies of a 640x320 case (a 15 deg cone, explicit SSP-RK3 stages;
     the fineness-3 ogive, LU-SGS passes), each kernel timed with CUDA events
-    over 20 launches; algorithmic bytes per cell as in DESIGN.md."""
+    over 20 launches against the algorithmic bytes per cell each kernel must
+    move (BYTES_PREPARE, BYTES_SWEEP, BYTES_UPDATE and the stage figures)."""
     from bowshock_b200.batch import CudaBatch
     from bowshock_b200.workloads import cone_case, ogive_case
 
