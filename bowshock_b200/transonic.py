@@ -112,22 +112,24 @@ def solve_transonic(problem: TransonicProblem, noise: float = 1e-7, max_steps: i
     reference's two-float engine: with FP32 metrics the drag's fixed point
     moves by 1e-6 to 5e-6 of its value on these far-field domains."""
     g = problem.grid.grid
+    w = None
+    if start is not None:
+        coarse, prims = start
+        ratio = problem.refinement / coarse.refinement
+        if not (ratio >= 1 and ratio == int(ratio)):
+            raise ValueError("a start must come from a coarser grid of the family")
+        r = int(ratio)
+        w = np.asarray(prims, np.float64).reshape(coarse.grid.grid.nj, coarse.grid.grid.ni, 4)
+        w = np.repeat(np.repeat(w, r, axis=0), r, axis=1)
+        if w.shape[:2] != (g.nj, g.ni):
+            raise ValueError("the start's grid is not the coarser grid of this family")
     t0 = time.perf_counter()
     with CudaEuler2D(problem.config) as engine:
         engine.set_metric_precision(metric_bits)
-        if start is None:
+        if w is None:
             engine.set_uniform(problem.free_stream.state)
             engine.set_implicit_cfl(1.0)
         else:
-            coarse, prims = start
-            ratio = problem.refinement / coarse.refinement
-            if not (ratio >= 1 and ratio == int(ratio)):
-                raise ValueError("a start must come from a coarser grid of the family")
-            r = int(ratio)
-            w = np.asarray(prims, np.float64).reshape(coarse.grid.grid.nj, coarse.grid.grid.ni, 4)
-            w = np.repeat(np.repeat(w, r, axis=0), r, axis=1)
-            if w.shape[:2] != (g.nj, g.ni):
-                raise ValueError("the start's grid is not the coarser grid of this family")
             engine.set_primitives(w.reshape(-1, 4))
             engine.set_implicit_cfl(cfl)
         engine.set_anderson(depth, plain_steps)

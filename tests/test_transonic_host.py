@@ -208,3 +208,18 @@ def test_oracle_solve_reproduces_the_measured_drag_on_the_base_grid():
     assert abs(out.drag - TN["drags"][0]) <= 5e-8
     exact = taylor_maccoll(TN["mach"], HALF, 1.4).surface_pressure_coefficient
     assert abs(out.drag / exact - 1) < TN["within_taylor_maccoll"]
+
+
+def test_a_start_must_come_from_a_coarser_grid_of_the_family():
+    # solveTransonic's refusal (transonic-flow.ts:162-166), before any GPU work.
+    from bowshock_b200.transonic import solve_transonic
+
+    coarse = transonic_problem(_cone(), TN["mach"], refinement=2)
+    fine = transonic_problem(_cone(), TN["mach"], refinement=1)
+    prims = np.ones((coarse.grid.grid.nj, coarse.grid.grid.ni, 4))
+    with pytest.raises(ValueError, match="coarser grid of the family"):
+        solve_transonic(fine, start=(coarse, prims))
+    other = transonic_problem(_cone(), TN["mach"], refinement=1, far_field=50)
+    with pytest.raises(ValueError, match="not the coarser grid"):
+        solve_transonic(transonic_problem(_cone(), TN["mach"], refinement=2),
+                        start=(other, np.ones((other.grid.grid.nj, other.grid.grid.ni, 4))))
