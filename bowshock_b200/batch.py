@@ -72,6 +72,10 @@ class CudaBatch:
         """64: two-float metrics in the residual; 32: FP32 metrics (default)."""
         self._call("bs_batch_set_metric_precision", int(bits))
 
+    def set_sweep_wait_limit(self, polls: int) -> None:
+        """As CudaEuler2D.set_sweep_wait_limit, for the batch's sweeps."""
+        self._call("bs_batch_set_sweep_wait_limit", int(polls))
+
     def set_anderson(self, depth: int, plain_steps: int = 30) -> None:
         """Anderson acceleration of later LU-SGS solves: `depth` differences
         kept (0: plain steps), after `plain_steps` plain steps."""

@@ -63,7 +63,7 @@ struct AndersonArgs {
   const int* active;
   StateView<R> q;
   StateView<R> last_x;
-  const float4* dq;       // diagonal-major, from the sweeps
+  const float4* dq;       // the sweeps' correction, row-major like the state
   float4* last_f;         // like the state
   float4* dx;             // depth columns: slot s of cell k at s * total + k
   float4* df;
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(TILE_THREADS) anderson_push_kernel(const Ander
   const int64_t k = cd.cell + i + int64_t(j) * cd.ni;
   float4 f = make_float4(0.f, 0.f, 0.f, 0.f), dfn = f;
   if (mine) {
-    f = A.dq[cd.skew + skew_slot(i, j, cd.nj)];
+    f = A.dq[k];
     const Cons<R> x = A.q.load(k);
     if (push) {
       const Cons<R> lx = A.last_x.load(k);
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(TILE_THREADS) anderson_apply_kernel(const Ande
   bool bad = false;
   if (anderson_cell(cd, tile, threadIdx.x, &i, &j)) {
     const int64_t k = cd.cell + i + int64_t(j) * cd.ni;
-    const float4 f = A.dq[cd.skew + skew_slot(i, j, cd.nj)];
+    const float4 f = A.dq[k];
     const Cons<R> x = A.q.load(k);
     R o0 = x.rho + R(f.x), o1 = x.mu + R(f.y), o2 = x.mv + R(f.z), o3 = x.e + R(f.w);
     for (int s = 0; s < n; s++) {
@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(TILE_THREADS) anderson_fallback_kernel(const A
   bool bad = false;
   if (anderson_cell(cd, tile, threadIdx.x, &i, &j)) {
     const int64_t k = cd.cell + i + int64_t(j) * cd.ni;
-    const Cons<R> q1 = implicit_update(A.last_x.load(k), A.dq[cd.skew + skew_slot(i, j, cd.nj)], R(cd.gamma));
+    const Cons<R> q1 = implicit_update(A.last_x.load(k), A.dq[k], R(cd.gamma));
     A.q.store(k, q1);
     bad = !is_physical(q1, R(cd.gamma));
   }

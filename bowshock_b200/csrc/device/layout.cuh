@@ -6,8 +6,10 @@
 //   i-faces    float4 (nx, ny, area, 0), (ni + 1) nj at `iface`;
 //   j-faces    float4 (nx, ny, area, 0), ni (nj + 1) at `jface`;
 //   cells      float2 (volume, planar area) at `cell`;
-//   LU-SGS     per-cell sweep records and corrections in diagonal-major
-//              order, (ni + nj - 1) nj slots at `skew` (skew_slot).
+//   LU-SGS     per-cell sweep records, one block per warp of 32 rows in
+//              diagonal-major order (sweep_block_slot), sweep_slots(ni, nj)
+//              slots at `slot`; the final correction dQ is row-major like
+//              the state.
 // Metrics are computed in FP64 on the host and stored as FP32; with the
 // two-float metrics on, also each value's FP32 low part (the FP64 value less
 // the FP32 one), which the residual adds back (about 48 bits). The state is
@@ -38,11 +40,32 @@ constexpr unsigned STATUS_NON_PHYSICAL = 1u;
 // A kernel gave up waiting for an asynchronous copy (bounded wait).
 constexpr unsigned STATUS_TIMEOUT = 2u;
 
-// Slot of cell (i, j) in a case's diagonal-major ("skewed") LU-SGS arrays:
-// anti-diagonal d = i + j, then j, so the cells of consecutive diagonals are
-// one contiguous range.
-__host__ __device__ __forceinline__ int64_t skew_slot(int i, int j, int nj) {
-  return int64_t(i + j) * nj + j;
+// LU-SGS sweep records. The rows of a case are cut into warps of 32 (the
+// last may hold fewer); warp w owns rows 32 w .. 32 w + rows - 1 and a block
+// of records of ni + rows diagonals by rows + 1 record rows, diagonal-major,
+// so that any run of diagonals is one contiguous range that a single bulk
+// copy brings into shared memory. Record row r of block diagonal t holds
+// cell (t - r, 32 w + r - 1) in the forward records (row 0 is a ghost: the
+// previous warp's last row) and cell (t - r, 32 w + r) in the backward
+// records (row `rows` is a ghost: the next warp's first row).
+__host__ __device__ __forceinline__ int sweep_warps(int nj) { return (nj + 31) / 32; }
+__host__ __device__ __forceinline__ int sweep_rows(int nj, int w) {
+  return nj - 32 * w < 32 ? nj - 32 * w : 32;
+}
+// First slot of warp w's block (the warps before it are full).
+__host__ __device__ __forceinline__ int64_t sweep_block_base(int ni, int w) {
+  return int64_t(w) * (ni + 32) * 33;
+}
+// Slot of record row r for column i in warp w's block.
+__host__ __device__ __forceinline__ int64_t sweep_block_slot(int ni, int nj, int w, int i, int r) {
+  const int rows = sweep_rows(nj, w);
+  return sweep_block_base(ni, w) + int64_t(i + r) * (rows + 1) + r;
+}
+// Slots of a case's records.
+__host__ __device__ __forceinline__ int64_t sweep_slots(int ni, int nj) {
+  const int last = sweep_warps(nj) - 1;
+  const int rows = sweep_rows(nj, last);
+  return sweep_block_base(ni, last) + int64_t(ni + rows) * (rows + 1);
 }
 
 struct CaseDev {
@@ -50,7 +73,7 @@ struct CaseDev {
   int64_t cell;   // offset of the case's cell arrays
   int64_t iface;  // offset of its i-face arrays
   int64_t jface;  // offset of its j-face arrays
-  int64_t skew;   // offset of its diagonal-major LU-SGS arrays, (ni + nj - 1) nj slots
+  int64_t slot;   // offset of its LU-SGS sweep records, sweep_slots(ni, nj) slots
   int32_t bc[4];  // bs_bc_kind per side
   int32_t flux, limiter, recon, axisym;
   int32_t integrator, local_dt;

@@ -4,20 +4,25 @@
 //
 // The forward sweep solves (D + L) dQ* = R cell by cell in the order j, then
 // i; cell (i, j) needs only (i - 1, j) and (i, j - 1), both on the previous
-// anti-diagonal i + j = d - 1, so every cell of a diagonal is independent and
-// the sweep is ni + nj - 1 dependent steps. One CTA owns a case; thread j
-// owns grid row j for the whole sweep and walks it along i as d advances:
-//   - its west (forward) / east (backward) neighbour is the cell it finished
-//     on the previous step, held in registers;
-//   - its south / north neighbour is the cell thread j -+ 1 finished on the
-//     previous step: its dQ by warp shuffle (shared memory across a warp
-//     edge), its state and face through double-buffered shared memory;
-//   - its own operands (residual or dQ*, state, (u, v, p, 1/D), faces) come
-//     from the per-cell records that the residual pass wrote diagonal-major,
-//     staged into shared memory by TMA bulk copies a chunk of diagonals at a
-//     time, two chunks in flight.
-// One barrier per diagonal orders the exchange. A step has no branch: every
-// thread computes, and only cells on the grid store.
+// anti-diagonal, so the sweep is ni + nj - 1 dependent steps. One CTA owns a
+// case and thread j owns grid row j; the rows are cut into warps of 32, and
+// the warps run decoupled, with no CTA-wide barrier in the sweeps:
+//   - a warp walks its own rows' cells diagonal by diagonal; the neighbour
+//     along the row is the lane's own previous cell (registers), the
+//     neighbour across rows is the next lane's previous cell: its dQ by warp
+//     shuffle, its state from the records in shared memory;
+//   - at a warp edge the neighbour row belongs to the next warp: its state
+//     is a ghost row of this warp's records (the residual pass writes that
+//     row's records twice), and its dQ arrives through a small ring of
+//     shared-memory slots, one per cell column, that the producing lane
+//     fills and the consuming lane empties (a slot holds a NaN sentinel
+//     while empty, so one 16-byte slot is both the flag and the data);
+//   - each warp stages its own records into shared memory by TMA bulk
+//     copies, a chunk of diagonals at a time, with a ring of chunk buffers
+//     whose mbarriers only that warp waits on.
+// The warps of a case therefore form a pipeline whose rate is one warp's
+// step, not a CTA barrier's. Every wait is bounded: a wait that gives up sets
+// STATUS_TIMEOUT and the kernel drains its copies and leaves.
 //
 // The operator runs in FP32. The neighbour term is the change of the
 // physical flux, F(Q + dQ) - F(Q), exactly as the reference forms it, but
@@ -36,21 +41,32 @@ struct SweepArgs {
   const CaseDev* cases;
   const int* case_list;   // blockIdx.x -> case
   const int* active;      // per case (may be null)
-  const float4* rec;      // sweep records, diagonal-major (5 float4 per slot, pass A)
-  float4* dq;             // diagonal-major: forward result dQ*, then the final dQ
+  const float4* rec_f;    // forward records (sweep_block_slot layout, 5 float4 per slot)
+  float4* rec_b;          // backward records; the forward sweep writes dQ* into field 0
+  float4* dq;             // final dQ, one float4 per cell at the case's cell offset (row-major)
   float* cfl;             // per case current CFL number (ramped after the sweep)
   const float* cfl_max;   // per case
   const float* growth;    // per case
   const float* omega;     // per case
   unsigned* status;       // per case
-  int chunk;              // diagonals per bulk copy
-  int wait_limit;         // mbarrier polls before a wait gives up
+  int chunk;              // diagonals per bulk copy (K)
+  int buffers;            // chunk buffers per warp (NB, 2..kMaxSweepBuffers)
+  int wait_limit;         // polls before a wait gives up
+  int drain_limit;        // polls per copy when draining after a failure
 };
 
-// Fields of the sweep record (five float4 per cell, written by the residual
-// pass): residual; state; (u, v, p, 1/D); west face and south face as
-// (nx, ny, A/2, omega lambda A / 2).
-enum { REC_R = 0, REC_Q = 1, REC_W = 2, REC_FW = 3, REC_FS = 4, REC_SIZE = 5 };
+// Fields of the records (five float4 per slot, written by the residual pass):
+//   forward:  residual | state | (u, v, p, 1/D) | west face | south face
+//   backward: dQ*      | state | (u, v, p, 1/D) | east face | north face
+// with each face as (nx, ny, A/2, omega lambda A / 2).
+enum { REC_R = 0, REC_Q = 1, REC_W = 2, REC_FA = 3, REC_FB = 4, REC_SIZE = 5 };
+
+constexpr int kMaxSweepWarps = 16;    // nj <= 512
+constexpr int kMaxSweepBuffers = 4;
+constexpr int kEdgeRing = 32;         // slots per warp-edge ring (a power of two)
+constexpr unsigned kEdgeEmpty = 0x7f80beefu;  // a NaN no arithmetic produces
+// Header: the warps' chunk mbarriers and the abort word.
+constexpr size_t kSweepHeader = 8 * kMaxSweepWarps * kMaxSweepBuffers + 128;
 
 // ---- TMA bulk copies and mbarriers (sm_90 and later; no multicast) --------
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -102,12 +118,66 @@ __device__ __forceinline__ float approx_rcp(float x) {
   return r;
 }
 
-// Shared memory of the sweep for `nt` threads, `nj` rows and chunks of
-// `chunk` diagonals: a 128-byte header (two mbarriers), the double-buffered
-// exchange (state, (u, v, p, 1/D), dQ, south face) and two chunk buffers of
-// records and of dQ*.
-__host__ __device__ constexpr size_t sweep_smem_bytes(int nt, int nj, int chunk) {
-  return 128 + size_t(nt) * 16 * 8 + 2 * size_t(chunk) * nj * 16 * (REC_SIZE + 1);
+// ---- the warp-edge rings ----------------------------------------------------
+__device__ __forceinline__ uint4 lds_volatile_u4(const float4* p) {
+  uint4 v;
+  asm volatile("ld.volatile.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(smem_u32(p))
+               : "memory");
+  return v;
+}
+__device__ __forceinline__ void sts_volatile_u4(float4* p, uint4 v) {
+  asm volatile("st.volatile.shared.v4.u32 [%0], {%1, %2, %3, %4};\n" ::"r"(smem_u32(p)), "r"(v.x),
+               "r"(v.y), "r"(v.z), "r"(v.w)
+               : "memory");
+}
+__device__ __forceinline__ bool all_empty(uint4 v) {
+  return v.x == kEdgeEmpty && v.y == kEdgeEmpty && v.z == kEdgeEmpty && v.w == kEdgeEmpty;
+}
+__device__ __forceinline__ bool none_empty(uint4 v) {
+  return v.x != kEdgeEmpty && v.y != kEdgeEmpty && v.z != kEdgeEmpty && v.w != kEdgeEmpty;
+}
+__device__ __forceinline__ bool aborted(const int* abort_word) {
+  return *reinterpret_cast<const volatile int*>(abort_word) != 0;
+}
+
+// Puts dQ of cell column i into its slot once the consumer has emptied it.
+// Each of the four words is checked, so a slot is taken only when the
+// consumer's emptying store has landed in full.
+__device__ __forceinline__ bool edge_put(float4* ring, int i, float4 d, int limit, const int* abort_word) {
+  float4* s = ring + (i & (kEdgeRing - 1));
+  for (int k = 0;; k++) {
+    if (all_empty(lds_volatile_u4(s))) break;
+    if (k >= limit || ((k & 63) == 63 && aborted(abort_word))) return false;
+  }
+  sts_volatile_u4(s, make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z),
+                                __float_as_uint(d.w)));
+  return true;
+}
+// Takes dQ of cell column i once all four words of the slot hold it, and
+// empties the slot.
+__device__ __forceinline__ bool edge_get(float4* ring, int i, float4& d, int limit, const int* abort_word) {
+  float4* s = ring + (i & (kEdgeRing - 1));
+  uint4 v;
+  for (int k = 0;; k++) {
+    v = lds_volatile_u4(s);
+    if (none_empty(v)) break;
+    if (k >= limit || ((k & 63) == 63 && aborted(abort_word))) return false;
+  }
+  sts_volatile_u4(s, make_uint4(kEdgeEmpty, kEdgeEmpty, kEdgeEmpty, kEdgeEmpty));
+  d = make_float4(__uint_as_float(v.x), __uint_as_float(v.y), __uint_as_float(v.z), __uint_as_float(v.w));
+  return true;
+}
+
+// Shared memory of the sweep for cases of up to `nj` rows, chunks of `chunk`
+// diagonals and `buffers` chunk buffers per warp: the header, two rings per
+// warp edge and the warps' chunk buffers (a warp of `rows` rows holds
+// rows + 1 record rows per diagonal).
+__host__ __device__ inline size_t sweep_smem_bytes(int nj, int chunk, int buffers) {
+  const int nw = sweep_warps(nj);
+  const size_t rows_sum = size_t(nj) + nw;
+  return kSweepHeader + 2 * size_t(nw - 1) * kEdgeRing * 16 + size_t(buffers) * chunk * rows_sum * 16 * REC_SIZE;
 }
 
 // The d-independent part of a neighbour's term: its state, the face normal
@@ -153,166 +223,204 @@ __device__ __forceinline__ void add_neighbour(float4& sum, const NeighbourTerm& 
   sum.w += t.half_area * ((d.w + dp) * t.un + (t.q.w + d.w + t.p + dp) * dun) - t.damp * d.w;
 }
 
-// The forward and backward sweeps of every active case, one CTA per case,
-// leaving the final correction dQ (diagonal-major) for lusgs_update_kernel.
-static __global__ void __launch_bounds__(512) lusgs_sweep_kernel(const SweepArgs A) {
+__device__ __forceinline__ float4 shfl4_up(float4 v) {
+  return make_float4(__shfl_up_sync(0xffffffffu, v.x, 1), __shfl_up_sync(0xffffffffu, v.y, 1),
+                     __shfl_up_sync(0xffffffffu, v.z, 1), __shfl_up_sync(0xffffffffu, v.w, 1));
+}
+__device__ __forceinline__ float4 shfl4_down(float4 v) {
+  return make_float4(__shfl_down_sync(0xffffffffu, v.x, 1), __shfl_down_sync(0xffffffffu, v.y, 1),
+                     __shfl_down_sync(0xffffffffu, v.z, 1), __shfl_down_sync(0xffffffffu, v.w, 1));
+}
+
+// The forward and backward sweeps of every active case, one CTA per case and
+// one warp per 32 rows, leaving the final correction dQ in A.dq (row-major).
+//
+// Indexing: a warp of `rows` rows owns a block of records of nT = ni + rows
+// diagonals by rows + 1 record rows (sweep_block_slot). Each pass visits the
+// block's diagonals in the order of a pass index u = 0 .. nT - 1 (forward:
+// the block diagonal; backward: nT - 1 less it); step s = 0 .. nT - 2 works on
+// the lane's cell at u = s + 1, whose neighbours are at u = s. Chunk cc of a
+// pass holds u in [cc K, cc K + K); the pass's chunks are numbered on from the
+// previous pass's (g = pass nch + cc) and cycle through the warp's buffers.
+static __global__ void __launch_bounds__(32 * kMaxSweepWarps) lusgs_sweep_kernel(const SweepArgs A) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int c = A.case_list[blockIdx.x];
   if (A.active != nullptr && A.active[c] == 0) return;
   const CaseDev& cd = A.cases[c];
   const int ni = cd.ni, nj = cd.nj;
-  const int nt = blockDim.x;
-  const int j = threadIdx.x;
-  const bool row = j < nj;
+  const int nw = sweep_warps(nj);
+  const int w = threadIdx.x >> 5;
+  const int l = threadIdx.x & 31;
+  const int K = A.chunk, NB = A.buffers;
   const float gm1 = float(cd.gamma) - 1.f;
-  const int ndiag = ni + nj - 1;
-  const int K = A.chunk;
-  const int nchunks = (ndiag + K - 1) / K;
 
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
-  float4* xq = reinterpret_cast<float4*>(smem_raw + 128);  // [2][nt] exchange: state
-  float4* xw = xq + 2 * nt;                                 // (u, v, p, 1/D)
-  float4* xd = xw + 2 * nt;                                 // dQ
-  float4* xf = xd + 2 * nt;                                 // south face
-  float4* ring_rec = xf + 2 * nt;                           // [2][K nj][5]
-  float4* ring_dq = ring_rec + 2 * size_t(K) * nj * REC_SIZE;  // [2][K nj]
-  const float4* rec_case = A.rec + REC_SIZE * cd.skew;
-  float4* dq_case = A.dq + cd.skew;
-  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-
-  if (j == 0) {
-    for (int b = 0; b < 2; b++) mbar_init(&bars[b], 1);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);  // [kMaxSweepWarps][kMaxSweepBuffers]
+  int* abort_word = reinterpret_cast<int*>(smem_raw + 8 * kMaxSweepWarps * kMaxSweepBuffers);
+  float4* rings = reinterpret_cast<float4*>(smem_raw + kSweepHeader);  // [2][nw - 1][kEdgeRing]
+  float4* bufs = rings + 2 * (nw - 1) * kEdgeRing;
+  const int n_ring_words = 2 * (nw - 1) * kEdgeRing;
+  for (int k = threadIdx.x; k < n_ring_words; k += blockDim.x)
+    sts_volatile_u4(rings + k, make_uint4(kEdgeEmpty, kEdgeEmpty, kEdgeEmpty, kEdgeEmpty));
+  if (threadIdx.x == 0) {
+    *abort_word = 0;
+    for (int b = 0; b < kMaxSweepWarps * kMaxSweepBuffers; b++) mbar_init(&bars[b], 1);
     mbar_fence_init();
   }
-  // Benign exchange contents: a slot read for an absent neighbour is
-  // multiplied by a zero dQ and must be finite.
-  for (int k = j; k < 2 * nt; k += nt) {
-    xq[k] = make_float4(1.f, 0.f, 0.f, 1.f);
-    xw[k] = make_float4(0.f, 0.f, 1.f, 1.f);
-    xd[k] = zero;
-    xf[k] = zero;
-  }
   __syncthreads();
+  if (w >= nw) return;
 
-  unsigned uses[2] = {};    // completed phases of each buffer's mbarrier
-  unsigned issued[2] = {};  // copies issued into each buffer
+  const int rows = sweep_rows(nj, w);
+  const int R1 = rows + 1;
+  const int nT = ni + rows;
+  const int nch = (nT + K - 1) / K;
+  const int le = min(l, rows - 1);  // the lane's row for addressing (lanes past the rows idle)
+  uint64_t* full = bars + w * kMaxSweepBuffers;
+  // This warp's chunk buffers: the warps before it hold rows' + 1 rows each.
+  float4* wbuf = bufs + size_t(NB) * K * REC_SIZE * (size_t(32 * w) + w);
+  const size_t buf_stride = size_t(K) * R1 * REC_SIZE;
+  float4* ring_f_in = w > 0 ? rings + (w - 1) * kEdgeRing : nullptr;            // from warp w - 1
+  float4* ring_f_out = w < nw - 1 ? rings + w * kEdgeRing : nullptr;            // to warp w + 1
+  float4* ring_b_in = w < nw - 1 ? rings + (nw - 1 + w) * kEdgeRing : nullptr;  // from warp w + 1
+  float4* ring_b_out = w > 0 ? rings + (nw - 1 + w - 1) * kEdgeRing : nullptr;  // to warp w - 1
+  const int64_t block = cd.slot + sweep_block_base(ni, w);
+
+  // Copies: chunk g of the sequence (forward chunks, then backward ones).
+  auto chunk_span = [&](int cc, int& u0, int& n) {
+    u0 = cc * K;
+    n = min(K, nT - u0);
+  };
+  auto issue = [&](int g) {
+    const int pass = g / nch, cc = g - pass * nch;
+    int u0, n;
+    chunk_span(cc, u0, n);
+    const int t_lo = pass == 0 ? u0 : nT - u0 - n;  // block diagonal of the chunk's first slot row
+    const float4* src = (pass == 0 ? A.rec_f : A.rec_b) + REC_SIZE * (block + int64_t(t_lo) * R1);
+    const unsigned bytes = unsigned(n) * unsigned(R1) * 16u * REC_SIZE;
+    if (l == 0) {
+      uint64_t* bar = &full[g % NB];
+      mbar_arrive_expect_tx(bar, bytes);
+      bulk_load(wbuf + size_t(g % NB) * buf_stride, src, bytes, bar);
+    }
+  };
+  int next = 0;      // next chunk to issue
+  int released = 0;  // chunks whose buffers are free again
+  int waited = 0;    // chunks waited for
+  bool fwd_done = false;
+  auto try_issue = [&]() {
+    while (next < 2 * nch && next < released + NB && (next < nch || fwd_done)) issue(next++);
+  };
   bool failed = false;
+  auto wait_chunk = [&](int g) -> bool {
+    const bool ok = mbar_wait(&full[g % NB], unsigned(g / NB) & 1u, A.wait_limit);
+    if (ok) waited = g + 1;
+    return __all_sync(0xffffffffu, ok);
+  };
+  try_issue();
+
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  const int j = 32 * w + le;
   for (int pass = 0; pass < 2 && !failed; pass++) {
     const bool fwd = pass == 0;
-    // Chunk cc holds the diagonals [dlo, dlo + n) in memory order.
-    auto chunk_range = [&](int cc, int& dlo, int& n) {
-      n = min(K, ndiag - cc * K);
-      dlo = fwd ? cc * K : ndiag - cc * K - n;
+    const float sgn = fwd ? -1.f : 1.f;
+    // Block rows: forward, own row l + 1 and the neighbour below at l (row 0
+    // is the ghost of the previous warp's last row); backward, own row l and
+    // the neighbour above at l + 1 (row `rows` is the ghost of the next
+    // warp's first row).
+    const int r_own = fwd ? le + 1 : le;
+    const int r_nb = fwd ? le : le + 1;
+    // Slot row of pass index u in chunk cc, within its buffer.
+    auto elem = [&](int cc, int u) {
+      int u0, n;
+      chunk_span(cc, u0, n);
+      return fwd ? u - u0 : u0 + n - 1 - u;
     };
-    auto issue = [&](int cc) {  // one thread
-      int dlo, n;
-      chunk_range(cc, dlo, n);
-      const int buf = cc % 2;
-      const unsigned rec_bytes = unsigned(n) * nj * 16u * REC_SIZE;
-      const unsigned dq_bytes = fwd ? 0u : unsigned(n) * nj * 16u;
-      mbar_arrive_expect_tx(&bars[buf], rec_bytes + dq_bytes);
-      bulk_load(ring_rec + size_t(buf) * K * nj * REC_SIZE, rec_case + size_t(REC_SIZE) * dlo * nj,
-                rec_bytes, &bars[buf]);
-      if (!fwd) bulk_load(ring_dq + size_t(buf) * K * nj, dq_case + size_t(dlo) * nj, dq_bytes, &bars[buf]);
-    };
-    if (j == 0) fence_proxy_async();
-    for (int k = 0; k < 2 && k < nchunks; k++) {
-      if (j == 0) issue(k);
-      issued[k]++;
+    auto buf_of = [&](int cc) { return wbuf + size_t((pass * nch + cc) % NB) * buf_stride; };
+    if (!wait_chunk(pass * nch)) {
+      failed = true;
+      break;
     }
-    // The cell this thread finished last step (its neighbour along the row).
-    float4 pq = make_float4(1.f, 0.f, 0.f, 1.f), pw = make_float4(0.f, 0.f, 1.f, 1.f);
-    float4 pd = zero, pfw = zero;
-    for (int cc = 0; cc < nchunks; cc++) {
-      const int buf = cc % 2;
-      const bool ok = mbar_wait(&bars[buf], uses[buf] & 1u, A.wait_limit);
-      if (ok) uses[buf]++;
-      if (__syncthreads_or(!ok)) {
+    // The lane's previous cell (its neighbour along the row): state and dQ.
+    float4 pq = make_float4(1.f, 0.f, 0.f, 1.f), pw = make_float4(0.f, 0.f, 1.f, 1.f), pd = zero;
+    for (int s = 0; s < nT - 1; s++) {
+      const int u = s + 1;
+      const int cc = u / K;
+      const bool new_chunk = u == cc * K;
+      if (new_chunk && !wait_chunk(pass * nch + cc)) {
         failed = true;
         break;
       }
-      int dlo, n;
-      chunk_range(cc, dlo, n);
-      const float4* rb = ring_rec + size_t(buf) * K * nj * REC_SIZE;
-      const float4* db = ring_dq + size_t(buf) * K * nj;
-      for (int t = 0; t < n; t++) {
-        const int step = cc * K + t;
-        const int d = fwd ? step : ndiag - 1 - step;
-        const int i = d - j;
-        // The dQ row j -+ 1 finished on the previous step, inside the warp.
-        float4 sh;
-        sh.x = fwd ? __shfl_up_sync(0xffffffffu, pd.x, 1) : __shfl_down_sync(0xffffffffu, pd.x, 1);
-        sh.y = fwd ? __shfl_up_sync(0xffffffffu, pd.y, 1) : __shfl_down_sync(0xffffffffu, pd.y, 1);
-        sh.z = fwd ? __shfl_up_sync(0xffffffffu, pd.z, 1) : __shfl_down_sync(0xffffffffu, pd.z, 1);
-        sh.w = fwd ? __shfl_up_sync(0xffffffffu, pd.w, 1) : __shfl_down_sync(0xffffffffu, pd.w, 1);
-        const bool lane_edge = (j & 31) == (fwd ? 0 : 31);
-        // Only cells on the grid store; the others compute on records of
-        // their chunk (possibly padding) and discard the result.
-        const bool active = row && i >= 0 && i < ni;
-        {
-          const int local = (d - dlo) * nj + min(j, nj - 1);
-          const float4* r5 = rb + size_t(REC_SIZE) * local;
-          const float4 q = r5[REC_Q], w = r5[REC_W], fw = r5[REC_FW], fs = r5[REC_FS];
-          const float4 base = fwd ? r5[REC_R] : db[local];
-          const bool has_i = fwd ? i > 0 : i < ni - 1;
-          const bool has_j = fwd ? j > 0 : j < nj - 1;
-          const int b = ((step - 1) & 1) * nt + (fwd ? j - 1 : j + 1);
-          const int bb = has_j ? b : (step & 1) * nt + j;  // an in-range slot either way
-          const float4 oq = xq[bb], ow = xw[bb], of = xf[bb];
-          float4 od = zero;
-          if (has_j) od = lane_edge ? xd[bb] : sh;
-          // Forward: this cell's west and south faces, the flux leaving
-          // through -n; backward: the east neighbour's west face and the
-          // north neighbour's south face, through +n.
-          const float sgn = fwd ? -1.f : 1.f;
-          const float4 face_i = fwd ? fw : pfw;
-          const float4 face_j = fwd ? fs : of;
-          float4 sum = zero;
-          const NeighbourTerm ti = neighbour_term(pq, pw, face_i, sgn);
-          const NeighbourTerm tj = neighbour_term(oq, ow, face_j, sgn);
-          add_neighbour(sum, ti, has_i ? pd : zero, gm1);
-          add_neighbour(sum, tj, od, gm1);
-          const float inv_d = w.w;
-          float4 dq;
-          if (fwd) {
-            dq = make_float4((base.x - sum.x) * inv_d, (base.y - sum.y) * inv_d,
-                             (base.z - sum.z) * inv_d, (base.w - sum.w) * inv_d);
-          } else {
-            dq = make_float4(base.x - sum.x * inv_d, base.y - sum.y * inv_d,
-                             base.z - sum.z * inv_d, base.w - sum.w * inv_d);
-          }
-          const int o = (step & 1) * nt + j;
-          if (active) {
-            xq[o] = q;
-            xw[o] = w;
-            xd[o] = dq;
-            xf[o] = fs;
-            dq_case[size_t(d) * nj + j] = dq;
-          }
-          pq = active ? q : pq;
-          pw = active ? w : pw;
-          pd = active ? dq : pd;
-          pfw = active ? fw : pfw;
-        }
-        __syncthreads();
+      const int i = fwd ? s - l : nT - 2 - s - l;
+      const bool active = l < rows && i >= 0 && i < ni;
+      const float4* own = buf_of(cc) + size_t(elem(cc, u) * R1 + r_own) * REC_SIZE;
+      const int ccn = s / K;
+      const float4* nb = buf_of(ccn) + size_t(elem(ccn, s) * R1 + r_nb) * REC_SIZE;
+      const float4 base = own[REC_R], q = own[REC_Q], wv = own[REC_W], fa = own[REC_FA], fb = own[REC_FB];
+      const float4 nq = nb[REC_Q], nwv = nb[REC_W];
+      // dQ of the neighbour across rows, finished by the next lane on the
+      // previous step (or by the next warp, through the ring).
+      float4 dn = fwd ? shfl4_up(pd) : shfl4_down(pd);
+      bool ok = true;
+      if (fwd && l == 0) {
+        dn = zero;
+        if (active && ring_f_in != nullptr) ok = edge_get(ring_f_in, i, dn, A.wait_limit, abort_word);
+      } else if (!fwd && l == 31) {
+        dn = zero;
+        if (active && ring_b_in != nullptr) ok = edge_get(ring_b_in, i, dn, A.wait_limit, abort_word);
       }
-      if (cc + 2 < nchunks) {
-        if (j == 0) issue(cc + 2);
-        issued[buf]++;
+      float4 sum = zero;
+      add_neighbour(sum, neighbour_term(pq, pw, fa, sgn), pd, gm1);
+      add_neighbour(sum, neighbour_term(nq, nwv, fb, sgn), dn, gm1);
+      const float inv_d = wv.w;
+      float4 dq;
+      if (fwd) {
+        dq = make_float4((base.x - sum.x) * inv_d, (base.y - sum.y) * inv_d, (base.z - sum.z) * inv_d,
+                         (base.w - sum.w) * inv_d);
+      } else {
+        dq = make_float4(base.x - sum.x * inv_d, base.y - sum.y * inv_d, base.z - sum.z * inv_d,
+                         base.w - sum.w * inv_d);
+      }
+      if (active) {
+        if (fwd) {
+          A.rec_b[REC_SIZE * (block + int64_t(i + le) * R1 + le) + REC_R] = dq;
+          if (l == 31 && ring_f_out != nullptr) ok = ok && edge_put(ring_f_out, i, dq, A.wait_limit, abort_word);
+        } else {
+          A.dq[cd.cell + i + int64_t(j) * ni] = dq;
+          if (l == 0 && ring_b_out != nullptr) ok = ok && edge_put(ring_b_out, i, dq, A.wait_limit, abort_word);
+        }
+        pq = q;
+        pw = wv;
+        pd = dq;
+      }
+      if (__any_sync(0xffffffffu, !ok)) {
+        failed = true;
+        break;
+      }
+      // The neighbours' diagonal u = s was the last of its chunk: free it.
+      if (new_chunk && cc > 0) {
+        released = pass * nch + cc;
+        try_issue();
       }
     }
-    // dQ* written by this pass is read by the next pass's bulk copies.
-    fence_proxy_async();
-    __syncthreads();
+    if (failed) break;
+    released = pass * nch + nch;
+    if (fwd) {
+      // dQ* written above is read by the backward pass's bulk copies.
+      fence_proxy_async();
+      __syncwarp();
+      fwd_done = true;
+    }
+    try_issue();
   }
   if (failed) {
-    // Let the copies still in flight land (bounded) before leaving.
-    for (int b = 0; b < 2; b++)
-      for (unsigned u = uses[b]; u < issued[b]; u++) mbar_wait(&bars[b], u & 1u, A.wait_limit);
-    if (j == 0) atomicOr(&A.status[c], STATUS_TIMEOUT);
+    if (l == 0) {
+      atomicExch(abort_word, 1);
+      atomicOr(&A.status[c], STATUS_TIMEOUT);
+    }
+    // Let this warp's copies still in flight land (bounded) before leaving.
+    for (int g = waited; g < next; g++) mbar_wait(&full[g % NB], unsigned(g / NB) & 1u, A.drain_limit);
     return;
   }
-  if (j == 0) A.cfl[c] = fminf(A.cfl_max[c], A.cfl[c] * A.growth[c]);
+  if (threadIdx.x == 0) A.cfl[c] = fminf(A.cfl_max[c], A.cfl[c] * A.growth[c]);
 }
 
 // applyImplicitUpdate (src/engine-cpu/euler2d.ts:816-847) for one cell:
@@ -343,6 +451,8 @@ __global__ void __launch_bounds__(TILE_THREADS) lusgs_update_kernel(const CaseDe
   const int2 tile = tiles[blockIdx.x];
   const int c = tile.x;
   if (active != nullptr && active[c] == 0) return;
+  // A sweep that gave up left dQ incomplete: the case keeps its state.
+  if (status[c] & STATUS_TIMEOUT) return;
   const CaseDev& cd = cases[c];
   const int ni = cd.ni, nj = cd.nj;
   const int tiles_i = (ni + TI - 1) / TI;
@@ -352,38 +462,66 @@ __global__ void __launch_bounds__(TILE_THREADS) lusgs_update_kernel(const CaseDe
   if (i < ni && j < nj && int(threadIdx.x) < TI * TJ) {
     const R gamma = R(cd.gamma);
     const int64_t k = cd.cell + i + int64_t(j) * ni;
-    const Cons<R> q1 = implicit_update(q.load(k), dq[cd.skew + skew_slot(i, j, nj)], gamma);
+    const Cons<R> q1 = implicit_update(q.load(k), dq[k], gamma);
     q.store(k, q1);
     bad = !is_physical(q1, gamma);
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&status[c], STATUS_NON_PHYSICAL);
 }
 
-// Diagonals per bulk copy for cases of up to `nj` rows (`nt` threads) when
-// `cases_in_flight` cases sweep at once: the largest (up to 8) that lets
-// the resident cases (up to 8 per SM) share an SM's shared memory, else the
-// largest that fits one CTA; 0 if not even one diagonal does.
-inline int sweep_chunk(int nt, int nj, int cases_in_flight) {
+// Launch shape of the sweep: diagonals per bulk copy and chunk buffers per
+// warp.
+struct SweepShape {
+  int chunk = 0, buffers = 0;
+};
+
+// The shape for cases of up to `nj` rows when `cases_in_flight` cases sweep
+// at once: within the shared memory each CTA may take (the resident cases,
+// up to 8 per SM, share an SM's), the one whose copies run furthest ahead of
+// the diagonal being swept ((buffers - 1) chunk - 1 diagonals), the smaller
+// footprint on a tie; chunks of up to `max_chunk` diagonals.
+inline SweepShape sweep_shape(int nj, int cases_in_flight, int max_chunk = 8) {
   const int per_sm = std::min(8, std::max(1, (cases_in_flight + 147) / 148));
-  for (size_t budget : {size_t(200 * 1024) / per_sm, size_t(200 * 1024)})
-    for (int k = 8; k >= 1; k--)
-      if (sweep_smem_bytes(nt, nj, k) <= budget) return k;
-  return 0;
+  for (size_t budget : {size_t(200 * 1024) / per_sm, size_t(200 * 1024)}) {
+    SweepShape best;
+    int best_lead = -1;
+    size_t best_bytes = 0;
+    for (int nb = 2; nb <= kMaxSweepBuffers; nb++)
+      for (int k = 1; k <= max_chunk; k++) {
+        const size_t bytes = sweep_smem_bytes(nj, k, nb);
+        if (bytes > budget) continue;
+        const int lead = (nb - 1) * k - 1;
+        if (lead > best_lead || (lead == best_lead && bytes < best_bytes)) {
+          best = {k, nb};
+          best_lead = lead;
+          best_bytes = bytes;
+        }
+      }
+    if (best.chunk > 0) return best;
+  }
+  return {};
 }
+
+constexpr int kSweepWaitLimit = 1 << 22;
 
 // `cases_in_flight`: cases of the whole batch sweeping at the same time
 // (other lanes included), which sets the shared memory each CTA may take.
+// `wait_limit` < 0 keeps the default bound.
 inline cudaError_t launch_sweep(SweepArgs A, int n_cases, int max_nj, int cases_in_flight,
-                                cudaStream_t stream) {
-  const int nt = ((max_nj + 31) / 32) * 32;
-  A.chunk = sweep_chunk(nt, max_nj, cases_in_flight);
-  if (A.chunk == 0 || nt > 512) return cudaErrorInvalidConfiguration;
-  A.wait_limit = 1 << 22;
-  const size_t bytes = sweep_smem_bytes(nt, max_nj, A.chunk);
+                                cudaStream_t stream, int wait_limit = -1, int max_chunk = 8) {
+  const int nw = sweep_warps(max_nj);
+  if (nw > kMaxSweepWarps) return cudaErrorInvalidConfiguration;
+  const SweepShape shape = sweep_shape(max_nj, cases_in_flight, max_chunk);
+  if (shape.chunk == 0) return cudaErrorInvalidConfiguration;
+  A.chunk = shape.chunk;
+  A.buffers = shape.buffers;
+  A.wait_limit = wait_limit < 0 ? kSweepWaitLimit : wait_limit;
+  A.drain_limit = kSweepWaitLimit;
+  const size_t bytes = sweep_smem_bytes(max_nj, shape.chunk, shape.buffers);
   const cudaError_t e = cudaFuncSetAttribute(lusgs_sweep_kernel,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
   if (e != cudaSuccess) return e;
-  lusgs_sweep_kernel<<<n_cases, nt, bytes, stream>>>(A);
+  lusgs_sweep_kernel<<<n_cases, 32 * nw, bytes, stream>>>(A);
   return cudaGetLastError();
 }
 

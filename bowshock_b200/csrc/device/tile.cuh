@@ -35,7 +35,8 @@ struct TileArgs {
   unsigned* status;       // per case status bits
   double a, b;            // STAGE coefficients
   int first_stage;        // STAGE: compute the time step from src (== u0)
-  float4* rec;            // PREPARE output: each cell's sweep record (5 float4, skewed)
+  float4* rec_f;          // PREPARE output: each cell's forward sweep record (5 float4)
+  float4* rec_b;          // PREPARE output: its backward record, fields 1-4
   const float* cfl;       // PREPARE: per case current implicit CFL number
   const float* omega;     // PREPARE: per case omega
   double* res_out;        // RESIDUAL: 4 values per cell, arena like the state
@@ -235,12 +236,36 @@ __global__ void __launch_bounds__(TILE_THREADS, kMinBlocks) tile_kernel(const Ti
       const float omega = A.omega[c];
       const float scale = 0.5f * (omega + 1.f / A.cfl[c]);
       const float diag = scale * (lw + le + ls + ln) + (cd.axisym ? cm.y * rad(sj, si, 0.f, 1.f) : 0.f);
-      float4* rec = A.rec + 5 * (cd.skew + skew_slot(i, j, nj));
-      rec[0] = make_float4(float(res[0]), float(res[1]), float(res[2]), float(res[3]));
-      rec[1] = make_float4(float(qs.rho), float(qs.mu), float(qs.mv), float(qs.e));
-      rec[2] = make_float4(float(W[1][sj][si]), float(W[2][sj][si]), float(W[3][sj][si]), 1.f / diag);
-      rec[3] = make_float4(fw.x, fw.y, 0.5f * fw.z, 0.5f * omega * lw);
-      rec[4] = make_float4(fs.x, fs.y, 0.5f * fs.z, 0.5f * omega * ls);
+      const float4 st = make_float4(float(qs.rho), float(qs.mu), float(qs.mv), float(qs.e));
+      const float4 wv = make_float4(float(W[1][sj][si]), float(W[2][sj][si]), float(W[3][sj][si]), 1.f / diag);
+      // The records of the warp of 32 rows that sweeps row j (sweep_block_slot):
+      // forward at record row j % 32 + 1, backward at j % 32.
+      const int w = j >> 5, l = j & 31;
+      const int64_t base = cd.slot;
+      float4* rf = A.rec_f + 5 * (base + sweep_block_slot(ni, nj, w, i, l + 1));
+      rf[0] = make_float4(float(res[0]), float(res[1]), float(res[2]), float(res[3]));
+      rf[1] = st;
+      rf[2] = wv;
+      rf[3] = make_float4(fw.x, fw.y, 0.5f * fw.z, 0.5f * omega * lw);
+      rf[4] = make_float4(fs.x, fs.y, 0.5f * fs.z, 0.5f * omega * ls);
+      float4* rb = A.rec_b + 5 * (base + sweep_block_slot(ni, nj, w, i, l));
+      rb[1] = st;
+      rb[2] = wv;
+      rb[3] = make_float4(fe.x, fe.y, 0.5f * fe.z, 0.5f * omega * le);
+      rb[4] = make_float4(fn.x, fn.y, 0.5f * fn.z, 0.5f * omega * ln);
+      // Ghost rows: the state of the neighbour row that belongs to the next
+      // (forward) or previous (backward) warp. Row 0 and the last row have
+      // no such neighbour; their ghost holds the cell's own state, which a
+      // zero correction turns into an exactly zero term.
+      auto put_ghost = [&](float4* rec, int wg, int r) {
+        float4* gr = rec + 5 * (base + sweep_block_slot(ni, nj, wg, i, r));
+        gr[1] = st;
+        gr[2] = wv;
+      };
+      if (l == 31 && j + 1 < nj) put_ghost(A.rec_f, w + 1, 0);
+      if (j == 0) put_ghost(A.rec_f, 0, 0);
+      if (l == 0 && j > 0) put_ghost(A.rec_b, w - 1, 32);
+      if (j == nj - 1) put_ghost(A.rec_b, w, sweep_rows(nj, w));
     } else if (A.res_out != nullptr) {
       double* o = A.res_out + 4 * k;
       o[0] = double(res[0]);

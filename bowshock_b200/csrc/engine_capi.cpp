@@ -263,6 +263,10 @@ bs_status bs_engine_set_anderson(bs_engine* engine, int32_t depth, int32_t plain
   BS_ENGINE_CALL(engine, { return engine->solver->set_anderson(depth, plain_steps); });
 }
 
+bs_status bs_engine_set_sweep_wait_limit(bs_engine* engine, int32_t polls) {
+  BS_ENGINE_CALL(engine, { return engine->solver->set_sweep_wait_limit(polls); });
+}
+
 }  // extern "C"
 
 // ---- batches ---------------------------------------------------------------
@@ -390,6 +394,10 @@ bs_status bs_batch_set_anderson(bs_batch* batch, int32_t depth, int32_t plain_st
 
 bs_status bs_batch_set_metric_precision(bs_batch* batch, int32_t bits) {
   BS_BATCH_CALL(batch, { return batch->solver->set_metric_precision(bits); });
+}
+
+bs_status bs_batch_set_sweep_wait_limit(bs_batch* batch, int32_t polls) {
+  BS_BATCH_CALL(batch, { return batch->solver->set_sweep_wait_limit(polls); });
 }
 
 bs_status bs_batch_anderson_restarts(bs_batch* batch, int32_t* restarts) {

@@ -151,7 +151,7 @@ class Solver final : public SolverBase {
     }
     std::vector<bsd::CaseDev> hc(n_);
     std::vector<int2> tiles;
-    int64_t cell = 0, ifc = 0, jfc = 0, bfc = 0, skw = 0;
+    int64_t cell = 0, ifc = 0, jfc = 0, bfc = 0, slots = 0;
     boundary_off_.resize(n_);
     cell_off_.resize(n_);
     for (int c = 0; c < n_; c++) {
@@ -164,9 +164,9 @@ class Solver final : public SolverBase {
       d.cell = cell;
       d.iface = ifc;
       d.jface = jfc;
-      d.skew = skw;
+      d.slot = slots;
       d.tile_base = int64_t(tiles.size());
-      skw += int64_t(cfg.ni + cfg.nj - 1) * cfg.nj;
+      slots += bsd::sweep_slots(cfg.ni, cfg.nj);
       for (int s = 0; s < 4; s++) d.bc[s] = cfg.boundaries[s].kind;
       d.flux = cfg.flux;
       d.limiter = cfg.limiter;
@@ -200,7 +200,7 @@ class Solver final : public SolverBase {
       max_along_ = std::max(max_along_, std::max(cfg.ni, cfg.nj));
     }
     total_cells_ = cell;
-    total_skew_ = skw;
+    total_slots_ = slots;
     n_tiles_ = int(tiles.size());
     steps_.assign(n_, 0);
     active_h_.assign(n_, 1);
@@ -787,6 +787,18 @@ class Solver final : public SolverBase {
     return BS_OK;
   }
 
+  bs_status set_sweep_wait_limit(int polls) override {
+    if (polls < -1) return fail(BS_INVALID_ARGUMENT, "the wait limit is -1 (default) or a number of polls");
+    if (polls == sweep_wait_limit_) return BS_OK;
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    sweep_wait_limit_ = polls;
+    // Captured graphs hold the old limit.
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+    graph_launches_.clear();
+    return BS_OK;
+  }
+
   bs_status anderson_restarts(int* out) override {
     if (ac_.p == nullptr) {
       for (int c = 0; c < n_; c++) out[c] = 0;
@@ -836,6 +848,9 @@ class Solver final : public SolverBase {
     int done = 0;
     for (int c = 0; c < n_; c++) done += active_h_[c] == 0;
     int64_t step = 0;
+    std::vector<double> rf(n_);
+    bool any_timeout = false;
+    for (;;) {
     while (done < n_ && step < max_steps) {
       const int chunk = int(std::min<int64_t>(check_every, max_steps - step));
       BS_CUDA(cudaMemsetAsync(norm_.p, 0, n_ * sizeof(double), stream_));
@@ -859,7 +874,13 @@ class Solver final : public SolverBase {
         // The residual of the state at the start of the chunk's last step.
         const double r = std::sqrt(sums[c] / (double(cases_[c].cfg.ni) * cases_[c].cfg.nj));
         results[c].residual = r;
-        if (status[c] & bsd::STATUS_NON_PHYSICAL) {
+        if (status[c] & bsd::STATUS_TIMEOUT) {
+          // A sweep gave up waiting for its records: the case keeps the
+          // state of its last complete step and stops.
+          results[c].status = BS_EXECUTION;
+          active_h_[c] = 0;
+          any_timeout = true;
+        } else if (status[c] & bsd::STATUS_NON_PHYSICAL) {
           results[c].status = BS_NON_PHYSICAL;
           active_h_[c] = 0;
         } else if (!(r == r)) {
@@ -876,11 +897,29 @@ class Solver final : public SolverBase {
       }
       if (changed) BS_TRY(upload_active());
     }
-    // The exact residual of each final state.
+    // The exact residual of each final state. The check above reads the
+    // residual of the state at the start of a chunk's last step; a case it
+    // passed whose returned state still misses the target marches on.
+    BS_TRY(residual_norms(rf.data()));
+    bool again = false;
+    for (int c = 0; c < n_; c++)
+      if (results[c].status == BS_OK && !(rf[c] <= target[c]) && step < max_steps) {
+        results[c].status = BS_NOT_CONVERGED;
+        active_h_[c] = 1;
+        done--;
+        again = true;
+      }
+    if (!again) break;
+    BS_TRY(upload_active());
+    }
     for (int c = 0; c < n_; c++) active_h_[c] = 1;
     BS_TRY(upload_active());
-    std::vector<double> rf(n_);
-    BS_TRY(residual_norms(rf.data()));
+    if (any_timeout) {
+      std::vector<unsigned> st(n_);
+      BS_CUDA(cudaMemcpyAsync(st.data(), status_.p, n_ * sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+      BS_CUDA(cudaStreamSynchronize(stream_));
+      BS_TRY(clear_timeouts(st));
+    }
     BS_CUDA(cudaEventRecord(ev1_, stream_));
     BS_CUDA(cudaEventSynchronize(ev1_));
     float ms = 0;
@@ -890,7 +929,7 @@ class Solver final : public SolverBase {
     for (int c = 0; c < n_; c++) {
       results[c].steps = taken[c];
       results[c].residual = rf[c];
-      if (results[c].status == BS_OK && !(rf[c] <= target[c] * 1.5)) results[c].status = BS_NOT_CONVERGED;
+      if (results[c].status == BS_OK && !(rf[c] <= target[c])) results[c].status = BS_NOT_CONVERGED;
     }
     return BS_OK;
   }
@@ -931,9 +970,10 @@ class Solver final : public SolverBase {
   }
 
   bs_status ensure_implicit() {
-    if (rec_.p != nullptr) return BS_OK;
-    BS_CUDA(rec_.alloc(5 * size_t(total_skew_)));
-    BS_CUDA(dq_.alloc(total_skew_));
+    if (rec_f_.p != nullptr) return BS_OK;
+    BS_CUDA(rec_f_.alloc(5 * size_t(total_slots_)));
+    BS_CUDA(rec_b_.alloc(5 * size_t(total_slots_)));
+    BS_CUDA(dq_.alloc(total_cells_));
     return BS_OK;
   }
 
@@ -988,10 +1028,24 @@ class Solver final : public SolverBase {
     return BS_OK;
   }
 
+  // Clears the timeout bits of the status words `st` read from the device.
+  bs_status clear_timeouts(std::vector<unsigned>& st) {
+    for (auto& v : st) v &= ~bsd::STATUS_TIMEOUT;
+    BS_CUDA(cudaMemcpyAsync(status_.p, st.data(), n_ * sizeof(unsigned), cudaMemcpyHostToDevice, stream_));
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    return BS_OK;
+  }
+
   bs_status check_status() {
     std::vector<unsigned> st(n_);
     BS_CUDA(cudaMemcpyAsync(st.data(), status_.p, n_ * sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
     BS_CUDA(cudaStreamSynchronize(stream_));
+    for (int c = 0; c < n_; c++)
+      if (st[c] & bsd::STATUS_TIMEOUT) {
+        BS_TRY(clear_timeouts(st));
+        return fail(BS_EXECUTION, "the LU-SGS sweep of case " + std::to_string(c) +
+                                      " gave up waiting for its records; the step was not applied in full");
+      }
     for (int c = 0; c < n_; c++)
       if (st[c] & bsd::STATUS_NON_PHYSICAL)
         return fail(BS_NON_PHYSICAL, "the GPU solution of case " + std::to_string(c) +
@@ -1029,7 +1083,8 @@ class Solver final : public SolverBase {
     A.a = a;
     A.b = b;
     A.first_stage = first ? 1 : 0;
-    A.rec = rec_.p;
+    A.rec_f = rec_f_.p;
+    A.rec_b = rec_b_.p;
     A.cfl = cfl_.p;
     A.omega = omega_.p;
     A.res_out = res_out;
@@ -1136,14 +1191,15 @@ class Solver final : public SolverBase {
     S.cases = d_cases_.p;
     S.case_list = lane.case_list;
     S.active = d_active_.p;
-    S.rec = rec_.p;
+    S.rec_f = rec_f_.p;
+    S.rec_b = rec_b_.p;
     S.dq = dq_.p;
     S.cfl = cfl_.p;
     S.cfl_max = cflmax_.p;
     S.growth = growth_.p;
     S.omega = omega_.p;
     S.status = status_.p;
-    BS_CUDA(bsd::launch_sweep(S, lane.n_cases, lane.max_nj, n_, lane.stream));
+    BS_CUDA(bsd::launch_sweep(S, lane.n_cases, lane.max_nj, n_, lane.stream, sweep_wait_limit_));
     launches_++;
     return BS_OK;
   }
@@ -1278,7 +1334,7 @@ class Solver final : public SolverBase {
   std::vector<HostCase> cases_;
   int n_ = 0;
   int64_t total_cells_ = 0;
-  int64_t total_skew_ = 0;
+  int64_t total_slots_ = 0;
   int n_tiles_ = 0;
   int max_nj_ = 0, max_along_ = 0;
   bool any_global_dt_ = false;
@@ -1290,7 +1346,7 @@ class Solver final : public SolverBase {
   DevBuf<int> d_case_list_, d_active_;
   DevBuf<R> q_[4], s1_[4], s2_[4];
   DevBuf<float> dt_, cfl_, cflmax_, growth_, omega_;
-  DevBuf<float4> iface_, jface_, rec_, dq_;
+  DevBuf<float4> iface_, jface_, rec_f_, rec_b_, dq_;
   DevBuf<float2> cellm_;
   // The two-float metrics' low parts, allocated when first switched on.
   DevBuf<float4> iface_lo_, jface_lo_;
@@ -1317,6 +1373,7 @@ class Solver final : public SolverBase {
   std::map<GraphKey, cudaGraphExec_t> graphs_;
   std::map<GraphKey, int64_t> graph_launches_;
   int64_t launches_ = 0;
+  int sweep_wait_limit_ = -1;
   double last_solve_ms_ = 0;
   int64_t last_solve_launches_ = 0;
   // Anderson acceleration: settings and its per-case history.

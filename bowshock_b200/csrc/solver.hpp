@@ -88,6 +88,9 @@ class SolverBase {
   virtual bs_status set_anderson(int depth, int plain_steps) = 0;
   // Per case, the times the last solve's acceleration forgot its history.
   virtual bs_status anderson_restarts(int* out) = 0;
+  // Polls each bounded wait of later LU-SGS sweeps makes before it gives up
+  // (-1: the default bound); the drain after a give-up keeps the default.
+  virtual bs_status set_sweep_wait_limit(int polls) = 0;
 };
 
 // precision: 64 (FP64 state and residual, FP32 LU-SGS operator) or 32 (all FP32).

@@ -12,10 +12,19 @@
 // library reserves on every GPU that loads it, for as long as the process runs.
 //
 // Limits and sharing: at most kStaticMaxCells cells (ni nj), kStaticMaxSlots
-// diagonal slots ((ni + nj - 1) nj) and 512 cells across (nj). Every call uses the same array, which keeps the last
-// call's contents; the per-call words that must start at zero are cleared by
-// each call. Calls whose work overlaps on the GPU (from several threads, or on
-// several streams of one device) race on the array; the caller must order them.
+// sweep-record slots (bsd::sweep_slots(ni, nj), a little over ni nj plus 33
+// per row: 128 x 512 needs 84,480 and is refused) and 512 cells across (nj).
+// Every call uses the same array, which keeps the last call's contents; the
+// per-call words that must start at zero are cleared by each call. Calls
+// whose work overlaps on the GPU (from several threads, or on several streams
+// of one device) race on the array; the caller must order them.
+//
+// Each call waits for its stream (it reads back the residual and the status),
+// so it must not be called while that stream is being captured into a graph.
+// The device address of the array is looked up once per device, by the first
+// call made on it with that device current; after cudaDeviceReset (or any
+// teardown of the device's primary context) that address is stale and the
+// entry point must not be used again in the process.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -31,8 +40,8 @@
 namespace {
 
 constexpr int64_t kStaticMaxCells = 65536;
-// Diagonal-major slots, (ni + nj - 1) nj, of the LU-SGS records.
-constexpr int64_t kStaticMaxSlots = 98304;
+// Slots of the LU-SGS sweep records (bsd::sweep_slots).
+constexpr int64_t kStaticMaxSlots = 81920;
 constexpr int kStaticMaxTiles = 4096;
 constexpr int kMaxDevices = 64;
 
@@ -42,11 +51,12 @@ constexpr size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign;
 constexpr size_t kOffCase = 0;
 constexpr size_t kOffTiles = kOffCase + align_up(sizeof(bsd::CaseDev));
 constexpr size_t kOffWords = kOffTiles + align_up(sizeof(int2) * kStaticMaxTiles);
-constexpr size_t kOffRec = kOffWords + kAlign;
-constexpr size_t kOffDq = kOffRec + align_up(5 * sizeof(float4) * kStaticMaxSlots);
-constexpr size_t kStaticBytes = kOffDq + align_up(sizeof(float4) * kStaticMaxSlots);
+constexpr size_t kOffRecF = kOffWords + kAlign;
+constexpr size_t kOffRecB = kOffRecF + align_up(5 * sizeof(float4) * kStaticMaxSlots);
+constexpr size_t kOffDq = kOffRecB + align_up(5 * sizeof(float4) * kStaticMaxSlots);
+constexpr size_t kStaticBytes = kOffDq + align_up(sizeof(float4) * kStaticMaxCells);
 
-// The scratch: about 9.5 MB on every device that loads the library.
+// The scratch: about 14.2 MB on every device that loads the library.
 static __device__ __align__(256) unsigned char g_step_scratch[kStaticBytes];
 
 // The per-case words inside the kOffWords region.
@@ -116,11 +126,11 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
                     "the grid has " + std::to_string(n_cells) +
                         " cells; the allocation-free step takes at most " +
                         std::to_string(kStaticMaxCells));
-  const int64_t n_slots = int64_t(ni + nj - 1) * nj;
+  const int64_t n_slots = bsd::sweep_slots(ni, nj);
   if (n_slots > kStaticMaxSlots)
     return bs::fail(BS_INVALID_ARGUMENT,
                     "the grid needs " + std::to_string(n_slots) +
-                        " diagonal slots ((ni + nj - 1) nj); the allocation-free step takes at most " +
+                        " sweep-record slots; the allocation-free step takes at most " +
                         std::to_string(kStaticMaxSlots));
   const int n_tiles = ((ni + bsd::TI - 1) / bsd::TI) * ((nj + bsd::TJ - 1) / bsd::TJ);
   if (n_tiles > kStaticMaxTiles)
@@ -141,7 +151,7 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
   cd.cell = 0;
   cd.iface = 0;
   cd.jface = 0;
-  cd.skew = 0;
+  cd.slot = 0;
   for (int k = 0; k < 4; k++) cd.bc[k] = config->boundaries[k].kind;
   cd.flux = config->flux;
   cd.limiter = config->limiter;
@@ -165,7 +175,8 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
   auto* d_case = reinterpret_cast<bsd::CaseDev*>(base + kOffCase);
   auto* d_tiles = reinterpret_cast<int2*>(base + kOffTiles);
   auto* d_words = reinterpret_cast<Words*>(base + kOffWords);
-  auto* d_rec = reinterpret_cast<float4*>(base + kOffRec);
+  auto* d_rec_f = reinterpret_cast<float4*>(base + kOffRecF);
+  auto* d_rec_b = reinterpret_cast<float4*>(base + kOffRecB);
   auto* d_dq = reinterpret_cast<float4*>(base + kOffDq);
 
   cudaError_t err = cudaMemcpyAsync(d_case, &cd, sizeof(cd), cudaMemcpyHostToDevice, st);
@@ -189,7 +200,8 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
     A.status = &d_words->status;
     A.a = 0;
     A.b = 1;
-    A.rec = d_rec;
+    A.rec_f = d_rec_f;
+    A.rec_b = d_rec_b;
     A.cfl = &d_words->cfl;
     A.omega = &d_words->omega;
     bsd::tile_kernel<double, bsd::MODE_PREPARE><<<n_tiles, bsd::TILE_THREADS, 0, st>>>(A);
@@ -199,7 +211,8 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
     bsd::SweepArgs S{};
     S.cases = d_case;
     S.case_list = &d_words->case_list;
-    S.rec = d_rec;
+    S.rec_f = d_rec_f;
+    S.rec_b = d_rec_b;
     S.dq = d_dq;
     S.cfl = &d_words->cfl;
     S.cfl_max = &d_words->cfl_max;
@@ -224,6 +237,10 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
     cudaGetLastError();
     return bs::fail(BS_EXECUTION, std::string("allocation-free LU-SGS step: ") + cudaGetErrorString(err));
   }
+  if (status & bsd::STATUS_TIMEOUT)
+    return bs::fail(BS_EXECUTION,
+                    "allocation-free LU-SGS step: the sweep gave up waiting for its records; "
+                    "the state was left as it was before the step");
   *residual = std::sqrt(norm / double(n_cells));
   *non_physical = (status & bsd::STATUS_NON_PHYSICAL) ? 1 : 0;
   return BS_OK;

@@ -192,6 +192,12 @@ class CudaEuler2D:
         low parts, as the reference's two-float engine); 32: FP32 metrics."""
         self._call("bs_engine_set_metric_precision", int(bits))
 
+    def set_sweep_wait_limit(self, polls: int) -> None:
+        """Polls each bounded wait of later LU-SGS sweeps makes before it
+        gives up (-1: the default bound). A sweep that gives up leaves the
+        state as it was and the call raises BS_EXECUTION; for tests."""
+        self._call("bs_engine_set_sweep_wait_limit", int(polls))
+
     def anderson_restarts(self) -> int:
         """The times the acceleration forgot its history since its last reset."""
         r = C.c_int32()

@@ -16,18 +16,27 @@ from .warmstart import warm_solve
 from .workloads import Case, NoseCase, make_cases
 
 # Device bytes per cell of a case in an FP64 LU-SGS batch: state 4 x 8,
-# time step 4, cell metrics 8, and the i- and j-face metrics 16 each (one
-# face of each per cell, the extra row and column counted separately);
-# sweep records 5 x 16 and corrections 16 per diagonal-major slot, of which
-# a case has (ni + nj - 1) nj.
-CELL_BYTES = 32 + 4 + 8 + 16 + 16
-SLOT_BYTES = 96
+# time step 4, cell metrics 8, the i- and j-face metrics 16 each (one face
+# of each per cell, the extra row and column counted separately) and the
+# correction dQ 16; forward and backward sweep records 5 x 16 each per slot,
+# of which a case has sweep_slots(ni, nj).
+CELL_BYTES = 32 + 4 + 8 + 16 + 16 + 16
+SLOT_BYTES = 160
+
+
+def sweep_slots(ni: int, nj: int) -> int:
+    """Record slots of a case: per warp of 32 rows (the last may hold
+    fewer) a block of ni + rows diagonals by rows + 1 record rows, as the
+    device layout (sweep_slots in device/layout.cuh)."""
+    nw = (nj + 31) // 32
+    rows = nj - 32 * (nw - 1)
+    return (nw - 1) * (ni + 32) * 33 + (ni + rows) * (rows + 1)
 
 
 def case_device_bytes(ni: int, nj: int) -> int:
     """Device memory one case takes in an FP64 LU-SGS batch (the network's
     buffers and the batch's per-case words aside)."""
-    return ni * nj * CELL_BYTES + (ni + nj) * 16 + (ni + nj - 1) * nj * SLOT_BYTES + 64 * (ni + nj)
+    return ni * nj * CELL_BYTES + (ni + nj) * 16 + sweep_slots(ni, nj) * SLOT_BYTES + 64 * (ni + nj)
 
 
 def plan_waves(specs: list[NoseCase], budget_bytes: int, order: list[int] | None = None) -> list[list[int]]:

@@ -293,6 +293,15 @@ BS_API bs_status bs_engine_anderson_restarts(bs_engine *engine, int32_t *restart
  * memory and of residual traffic. Engines of precision 32 refuse 64. */
 BS_API bs_status bs_engine_set_metric_precision(bs_engine *engine, int32_t bits);
 
+/* Polls each bounded wait of the engine's later LU-SGS sweeps makes before it
+ * gives up (-1 restores the default of 2^22; 0 makes the first wait give up
+ * at once). A sweep that gives up drains its copies in flight under the
+ * default bound, leaves the case's state as it was before the step, and the
+ * call that ran it returns BS_EXECUTION; the engine stays usable. For tests
+ * of that path; the reference detects a GPU step that did not complete by
+ * its step ledger instead (src/engine-gpu/time-loop.ts:125-150). */
+BS_API bs_status bs_engine_set_sweep_wait_limit(bs_engine *engine, int32_t polls);
+
 /* ---- an LU-SGS step that allocates nothing -------------------------------- */
 
 /* One LU-SGS step (residual and diagonal pass, forward and backward wavefront
@@ -302,13 +311,18 @@ BS_API bs_status bs_engine_set_metric_precision(bs_engine *engine, int32_t bits)
  * that hand out all GPU memory from their own pool (cudaMalloc would bypass
  * their budget, and cudaMalloc/cudaFree synchronise the device) and solver
  * loops that must not allocate once running. All scratch lives in one static
- * device array of the library, reserved on every GPU that loads it until the
- * process exits: at most 65536 cells (ni nj), 512 cells across (nj) and
- * 98304 diagonal-major record slots ((ni + nj - 1) nj); larger grids return
- * BS_INVALID_ARGUMENT. The first call on a device looks up
- * the array's device address with that device current; make that first call
- * before any stream capture. Every call shares the array, so calls that
- * overlap on the GPU race: order them. Device inputs (layout as the engine's,
+ * device array of the library (about 14.2 MB), reserved on every GPU that
+ * loads it until the process exits: at most 65536 cells (ni nj), 512 cells
+ * across (nj) and 81920 sweep-record slots (33 (ni + 32) per 32 rows, the
+ * last warp's rows r taking (ni + r)(r + 1): 256 x 256 needs 76032,
+ * 128 x 512 needs 84480); larger grids return BS_INVALID_ARGUMENT. The first
+ * call on a device looks up the array's device address with that device
+ * current; after cudaDeviceReset that address is stale and the entry point
+ * must not be called again in the process. Each call waits for `stream` (it
+ * reads back the residual and the status), so no call may be made while that
+ * stream is being captured. Every call shares the array, so calls that
+ * overlap on the GPU race: order them. A sweep that gives up waiting for its
+ * records returns BS_EXECUTION and leaves the state as it was. Device inputs (layout as the engine's,
  * device/layout.cuh): iface (ni + 1) nj float4 (nx, ny, area, 0), jface
  * ni (nj + 1) float4, cells ni nj float2 (volume, planar area); the state as
  * four FP64 arrays of ni nj, updated in place. `stream` is a cudaStream_t
@@ -378,6 +392,9 @@ BS_API bs_status bs_batch_solve(bs_batch *batch, int32_t method, double cfl, dou
 BS_API bs_status bs_batch_set_anderson(bs_batch *batch, int32_t depth, int32_t plain_steps);
 /* As bs_engine_set_metric_precision, for every case of the batch. */
 BS_API bs_status bs_batch_set_metric_precision(bs_batch *batch, int32_t bits);
+/* As bs_engine_set_sweep_wait_limit, for the batch's later LU-SGS sweeps; a
+ * solve reports a case whose sweep gave up as BS_EXECUTION in its result. */
+BS_API bs_status bs_batch_set_sweep_wait_limit(bs_batch *batch, int32_t polls);
 /* Per case, the times the last solve's acceleration forgot its history. */
 BS_API bs_status bs_batch_anderson_restarts(bs_batch *batch, int32_t *restarts);
 

@@ -2,7 +2,7 @@
 waves it plans within a device-memory budget."""
 from __future__ import annotations
 
-from bowshock_b200.stream import by_grid_size, case_device_bytes, plan_waves
+from bowshock_b200.stream import sweep_slots, by_grid_size, case_device_bytes, plan_waves
 from bowshock_b200.workloads import STREAM_MACHS, stream_specs
 
 
@@ -38,11 +38,14 @@ def test_a_case_larger_than_the_budget_is_a_wave_of_its_own():
     assert waves == [[k] for k in range(len(specs))]
 
 
-def test_device_bytes_grow_with_the_diagonal_slots():
-    # 80 x 40: 3,200 cells and 119 x 40 diagonal-major slots.
+def test_device_bytes_grow_with_the_sweep_record_slots():
+    # 80 x 40: 3,200 cells; rows 0-31 a block of 112 x 33 slots, rows 32-39 one of 88 x 9.
+    assert sweep_slots(80, 40) == 112 * 33 + 88 * 9
+    assert sweep_slots(160, 80) == 2 * 192 * 33 + 176 * 17
+    assert sweep_slots(40, 32) == 72 * 33
     b = case_device_bytes(80, 40)
-    assert b == 3200 * 76 + 120 * 16 + 119 * 40 * 96 + 64 * 120
-    assert case_device_bytes(640, 320) > 60 * b
+    assert b == 3200 * 92 + 120 * 16 + (112 * 33 + 88 * 9) * 160 + 64 * 120
+    assert case_device_bytes(640, 320) > 50 * b
 
 
 def test_waves_by_grid_size_hold_one_size_where_the_budget_allows():
