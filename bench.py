@@ -184,6 +184,57 @@ def run_reference(args, world, rank) -> None:
     print(json.dumps(line), flush=True)
 
 
+TRAIN_MACHS = 48  # seeded Mach numbers of the drag-curve body that train the warm start
+
+
+def warm_start_target(cases) -> dict:
+    """The north-star comparison on the drag curve: the warm-started batch
+    against the plain cold-started single-case GPU path.
+
+    Setup, untimed: the drag curve's body at TRAIN_MACHS seeded Mach numbers
+    (SplitMix64 seeds 1.., uniform in [1.5, 3.0]) is solved cold in one
+    batch at 160 x 80, and the 5 x 256 network trains (3,000 Adam steps) on
+    4,096 random cells of each converged field. Timed, on the 16 cases:
+    (a) each case alone from the free stream, one after another - the device
+    time of each solve; (b) the 16 cases in one batch from the network's
+    fields - device time plus the prediction's wall time, a case whose warm
+    start fails solved again from the free stream (its time added)."""
+    from bowshock_b200.warmstart import solve_cases, train_on_solves, warm_solve
+    from bowshock_b200.workloads import SplitMix64, ogive_case
+
+    machs = [SplitMix64(s).uniform(1.5, 3.0) for s in range(1, TRAIN_MACHS + 1)]
+    tr = train_on_solves([ogive_case(m) for m in machs], cells_per_case=4096, train_steps=3000,
+                         max_steps=MAX_STEPS)
+    single_ms, single_steps = [], []
+    for c in cases:
+        r = solve_cases([c], max_steps=MAX_STEPS)
+        assert r.status[0] == 0, c.name
+        single_ms.append(r.device_ms)
+        single_steps.append(r.steps[0])
+    warm, fell_back = warm_solve(tr.net, cases, max_steps=MAX_STEPS)
+    tr.net.destroy()
+    n = len(cases)
+    cold_rate = n / (sum(single_ms) / 1000)
+    warm_s = warm.device_ms / 1000 + warm.predict_s
+    warm_rate = sum(1 for s in warm.status if s == 0) / warm_s
+    return {
+        "single_cold_solves_per_s": cold_rate,
+        "warm_batch_solves_per_s": warm_rate,
+        "ratio": warm_rate / cold_rate,
+        "target_ratio": 5.0,
+        "fell_back": len(fell_back),
+        "fell_back_fraction": len(fell_back) / n,
+        "converged": sum(1 for s in warm.status if s == 0),
+        "single_cold_steps_median": int(statistics.median(single_steps)),
+        "warm_steps_median": int(statistics.median(warm.steps)),
+        "warm_device_ms": warm.device_ms, "predict_s": warm.predict_s,
+        "single_cold_device_ms": sum(single_ms),
+        "train": {"cases": len(machs), "converged": tr.solved, "samples": tr.samples,
+                  "adam_steps": tr.steps, "seconds": tr.seconds, "loss_last": tr.loss_last},
+        "drags": warm.drags,
+    }
+
+
 def run_gpu(args, world, rank, local) -> None:
     import torch
     import torch.distributed as dist
@@ -267,6 +318,9 @@ def run_gpu(args, world, rank, local) -> None:
     e2e_total = max_over_ranks(sum(e2e_times), world, f"cuda:{local}")
     e2e_value = job_solves_per_s(world, n, args.steps, 1000 * e2e_total)
 
+    # Rank 0 alone (no collective follows before its line is printed).
+    target = warm_start_target(cases) if rank == 0 and not args.no_target else None
+
     # Roofline of the dominant kernel, timed with CUDA events on the
     # library's stream over the same solve from the free stream.
     batch.set_free_stream()
@@ -305,11 +359,17 @@ def run_gpu(args, world, rank, local) -> None:
                    "sample": f"the full 16-case sweep once ({sum(cpu_steps)} LU-SGS steps), one "
                              "case per host thread (C++ FP64 restatement of the reference engine)"}
             cd_err = max(abs(a / b - 1) for a, b in zip(drags, cpu_drags))
+            if target is not None:
+                target["cd_max_rel_err_vs_fp64_oracle"] = max(
+                    abs(a / b - 1) for a, b in zip(target["drags"], cpu_drags))
+        if target is not None:
+            del target["drags"]
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": dict(workload_config(), lanes=lanes),
+            "data": "synthetic", "config": workload_config(), "tuning": {"lanes": lanes},
+            "target": target,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
@@ -930,6 +990,8 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-target", action="store_true",
+                    help="drag curve: leave out the warm-started batch against the single-case cold path")
     ap.add_argument("--probe", type=int, default=0,
                     help="run this many LU-SGS steps of the batch with per-kernel timing and exit")
     ap.add_argument("--workload", choices=["drag-curve", "seeded", "warmstart", "stream", "fitted", "gemm", "stencil", "verified",

@@ -60,6 +60,23 @@ __device__ __forceinline__ bool is_physical(const Cons<R>& q, R gamma) {
          fabs(w.v) < big;
 }
 
+// applyImplicitUpdate (src/engine-cpu/euler2d.ts:816-847) for one cell:
+// Q + alpha dQ with alpha halved until density and pressure stay within a
+// factor of two of Q's.
+template <class R>
+__device__ __forceinline__ Cons<R> implicit_update(const Cons<R>& q0, float4 d4, R gamma) {
+  const R p0 = pressure_of(q0.rho, q0.mu, q0.mv, q0.e, gamma);
+  const R d0 = R(d4.x), d1 = R(d4.y), d2 = R(d4.z), d3 = R(d4.w);
+  R alpha = R(1);
+  for (int tries = 0; tries < 30; tries++) {
+    const R rho1 = q0.rho + alpha * d0;
+    const R p1 = pressure_of(rho1, q0.mu + alpha * d1, q0.mv + alpha * d2, q0.e + alpha * d3, gamma);
+    if (rho1 > R(0.5) * q0.rho && rho1 < R(2) * q0.rho && p1 > R(0.5) * p0 && p1 < R(2) * p0) break;
+    alpha *= R(0.5);
+  }
+  return {q0.rho + alpha * d0, q0.mu + alpha * d1, q0.mv + alpha * d2, q0.e + alpha * d3};
+}
+
 // LIMITERS (src/scheme/limiters.ts:24-94).
 template <class R>
 __device__ __forceinline__ R limit(int limiter, R a, R b) {

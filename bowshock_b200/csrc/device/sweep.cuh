@@ -423,36 +423,21 @@ static __global__ void __launch_bounds__(32 * kMaxSweepWarps) lusgs_sweep_kernel
   if (threadIdx.x == 0) A.cfl[c] = fminf(A.cfl_max[c], A.cfl[c] * A.growth[c]);
 }
 
-// applyImplicitUpdate (src/engine-cpu/euler2d.ts:816-847) for one cell:
-// Q + alpha dQ with alpha halved until density and pressure stay within a
-// factor of two of Q's.
-template <class R>
-__device__ __forceinline__ Cons<R> implicit_update(const Cons<R>& q0, float4 d4, R gamma) {
-  const R p0 = pressure_of(q0.rho, q0.mu, q0.mv, q0.e, gamma);
-  const R d0 = R(d4.x), d1 = R(d4.y), d2 = R(d4.z), d3 = R(d4.w);
-  R alpha = R(1);
-  for (int tries = 0; tries < 30; tries++) {
-    const R rho1 = q0.rho + alpha * d0;
-    const R p1 = pressure_of(rho1, q0.mu + alpha * d1, q0.mv + alpha * d2, q0.e + alpha * d3, gamma);
-    if (rho1 > R(0.5) * q0.rho && rho1 < R(2) * q0.rho && p1 > R(0.5) * p0 && p1 < R(2) * p0) break;
-    alpha *= R(0.5);
-  }
-  return {q0.rho + alpha * d0, q0.mu + alpha * d1, q0.mv + alpha * d2, q0.e + alpha * d3};
-}
-
-// The update for every cell of every active case; flags non-physical results.
+// The update of every cell of every active case, from `src` into `dst` (the
+// same arrays, or the other buffer of the state); flags non-physical
+// results. A case whose sweep gave up (dQ incomplete) keeps its state.
 template <class R>
 __global__ void __launch_bounds__(TILE_THREADS) lusgs_update_kernel(const CaseDev* cases,
                                                                     const int2* tiles,
                                                                     const int* active,
-                                                                    StateView<R> q,
+                                                                    StateView<R> src,
+                                                                    StateView<R> dst,
                                                                     const float4* dq,
                                                                     unsigned* status) {
   const int2 tile = tiles[blockIdx.x];
   const int c = tile.x;
   if (active != nullptr && active[c] == 0) return;
-  // A sweep that gave up left dQ incomplete: the case keeps its state.
-  if (status[c] & STATUS_TIMEOUT) return;
+  const bool keep = (status[c] & STATUS_TIMEOUT) != 0;
   const CaseDev& cd = cases[c];
   const int ni = cd.ni, nj = cd.nj;
   const int tiles_i = (ni + TI - 1) / TI;
@@ -462,8 +447,9 @@ __global__ void __launch_bounds__(TILE_THREADS) lusgs_update_kernel(const CaseDe
   if (i < ni && j < nj && int(threadIdx.x) < TI * TJ) {
     const R gamma = R(cd.gamma);
     const int64_t k = cd.cell + i + int64_t(j) * ni;
-    const Cons<R> q1 = implicit_update(q.load(k), dq[k], gamma);
-    q.store(k, q1);
+    const Cons<R> q0 = src.load(k);
+    const Cons<R> q1 = keep ? q0 : implicit_update(q0, dq[k], gamma);
+    dst.store(k, q1);
     bad = !is_physical(q1, gamma);
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&status[c], STATUS_NON_PHYSICAL);

@@ -40,6 +40,13 @@ struct TileArgs {
   const float* cfl;       // PREPARE: per case current implicit CFL number
   const float* omega;     // PREPARE: per case omega
   double* res_out;        // RESIDUAL: 4 values per cell, arena like the state
+  // PREPARE: the previous LU-SGS step's correction (row-major like the
+  // state), or null. Each cell the tile reads (its own and its halo) is
+  // src updated by it (applyImplicitUpdate), and the tile's own updated
+  // cells are stored in upd_out - the other buffer of the state, since
+  // neighbouring tiles still read src.
+  const float4* dq_in;
+  StateView<R> upd_out;
 };
 
 // Spectral radius |u . n| + a of a primitive state along (nx, ny), in FP32
@@ -76,10 +83,24 @@ __global__ void __launch_bounds__(TILE_THREADS, kMinBlocks) tile_kernel(const Ti
   const int i = i0 + li, j = j0 + lj;
   const int64_t k = cd.cell + i + int64_t(j) * ni;
 
+  // Every cell is read through `at`: src, or src with the previous step's
+  // correction applied (the same arithmetic in every tile that reads it, so
+  // the halo of one tile is the interior of its neighbour exactly). A case
+  // whose previous sweep gave up keeps its state.
+  const bool apply = MODE == MODE_PREPARE && A.dq_in != nullptr && (A.status[c] & STATUS_TIMEOUT) == 0;
+  auto at = [&](int64_t kk) -> Cons<R> {
+    const Cons<R> q0 = A.src.load(kk);
+    return apply ? implicit_update(q0, A.dq_in[kk], gamma) : q0;
+  };
+
   // Own cell: conserved in registers, primitives in shared memory.
   Cons<R> qs{};
   if (mine) {
-    qs = A.src.load(k);
+    qs = at(k);
+    if (MODE == MODE_PREPARE && A.dq_in != nullptr) {
+      A.upd_out.store(k, qs);
+      if (!is_physical(qs, gamma)) atomicOr(&A.status[c], STATUS_NON_PHYSICAL);
+    }
     const Prim<R> w = to_prim(qs, gamma);
     W[0][lj + 2][li + 2] = w.rho;
     W[1][lj + 2][li + 2] = w.u;
@@ -104,7 +125,7 @@ __global__ void __launch_bounds__(TILE_THREADS, kMinBlocks) tile_kernel(const Ti
       hi = i0 + col;
     }
     if (valid) {
-      const Prim<R> w = to_prim(load_cell(cd, A.src, A.m, hi, hj), gamma);
+      const Prim<R> w = to_prim(cell_or_ghost<R>(cd, A.m, hi, hj, gamma, false, at), gamma);
       W[0][hj - j0 + 2][hi - i0 + 2] = w.rho;
       W[1][hj - j0 + 2][hi - i0 + 2] = w.u;
       W[2][hj - j0 + 2][hi - i0 + 2] = w.v;

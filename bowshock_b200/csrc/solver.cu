@@ -527,20 +527,27 @@ class Solver final : public SolverBase {
       st = ensure_implicit();
       if (st == BS_OK) st = set_implicit_params(cfl, omega, 1.0);
       if (st == BS_OK) st = set_implicit_cfl(cfl);
+      // One untimed residual pass and sweep give the timed passes a correction to apply.
+      const bsd::StateView<R> q = q_view();
+      if (st == BS_OK) st = launch_tile<bsd::MODE_PREPARE>(q, q, q, 0, 1, false, nullptr, nullptr, false);
+      if (st == BS_OK) st = launch_sweep();
     } else {
       st = ensure_explicit();
     }
     for (int it = 0; it < iterations && st == BS_OK; it++) {
       cudaEventRecord(ev[0], stream_);
       if (method == kMethodImplicit) {
-        const bsd::StateView<R> q = q_view();
-        st = launch_tile<bsd::MODE_PREPARE>(q, q, q, 0, 1, false, norm_.p, nullptr, false);
+        // A step's residual pass with the previous step's update fused in
+        // (read from q, written to the other buffer, so q stays as it was),
+        // the sweeps, and a run's closing update (out of place as well).
+        const bsd::StateView<R> q = q_view(), qb = qb_view();
+        st = launch_tile<bsd::MODE_PREPARE>(q, q, q, 0, 1, false, norm_.p, nullptr, false, dq_.p, qb);
         cudaEventRecord(ev[1], stream_);
         cudaEventRecord(ev[2], stream_);
         if (st == BS_OK) st = launch_sweep();
         cudaEventRecord(ev[3], stream_);
         cudaEventRecord(ev[4], stream_);
-        if (st == BS_OK) st = launch_update();
+        if (st == BS_OK) st = launch_update_on(whole(), q, qb);
       } else {
         const bsd::StateView<R> q = q_view(), s1 = s1_view(), s2 = s2_view();
         st = launch_tile<bsd::MODE_STAGE>(q, q, s1, 0.0, 1.0, true, norm_.p, nullptr, false);
@@ -949,6 +956,8 @@ class Solver final : public SolverBase {
 
   bsd::StateView<R> q_view() const { return {q_[0].p, q_[1].p, q_[2].p, q_[3].p}; }
   bsd::StateView<R> s1_view() const { return {s1_[0].p, s1_[1].p, s1_[2].p, s1_[3].p}; }
+  // The other buffer of the state, which LU-SGS steps alternate with q.
+  bsd::StateView<R> qb_view() const { return {qb_[0].p, qb_[1].p, qb_[2].p, qb_[3].p}; }
   bsd::StateView<R> s2_view() const { return {s2_[0].p, s2_[1].p, s2_[2].p, s2_[3].p}; }
   bsd::MetricsView metrics() const {
     bsd::MetricsView m{iface_.p, jface_.p, cellm_.p};
@@ -974,6 +983,7 @@ class Solver final : public SolverBase {
     BS_CUDA(rec_f_.alloc(5 * size_t(total_slots_)));
     BS_CUDA(rec_b_.alloc(5 * size_t(total_slots_)));
     BS_CUDA(dq_.alloc(total_cells_));
+    for (int v = 0; v < 4; v++) BS_CUDA(qb_[v].alloc(total_cells_));
     return BS_OK;
   }
 
@@ -1060,14 +1070,16 @@ class Solver final : public SolverBase {
   template <int MODE>
   bs_status launch_tile(bsd::StateView<R> src, bsd::StateView<R> u0, bsd::StateView<R> out,
                         double a, double b, bool first, double* norm, double* res_out,
-                        bool all_cases) {
-    return launch_tile_on<MODE>(whole(), src, u0, out, a, b, first, norm, res_out, all_cases);
+                        bool all_cases, const float4* dq_in = nullptr, bsd::StateView<R> upd_out = {}) {
+    return launch_tile_on<MODE>(whole(), src, u0, out, a, b, first, norm, res_out, all_cases, dq_in,
+                                upd_out);
   }
 
   template <int MODE>
   bs_status launch_tile_on(const LaneView& lane, bsd::StateView<R> src, bsd::StateView<R> u0,
                            bsd::StateView<R> out, double a, double b, bool first, double* norm,
-                           double* res_out, bool all_cases) {
+                           double* res_out, bool all_cases, const float4* dq_in = nullptr,
+                           bsd::StateView<R> upd_out = {}) {
     bsd::TileArgs<R> A{};
     A.cases = d_cases_.p;
     A.tiles = lane.tiles;
@@ -1088,6 +1100,8 @@ class Solver final : public SolverBase {
     A.cfl = cfl_.p;
     A.omega = omega_.p;
     A.res_out = res_out;
+    A.dq_in = dq_in;
+    A.upd_out = upd_out;
     if (lane.n_tiles >= 4 * sm_count_)
       bsd::tile_kernel<R, MODE, 4><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
     else
@@ -1137,14 +1151,24 @@ class Solver final : public SolverBase {
     return BS_OK;
   }
 
-  bs_status record_implicit_step(bool norm) { return record_implicit_step_on(whole(), norm); }
-
-  bs_status record_implicit_step_on(const LaneView& lane, bool norm) {
-    const bsd::StateView<R> q = q_view();
-    BS_TRY(launch_tile_on<bsd::MODE_PREPARE>(lane, q, q, q, 0, 1, false, norm ? norm_.p : nullptr,
-                                             nullptr, false));
+  // Step s (from 0) of a run of `count` LU-SGS steps on one lane. The update
+  // of each step is applied by the next step's residual pass as it reads the
+  // state (the first step has none to apply), which stores the updated state
+  // in the other buffer: step s >= 1 reads q when s is odd and qb when even,
+  // and writes the other. After the last step a closing update brings the
+  // state back into q, so every run begins and ends with the state in q.
+  bs_status record_implicit_step_on(const LaneView& lane, bool norm, int s, int count) {
+    const bsd::StateView<R> q = q_view(), qb = qb_view();
+    const bsd::StateView<R> src = (s == 0 || s % 2 == 1) ? q : qb;
+    const bsd::StateView<R> dst = s % 2 == 1 ? qb : q;
+    BS_TRY(launch_tile_on<bsd::MODE_PREPARE>(lane, src, src, src, 0, 1, false, norm ? norm_.p : nullptr,
+                                             nullptr, false, s == 0 ? nullptr : dq_.p, dst));
     BS_TRY(launch_sweep_on(lane));
-    return launch_update_on(lane);
+    if (s == count - 1) {
+      const bsd::StateView<R> last = (s == 0 || s % 2 == 0) ? q : qb;
+      return launch_update_on(lane, last, q);
+    }
+    return BS_OK;
   }
 
   // One LU-SGS step with Anderson acceleration: the residual pass and the
@@ -1184,7 +1208,7 @@ class Solver final : public SolverBase {
   }
 
   bs_status launch_sweep() { return launch_sweep_on(whole()); }
-  bs_status launch_update() { return launch_update_on(whole()); }
+
 
   bs_status launch_sweep_on(const LaneView& lane) {
     bsd::SweepArgs S{};
@@ -1204,9 +1228,9 @@ class Solver final : public SolverBase {
     return BS_OK;
   }
 
-  bs_status launch_update_on(const LaneView& lane) {
+  bs_status launch_update_on(const LaneView& lane, bsd::StateView<R> src, bsd::StateView<R> dst) {
     bsd::lusgs_update_kernel<R><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(
-        d_cases_.p, lane.tiles, d_active_.p, q_view(), dq_.p, status_.p);
+        d_cases_.p, lane.tiles, d_active_.p, src, dst, dq_.p, status_.p);
     launches_++;
     BS_CUDA(cudaGetLastError());
     return BS_OK;
@@ -1229,7 +1253,7 @@ class Solver final : public SolverBase {
         else if (method == kMethodAnderson)
           BS_TRY(record_anderson_step_on(whole(), norm));
         else
-          BS_TRY(record_implicit_step(norm));
+          BS_TRY(record_implicit_step_on(whole(), norm, s, count));
       }
       return BS_OK;
     }
@@ -1245,7 +1269,7 @@ class Solver final : public SolverBase {
         else if (method == kMethodAnderson)
           BS_TRY(record_anderson_step_on(lane, norm));
         else
-          BS_TRY(record_implicit_step_on(lane, norm));
+          BS_TRY(record_implicit_step_on(lane, norm, s, count));
       }
     }
     for (size_t k = 0; k < lanes_.size(); k++) {
@@ -1344,7 +1368,7 @@ class Solver final : public SolverBase {
   DevBuf<bsd::CaseDev> d_cases_;
   DevBuf<int2> d_tiles_;
   DevBuf<int> d_case_list_, d_active_;
-  DevBuf<R> q_[4], s1_[4], s2_[4];
+  DevBuf<R> q_[4], qb_[4], s1_[4], s2_[4];
   DevBuf<float> dt_, cfl_, cflmax_, growth_, omega_;
   DevBuf<float4> iface_, jface_, rec_f_, rec_b_, dq_;
   DevBuf<float2> cellm_;

@@ -223,7 +223,7 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
   }
   if (err == cudaSuccess) {
     bsd::lusgs_update_kernel<double><<<n_tiles, bsd::TILE_THREADS, 0, st>>>(
-        d_case, d_tiles, nullptr, q, d_dq, &d_words->status);
+        d_case, d_tiles, nullptr, q, q, d_dq, &d_words->status);
     err = cudaGetLastError();
   }
   double norm = 0;

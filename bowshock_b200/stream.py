@@ -15,12 +15,13 @@ from .mlp import WarmStartNet
 from .warmstart import warm_solve
 from .workloads import Case, NoseCase, make_cases
 
-# Device bytes per cell of a case in an FP64 LU-SGS batch: state 4 x 8,
-# time step 4, cell metrics 8, the i- and j-face metrics 16 each (one face
-# of each per cell, the extra row and column counted separately) and the
-# correction dQ 16; forward and backward sweep records 5 x 16 each per slot,
-# of which a case has sweep_slots(ni, nj).
-CELL_BYTES = 32 + 4 + 8 + 16 + 16 + 16
+# Device bytes per cell of a case in an FP64 LU-SGS batch: the state and
+# the other buffer it alternates with over a run of steps, 2 x 4 x 8; time
+# step 4, cell metrics 8, the i- and j-face metrics 16 each (one face of each
+# per cell, the extra row and column counted separately) and the correction
+# dQ 16; forward and backward sweep records 5 x 16 each per slot, of which a
+# case has sweep_slots(ni, nj).
+CELL_BYTES = 64 + 4 + 8 + 16 + 16 + 16
 SLOT_BYTES = 160
 
 

@@ -172,6 +172,13 @@ BS_API bs_status bs_device_count(int32_t *count);
  * objects stay on the device they were created on. */
 BS_API bs_status bs_set_device(int32_t device);
 
+/* The measured FP64 fused multiply-add rate of the current device: a grid
+ * that fills every SM, each thread running 8 independent FMA chains of
+ * `iterations` steps, timed by CUDA events after one warm-up launch. The
+ * denominator of the flux kernels' FP64 fraction (their residual is FP64
+ * arithmetic). No counterpart in the reference. */
+BS_API bs_status bs_fp64_fma_rate(int32_t iterations, double *tflops, double *ms);
+
 /* ---- single-grid engine: Euler2D / GpuEuler2D --------------------------- */
 
 /* new Euler2D(config) / GpuEuler2D.create (src/engine-cpu/euler2d.ts:318,

@@ -48,6 +48,7 @@ def lib() -> C.CDLL:
             "bso_set_conserved": [vp, dp],
             "bso_set_face_states": [vp, C.c_int, dp],
             "bso_set_face_fluxes": [vp, C.c_int, dp],
+            "bso_set_quantize": [vp, C.c_int],
             "bso_iterate": [vp, C.c_int],
             "bso_iterate_implicit": [vp, C.c_int, C.c_double, C.c_double],
             "bso_implicit_correction": [vp, C.c_double, C.c_double, dp],
@@ -163,6 +164,12 @@ class OracleEuler2D:
     def set_conserved(self, q: np.ndarray) -> None:
         q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1)
         _check(lib().bso_set_conserved(self._h, _dp(q)))
+
+    def set_quantize(self, on: bool) -> None:
+        """FP64 engine only: round the stored state to FP32 after every update
+        (FP32 storage, FP64 arithmetic) - a probe of what an FP32 field
+        loses, not a mode of the reference."""
+        _check(lib().bso_set_quantize(self._h, 1 if on else 0))
 
     def iterate(self, steps: int) -> None:
         _check(lib().bso_iterate(self._h, steps))

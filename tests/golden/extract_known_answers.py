@@ -1,9 +1,9 @@
 """Extracts the known answers that pin the steady Euler path from the
 reference's own test files (read as text; nothing of the reference runs) into
-reference_known_answers.json. Run from the repository root with the
-reference checked out at REFERENCE (default /root/reference):
+reference_known_answers.json. Run from the repository root with the path of
+a checkout of the reference, as an argument or in the REFERENCE variable:
 
-    python tests/golden/extract_known_answers.py
+    python tests/golden/extract_known_answers.py <reference checkout>
 
 The tests read only the JSON file."""
 from __future__ import annotations
@@ -14,7 +14,15 @@ import re
 import sys
 from pathlib import Path
 
-REF = Path(os.environ.get("REFERENCE", "/root/reference"))
+def reference_root() -> Path:
+    """The reference checkout: the first argument, else REFERENCE."""
+    where = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFERENCE")
+    if not where:
+        sys.exit("usage: extract_known_answers.py <reference checkout> (or set REFERENCE)")
+    return Path(where)
+
+
+REF = Path()
 OUT = Path(__file__).resolve().parent / "reference_known_answers.json"
 
 
@@ -26,6 +34,8 @@ def find_line(text: str, needle: str) -> int:
 
 
 def main() -> None:
+    global REF
+    REF = reference_root()
     out: dict = {}
     # Verified drag of the CPU engine on the 20 deg cone at Mach 3 (cylinder 4,
     # nj = 20), refinements 1 and 2.

@@ -44,7 +44,7 @@ def test_device_bytes_grow_with_the_sweep_record_slots():
     assert sweep_slots(160, 80) == 2 * 192 * 33 + 176 * 17
     assert sweep_slots(40, 32) == 72 * 33
     b = case_device_bytes(80, 40)
-    assert b == 3200 * 92 + 120 * 16 + (112 * 33 + 88 * 9) * 160 + 64 * 120
+    assert b == 3200 * 124 + 120 * 16 + (112 * 33 + 88 * 9) * 160 + 64 * 120
     assert case_device_bytes(640, 320) > 50 * b
 
 
