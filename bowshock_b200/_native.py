@@ -94,6 +94,8 @@ SIGNATURES: dict[str, list] = {
     "bs_engine_set_sweep_wait_limit": [_vp, C.c_int32],
     "bs_fp64_fma_rate": [C.c_int32, _dp, _dp],
     "bs_batch_set_sweep_wait_limit": [_vp, C.c_int32],
+    "bs_batch_set_tile_shape": [_vp, C.c_int32],
+    "bs_batch_tuning": [_vp, _ip, _ip, _ip, _ip, _ip],
     "bs_batch_set_metric_precision": [_vp, C.c_int32],
     "bs_batch_forebody_drag": [_vp, C.c_int32, C.c_double, C.c_double, C.c_double, _dp],
     "bs_batch_read_primitives": [_vp, C.c_int32, _dp],

@@ -72,6 +72,18 @@ class CudaBatch:
         """64: two-float metrics in the residual; 32: FP32 metrics (default)."""
         self._call("bs_batch_set_metric_precision", int(bits))
 
+    def set_tile_shape(self, shape: int) -> None:
+        """The residual pass's tile shape: -1 the default, 0 .. 4 the
+        autotuner's choices (bs_batch_set_tile_shape)."""
+        self._call("bs_batch_set_tile_shape", int(shape))
+
+    def tuning(self) -> dict:
+        """Lanes and tile shape as set or tuned."""
+        v = [C.c_int32() for _ in range(5)]
+        self._call("bs_batch_tuning", *[C.byref(x) for x in v])
+        lanes, shape, ti, tj, threads = (x.value for x in v)
+        return {"lanes": lanes, "tile_shape": shape, "tile": f"{ti}x{tj}", "threads": threads}
+
     def set_sweep_wait_limit(self, polls: int) -> None:
         """As CudaEuler2D.set_sweep_wait_limit, for the batch's sweeps."""
         self._call("bs_batch_set_sweep_wait_limit", int(polls))

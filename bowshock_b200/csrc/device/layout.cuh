@@ -35,6 +35,24 @@ constexpr int TJ = 15;
 constexpr int TILE_THREADS = 256;
 static_assert(TI * TJ <= TILE_THREADS, "a tile has at most one cell per thread");
 
+// Tile shapes the residual pass and the explicit stages can run with, the
+// autotuner's choices: TI x TJ cells on `threads` threads, `min_blocks`
+// resident CTAs asked of the compiler. Shape 0 is the default above with one
+// resident CTA asked for, shape 1 the same with four. Smaller tiles put more
+// CTAs on a case (more SMs on one case's pass, at more halo per cell); the
+// 24 x 15 tile reads the least halo (43 % of its cells against 52 %).
+struct TileShape {
+  int ti, tj, threads, min_blocks;
+};
+constexpr int kTileShapes = 5;
+__host__ __device__ constexpr TileShape tile_shape(int k) {
+  return k == 0   ? TileShape{TI, TJ, TILE_THREADS, 1}
+         : k == 1 ? TileShape{TI, TJ, TILE_THREADS, 4}
+         : k == 2 ? TileShape{16, 7, 128, 1}
+         : k == 3 ? TileShape{8, 15, 128, 1}
+                  : TileShape{24, 15, 384, 1};
+}
+
 // Per-case status bits.
 constexpr unsigned STATUS_NON_PHYSICAL = 1u;
 // A kernel gave up waiting for an asynchronous copy (bounded wait).

@@ -57,12 +57,15 @@ __device__ __forceinline__ float radius32(R rho, R u, R v, R p, float gamma, flo
   return fabsf(fu * nx + fv * ny) + __fsqrt_rn((gamma * fp) / fr);
 }
 
-// kMinBlocks 4 asks for four resident CTAs per SM (at some spilling): on
-// launches of several waves the fourth CTA's warps fill the issue slots that
-// the others leave while they wait at a barrier for their slowest face; on
-// one wave the default is faster.
-template <class R, int MODE, int kMinBlocks = 1>
-__global__ void __launch_bounds__(TILE_THREADS, kMinBlocks) tile_kernel(const TileArgs<R> A) {
+// The tile is TI x TJ cells on kThreads threads (the batch's default shape,
+// or another the autotuner picked for the residual pass). kMinBlocks asks for
+// that many resident CTAs per SM (at some spilling): on launches of several
+// waves the extra CTA's warps fill the issue slots that the others leave
+// while they wait at a barrier for their slowest face; on one wave fewer,
+// larger register budgets are faster.
+template <class R, int MODE, int kMinBlocks = 1, int TI = bsd::TI, int TJ = bsd::TJ, int kThreads = TILE_THREADS>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) tile_kernel(const TileArgs<R> A) {
+  static_assert(TI * TJ <= kThreads, "a tile has at most one cell per thread");
   __shared__ R W[4][TJ + 4][TI + 4];
   __shared__ R Fi[4][TJ][TI + 1];
   __shared__ R Fj[4][TJ + 1][TI];
@@ -109,7 +112,7 @@ __global__ void __launch_bounds__(TILE_THREADS, kMinBlocks) tile_kernel(const Ti
   }
   // Halo: two columns each side of the tile's rows, two rows each side of
   // its columns (the stencils are one-dimensional; corners are unused).
-  for (int h = tid; h < 4 * TJ + 4 * TI; h += TILE_THREADS) {
+  for (int h = tid; h < 4 * TJ + 4 * TI; h += kThreads) {
     int hi, hj;
     bool valid;
     if (h < 4 * TJ) {
@@ -140,7 +143,7 @@ __global__ void __launch_bounds__(TILE_THREADS, kMinBlocks) tile_kernel(const Ti
 
   // Every face of the tile once: its flux times its area.
   const int nfi = (ti + 1) * tj, nfj = ti * (tj + 1);
-  for (int f = tid; f < nfi + nfj; f += TILE_THREADS) {
+  for (int f = tid; f < nfi + nfj; f += kThreads) {
     R flux[4];
     Prim<R> left, right;
     if (f < nfi) {

@@ -396,6 +396,22 @@ bs_status bs_batch_set_metric_precision(bs_batch* batch, int32_t bits) {
   BS_BATCH_CALL(batch, { return batch->solver->set_metric_precision(bits); });
 }
 
+bs_status bs_batch_set_tile_shape(bs_batch* batch, int32_t shape) {
+  BS_BATCH_CALL(batch, { return batch->solver->set_tile_shape(shape); });
+}
+
+bs_status bs_batch_tuning(bs_batch* batch, int32_t* lanes, int32_t* shape, int32_t* tile_i, int32_t* tile_j,
+                          int32_t* threads) {
+  BS_BATCH_CALL(batch, {
+    if (lanes == nullptr || shape == nullptr || tile_i == nullptr || tile_j == nullptr || threads == nullptr)
+      return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+    *lanes = batch->solver->lanes();
+    *shape = batch->solver->tile_shape();
+    bs::tile_dims(*shape, tile_i, tile_j, threads);
+    return BS_OK;
+  });
+}
+
 bs_status bs_batch_set_sweep_wait_limit(bs_batch* batch, int32_t polls) {
   BS_BATCH_CALL(batch, { return batch->solver->set_sweep_wait_limit(polls); });
 }

@@ -118,7 +118,21 @@ struct LaneView {
   int n_cases;
   int max_nj;
   cudaStream_t stream;
+  // The residual pass's tiles when the batch runs a tuned tile shape (else
+  // the default tiles above).
+  const int2* rtiles = nullptr;
+  int n_rtiles = 0;
 };
+
+// The tiles of `cases` for a tile shape of ti x tj cells, case by case.
+std::vector<int2> tiles_for(const std::vector<bsd::CaseDev>& hc, const std::vector<int>& cases, int ti, int tj) {
+  std::vector<int2> t;
+  for (int c : cases) {
+    const int n = ((hc[c].ni + ti - 1) / ti) * ((hc[c].nj + tj - 1) / tj);
+    for (int k = 0; k < n; k++) t.push_back(make_int2(c, k));
+  }
+  return t;
+}
 
 constexpr int kMaxLanes = 64;
 constexpr int kDefaultLanes = 16;
@@ -349,6 +363,7 @@ class Solver final : public SolverBase {
       }
       lane->n_cases = int(members[l].size());
       lane->n_tiles = int(tiles.size());
+      lane->members = members[l];
       BS_CUDA(lane->tiles.alloc(tiles.size()));
       BS_CUDA(cudaMemcpy(lane->tiles.p, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice));
       BS_CUDA(lane->case_list.alloc(members[l].size()));
@@ -360,7 +375,7 @@ class Solver final : public SolverBase {
       ev_join_.push_back(ev);
       lanes_.push_back(std::move(lane));
     }
-    return BS_OK;
+    return build_rtiles();
   }
 
   int n_cases() const override { return n_; }
@@ -422,10 +437,47 @@ class Solver final : public SolverBase {
     return BS_OK;
   }
 
+  // The residual-pass tile lists (whole batch and every lane) for rshape_.
+  bs_status build_rtiles() {
+    if (rshape_ < 0) return BS_OK;
+    const bsd::TileShape sh = bsd::tile_shape(rshape_);
+    std::vector<int> all(n_);
+    for (int c = 0; c < n_; c++) all[c] = c;
+    std::vector<int2> t = tiles_for(hc_, all, sh.ti, sh.tj);
+    BS_CUDA(d_rtiles_.alloc(t.size()));
+    BS_CUDA(cudaMemcpy(d_rtiles_.p, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    n_rtiles_ = int(t.size());
+    for (auto& l : lanes_) {
+      t = tiles_for(hc_, l->members, sh.ti, sh.tj);
+      BS_CUDA(l->rtiles.alloc(t.size()));
+      BS_CUDA(cudaMemcpy(l->rtiles.p, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice));
+      l->n_rtiles = int(t.size());
+    }
+    return BS_OK;
+  }
+
+  bs_status set_tile_shape(int shape) override {
+    if (shape < -1 || shape >= bsd::kTileShapes)
+      return fail(BS_INVALID_ARGUMENT, "tile shape: -1 (default) or 0 .. " + std::to_string(bsd::kTileShapes - 1));
+    if (shape >= 0 && sizeof(R) != sizeof(double))
+      return fail(BS_INVALID_ARGUMENT, "the all-FP32 engine keeps the default tile shape");
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    rshape_ = shape;
+    BS_TRY(build_rtiles());
+    // Captured graphs hold the old launches.
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+    graph_launches_.clear();
+    return BS_OK;
+  }
+
+  int tile_shape() const override { return rshape_; }
+
   // Times `steps` steps from the current state with 1, 2, 4, ... lanes (up to
-  // 64 and the case count), each after one untimed run that captures its
-  // graphs, restoring the state before every run; keeps the fastest. The
-  // state, CFL numbers and status words are as before the call.
+  // 64 and the case count), then, with the fastest lane count, each tile shape
+  // of the residual pass (FP64 batches), each run after one untimed run that
+  // captures its graphs, restoring the state before every run; keeps the
+  // fastest. The state, CFL numbers and status words are as before the call.
   bs_status autotune(int method, int steps, double cfl, double omega, int* lanes, double* ms_per_step) override {
     if (steps < 1) return fail(BS_INVALID_ARGUMENT, "autotune needs steps >= 1");
     if (method == kMethodImplicit) {
@@ -470,6 +522,29 @@ class Solver final : public SolverBase {
     }
     release_lanes();
     BS_TRY(init_lanes(hc_, best));
+    // Then the residual pass's tile shape, with those lanes (FP64 batches;
+    // -1 is the untuned default).
+    if (sizeof(R) == sizeof(double)) {
+      const int before = rshape_;
+      int best_shape = before;
+      for (int k = -1; k < bsd::kTileShapes; k++) {
+        BS_TRY(set_tile_shape(k));
+        BS_TRY(restore());
+        BS_TRY(run_steps(method, steps, false));
+        BS_TRY(restore());
+        BS_CUDA(cudaEventRecord(ev0_, stream_));
+        BS_TRY(run_steps(method, steps, false));
+        BS_CUDA(cudaEventRecord(ev1_, stream_));
+        BS_CUDA(cudaEventSynchronize(ev1_));
+        float t = 0;
+        BS_CUDA(cudaEventElapsedTime(&t, ev0_, ev1_));
+        if (t < best_ms) {
+          best_ms = t;
+          best_shape = k;
+        }
+      }
+      BS_TRY(set_tile_shape(best_shape));
+    }
     BS_TRY(restore());
     BS_CUDA(cudaStreamSynchronize(stream_));
     *lanes = best;
@@ -1064,7 +1139,7 @@ class Solver final : public SolverBase {
   }
 
   LaneView whole() const {
-    return {d_tiles_.p, n_tiles_, d_case_list_.p, n_, max_nj_, stream_};
+    return {d_tiles_.p, n_tiles_, d_case_list_.p, n_, max_nj_, stream_, d_rtiles_.p, n_rtiles_};
   }
 
   template <int MODE>
@@ -1102,10 +1177,29 @@ class Solver final : public SolverBase {
     A.res_out = res_out;
     A.dq_in = dq_in;
     A.upd_out = upd_out;
-    if (lane.n_tiles >= 4 * sm_count_)
-      bsd::tile_kernel<R, MODE, 4><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
-    else
-      bsd::tile_kernel<R, MODE><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
+    bool tuned = false;
+    if constexpr (sizeof(R) == sizeof(double) && MODE != bsd::MODE_RESIDUAL) {
+      if (rshape_ >= 0) {
+        tuned = true;
+        A.tiles = lane.rtiles;
+        const int n = lane.n_rtiles;
+        switch (rshape_) {
+          case 0: bsd::tile_kernel<R, MODE, 1><<<n, bsd::TILE_THREADS, 0, lane.stream>>>(A); break;
+          case 1: bsd::tile_kernel<R, MODE, 4><<<n, bsd::TILE_THREADS, 0, lane.stream>>>(A); break;
+          case 2: bsd::tile_kernel<R, MODE, 1, 16, 7, 128><<<n, 128, 0, lane.stream>>>(A); break;
+          case 3: bsd::tile_kernel<R, MODE, 1, 8, 15, 128><<<n, 128, 0, lane.stream>>>(A); break;
+          default: bsd::tile_kernel<R, MODE, 1, 24, 15, 384><<<n, 384, 0, lane.stream>>>(A); break;
+        }
+      }
+    }
+    if (!tuned) {
+      // Untuned: the default tile, four resident CTAs asked for on launches
+      // of at least four waves.
+      if (lane.n_tiles >= 4 * sm_count_)
+        bsd::tile_kernel<R, MODE, 4><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
+      else
+        bsd::tile_kernel<R, MODE><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
+    }
     launches_++;
     BS_CUDA(cudaGetLastError());
     return BS_OK;
@@ -1261,7 +1355,8 @@ class Solver final : public SolverBase {
     BS_CUDA(cudaEventRecord(ev_fork_, stream_));
     for (auto& l : lanes_) BS_CUDA(cudaStreamWaitEvent(l->stream, ev_fork_, 0));
     for (auto& l : lanes_) {
-      const LaneView lane{l->tiles.p, l->n_tiles, l->case_list.p, l->n_cases, l->max_nj, l->stream};
+      const LaneView lane{l->tiles.p,  l->n_tiles, l->case_list.p, l->n_cases,
+                          l->max_nj,   l->stream,  l->rtiles.p,    l->n_rtiles};
       for (int s = 0; s < count; s++) {
         const bool norm = norm_last && s == count - 1;
         if (method == kMethodExplicit)
@@ -1382,9 +1477,10 @@ class Solver final : public SolverBase {
   cudaStream_t stream_ = nullptr;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   struct Lane {
-    DevBuf<int2> tiles;
+    DevBuf<int2> tiles, rtiles;
     DevBuf<int> case_list;
-    int n_tiles = 0, n_cases = 0, max_nj = 0;
+    std::vector<int> members;
+    int n_tiles = 0, n_rtiles = 0, n_cases = 0, max_nj = 0;
     cudaStream_t stream = nullptr;
   };
   std::vector<std::unique_ptr<Lane>> lanes_;
@@ -1398,6 +1494,11 @@ class Solver final : public SolverBase {
   std::map<GraphKey, int64_t> graph_launches_;
   int64_t launches_ = 0;
   int sweep_wait_limit_ = -1;
+  // The residual pass's tile shape (bsd::tile_shape), or -1 for the default
+  // choice; the whole batch's tiles of that shape.
+  int rshape_ = -1;
+  DevBuf<int2> d_rtiles_;
+  int n_rtiles_ = 0;
   double last_solve_ms_ = 0;
   int64_t last_solve_launches_ = 0;
   // Anderson acceleration: settings and its per-case history.
@@ -1413,6 +1514,13 @@ class Solver final : public SolverBase {
 };
 
 }  // namespace
+
+void tile_dims(int shape, int32_t* ti, int32_t* tj, int32_t* threads) {
+  const bsd::TileShape sh = bsd::tile_shape(shape < 0 ? 0 : shape);
+  *ti = sh.ti;
+  *tj = sh.tj;
+  *threads = sh.threads;
+}
 
 bs_status make_solver(std::vector<HostCase>&& cases, int precision,
                       std::unique_ptr<SolverBase>& out) {

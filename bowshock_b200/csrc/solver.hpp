@@ -91,7 +91,15 @@ class SolverBase {
   // Polls each bounded wait of later LU-SGS sweeps makes before it gives up
   // (-1: the default bound); the drain after a give-up keeps the default.
   virtual bs_status set_sweep_wait_limit(int polls) = 0;
+  // The residual pass's tile shape (bsd::tile_shape index, -1 the default),
+  // which autotune also chooses.
+  virtual bs_status set_tile_shape(int shape) = 0;
+  virtual int tile_shape() const = 0;
 };
+
+// Cells along i and j and threads of a residual-pass tile shape (-1: the
+// default shape).
+void tile_dims(int shape, int32_t* ti, int32_t* tj, int32_t* threads);
 
 // precision: 64 (FP64 state and residual, FP32 LU-SGS operator) or 32 (all FP32).
 bs_status make_solver(std::vector<HostCase>&& cases, int precision,

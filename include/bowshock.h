@@ -399,6 +399,19 @@ BS_API bs_status bs_batch_solve(bs_batch *batch, int32_t method, double cfl, dou
 BS_API bs_status bs_batch_set_anderson(bs_batch *batch, int32_t depth, int32_t plain_steps);
 /* As bs_engine_set_metric_precision, for every case of the batch. */
 BS_API bs_status bs_batch_set_metric_precision(bs_batch *batch, int32_t bits);
+/* The tile shape of the batch's residual passes and explicit stages: -1 the
+ * default (16 x 15 cells on 256 threads, four resident CTAs asked for on
+ * launches of four waves or more), 0 .. 4 the autotuner's choices (16 x 15
+ * with one or four resident CTAs asked for, 16 x 7 and 8 x 15 on 128
+ * threads, 24 x 15 on 384). Every shape computes the same residual, cell
+ * for cell; bs_batch_autotune picks the fastest. FP32 batches keep -1. No
+ * counterpart in the reference (its passes are one dispatch per face
+ * direction, src/engine-gpu/shaders/euler2d.wgsl:316-367). */
+BS_API bs_status bs_batch_set_tile_shape(bs_batch *batch, int32_t shape);
+/* The batch's lanes and tile shape as set or tuned, with the shape's cells
+ * along i and j and its threads. */
+BS_API bs_status bs_batch_tuning(bs_batch *batch, int32_t *lanes, int32_t *shape, int32_t *tile_i,
+                                 int32_t *tile_j, int32_t *threads);
 /* As bs_engine_set_sweep_wait_limit, for the batch's later LU-SGS sweeps; a
  * solve reports a case whose sweep gave up as BS_EXECUTION in its result. */
 BS_API bs_status bs_batch_set_sweep_wait_limit(bs_batch *batch, int32_t polls);

@@ -121,8 +121,9 @@ def _layer_errors(net, g, ref):
     return errs
 
 
-def test_network_gradients_match_float64_reference():
-    net = WarmStartNet(hidden_layers=3, batch=256, seed=3)
+@pytest.mark.parametrize("hidden_layers", [3, 5])  # 5: the warm start's own network
+def test_network_gradients_match_float64_reference(hidden_layers):
+    net = WarmStartNet(hidden_layers=hidden_layers, batch=256, seed=3)
     samples, targets = _samples(200, 1)
     params = net.params()
     loss, grads = net.loss_grad(samples, targets)

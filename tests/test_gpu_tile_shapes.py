@@ -1,0 +1,67 @@
+"""Every tile shape of the residual pass computes the same steps.
+
+The autotuner picks the tile shape the residual pass and the explicit stages
+run with (bs_batch_set_tile_shape); the shape only decides which CTA
+computes which cell, so the state after any number of steps must be the
+same bit for bit whatever the shape, on grids whose sizes are multiples of
+no tile size and in a batch of uneven cases.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from bowshock_b200.batch import CudaBatch
+from bowshock_b200.workloads import ogive_case
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [-1, 0, 1, 2, 3, 4]
+
+
+def cases():
+    return [ogive_case(2.2, 40, 20), ogive_case(1.7, 58, 27), ogive_case(3.1, 100, 45)]
+
+
+def states_after(shape: int, method: str) -> list[np.ndarray]:
+    cs = cases()
+    b = CudaBatch([c.config for c in cs], precision=64)
+    try:
+        b.set_tile_shape(shape)
+        t = b.tuning()
+        assert t["tile_shape"] == shape
+        b.set_free_stream()
+        if method == "lusgs":
+            # 40 steps: tolerance out of reach, so every case takes them all.
+            res = b.solve("lusgs", 1e-14, max_steps=40, check_every=20)
+            assert all(r.steps == 40 for r in res)
+        else:
+            b.iterate(30)
+        return [b.primitives(k) for k in range(len(cs))]
+    finally:
+        b.destroy()
+
+
+@pytest.mark.parametrize("method", ["lusgs", "explicit"])
+def test_every_tile_shape_takes_the_same_steps(method):
+    ref = states_after(-1, method)
+    for shape in SHAPES[1:]:
+        got = states_after(shape, method)
+        for a, b in zip(ref, got):
+            assert np.array_equal(a, b), (method, shape)
+
+
+def test_autotune_picks_a_shape_and_keeps_the_state():
+    cs = cases()
+    b = CudaBatch([c.config for c in cs], precision=64)
+    try:
+        b.set_free_stream()
+        b.solve("lusgs", 1e-14, max_steps=20, check_every=20)
+        before = [b.primitives(k) for k in range(len(cs))]
+        lanes, ms = b.autotune("lusgs", 10)
+        t = b.tuning()
+        assert t["lanes"] == lanes and -1 <= t["tile_shape"] < 5 and ms > 0
+        for k in range(len(cs)):
+            assert np.array_equal(b.primitives(k), before[k])
+    finally:
+        b.destroy()
