@@ -18,6 +18,7 @@ FP64 engine (the oracle) on the host cores instead.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -41,15 +42,23 @@ MAX_STEPS = 20000
 CHECK_EVERY = 20
 # Algorithmic bytes per cell of each LU-SGS kernel launch: every array
 # element a pass reads or writes, counted once (FP64 state, FP32 sweep
-# records, float4 face metrics), halo re-reads not counted.
-#   residual pass: state 32 + i-face 16 + j-face 16 + cell 8
-#                  + sweep record 80 (residual, state, u/v/p/(1/D), 2 faces) = 152
+# records, float4 face metrics), halo re-reads and the records' padding and
+# ghost rows not counted.
+#   residual pass, with the previous step's update applied as it reads:
+#                  state 32 + dQ 16 + i-face 16 + j-face 16 + cell 8
+#                  + updated state 32 + forward record 80 (residual, state,
+#                  u/v/p/(1/D), west and south faces) + backward record 64
+#                  (state, u/v/p/(1/D), east and north faces) = 264
 #   sweeps: forward  record 80 + dQ* 16 = 96
-#           backward record 80 + dQ* 16 + dQ 16 = 112
-#   update: state 32 + dQ 16 + state 32 = 80
-BYTES_PREPARE = 152
-BYTES_SWEEP = 208
+#           backward record 80 (dQ*, state, u/v/p/(1/D), 2 faces) + dQ 16 = 96
+#   closing update, once per run of up to 16 steps: state 32 + dQ 16 + state 32 = 80
+BYTES_PREPARE = 264
+BYTES_SWEEP = 192
 BYTES_UPDATE = 80
+# FP64 operations per cell of the residual pass (DADD + DMUL + 2 DFMA,
+# thread instructions counted by ncu on the drag curve's residual pass,
+# divided by its cells; the summary in profiles/ names the capture).
+FLOPS_PREPARE = None
 
 
 def workload_config() -> dict:
@@ -258,9 +267,10 @@ def run_gpu(args, world, rank, local) -> None:
     cases = drag_sweep_cases()
     n = len(cases)
     batch = CudaBatch([c.config for c in cases], precision=64)
-    # Setup, untimed: the autotuner picks the number of lanes.
+    # Setup, untimed: the autotuner picks the number of lanes and the tile shape.
     batch.set_free_stream()
-    lanes, _ = batch.autotune("lusgs", 40, CFL, OMEGA)
+    batch.autotune("lusgs", 40, CFL, OMEGA)
+    tuning = batch.tuning()
     flush = torch.empty(512 * 2**20 // 4, dtype=torch.int32, device=f"cuda:{local}")
     start_fields = [np.tile(np.array([c.free.state.rho, c.free.state.u, c.free.state.v,
                                       c.free.state.p]), c.config.grid.ni * c.config.grid.nj)
@@ -341,6 +351,19 @@ def run_gpu(args, world, rank, local) -> None:
     dominant = max(kernels, key=lambda k: kernels[k][0])
     kms, kbytes = kernels[dominant]
     achieved = kbytes / (kms / 1000) / 1e9
+    # The residual pass is FP64 arithmetic: its rate against the measured
+    # FP64 FMA rate of this GPU.
+    fp64 = None
+    rate = C.c_double()
+    rate_ms = C.c_double()
+    _native.check(lib.bs_fp64_fma_rate(200000, C.byref(rate), C.byref(rate_ms)), lib)
+    if FLOPS_PREPARE is not None:
+        tf = FLOPS_PREPARE * cells / (prep_ms / 1000) / 1e12
+        fp64 = {"kernel": "lusgs_prepare", "achieved_tflops": tf, "peak_tflops": rate.value,
+                "peak_source": "measured (bs_fp64_fma_rate)", "frac": tf / rate.value,
+                "flops_per_cell": FLOPS_PREPARE}
+    else:
+        fp64 = {"peak_tflops": rate.value, "peak_source": "measured (bs_fp64_fma_rate)"}
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
@@ -368,7 +391,7 @@ def run_gpu(args, world, rank, local) -> None:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": workload_config(), "tuning": {"lanes": lanes},
+            "data": "synthetic", "config": workload_config(), "tuning": tuning,
             "target": target,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -378,7 +401,8 @@ def run_gpu(args, world, rank, local) -> None:
                          "traffic": traffic,
                          "kernel_ms": {k: v[0] for k, v in kernels.items()},
                          "bytes_per_cell": {"lusgs_sweep": BYTES_SWEEP, "lusgs_prepare": BYTES_PREPARE,
-                                            "lusgs_update": BYTES_UPDATE}},
+                                            "lusgs_update": BYTES_UPDATE},
+                         "fp64": fp64},
             "cpu_baseline": cpu,
             "clocks": clock_info,
             "accuracy": {"converged": converged, "lusgs_steps": steps_taken,
@@ -429,7 +453,8 @@ def run_seeded(args) -> None:
     cells = [c.config.grid.ni * c.config.grid.nj for c in cases]
     batch = CudaBatch([c.config for c in cases], precision=64)
     batch.set_free_stream()
-    lanes, _ = batch.autotune("lusgs", 40, CFL, OMEGA)
+    batch.autotune("lusgs", 40, CFL, OMEGA)
+    tuning = batch.tuning()
     flush = torch.empty(512 * 2**20 // 4, dtype=torch.int32, device="cuda:0")
 
     def one_step():

@@ -73,7 +73,7 @@ class CudaBatch:
         self._call("bs_batch_set_metric_precision", int(bits))
 
     def set_tile_shape(self, shape: int) -> None:
-        """The residual pass's tile shape: -1 the default, 0 .. 4 the
+        """The residual pass's tile shape: -1 the default, 0 .. 6 the
         autotuner's choices (bs_batch_set_tile_shape)."""
         self._call("bs_batch_set_tile_shape", int(shape))
 

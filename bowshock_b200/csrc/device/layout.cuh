@@ -37,20 +37,24 @@ static_assert(TI * TJ <= TILE_THREADS, "a tile has at most one cell per thread")
 
 // Tile shapes the residual pass and the explicit stages can run with, the
 // autotuner's choices: TI x TJ cells on `threads` threads, `min_blocks`
-// resident CTAs asked of the compiler. Shape 0 is the default above with one
-// resident CTA asked for, shape 1 the same with four. Smaller tiles put more
-// CTAs on a case (more SMs on one case's pass, at more halo per cell); the
-// 24 x 15 tile reads the least halo (43 % of its cells against 52 %).
+// resident CTAs asked of the compiler. Shape 0 is the default above (about
+// two faces per thread) with one resident CTA asked for, shape 1 the same
+// with four. Shapes 2 to 4 give each thread about one face, which halves the
+// dependent FP64 work a thread does and so a CTA's latency (a case's pass on
+// idle SMs is latency-bound); shape 5 reads the least halo (43 % of its
+// cells against 52 %) and shape 6 puts twice as many CTAs on a case.
 struct TileShape {
   int ti, tj, threads, min_blocks;
 };
-constexpr int kTileShapes = 5;
+constexpr int kTileShapes = 7;
 __host__ __device__ constexpr TileShape tile_shape(int k) {
   return k == 0   ? TileShape{TI, TJ, TILE_THREADS, 1}
          : k == 1 ? TileShape{TI, TJ, TILE_THREADS, 4}
-         : k == 2 ? TileShape{16, 7, 128, 1}
-         : k == 3 ? TileShape{8, 15, 128, 1}
-                  : TileShape{24, 15, 384, 1};
+         : k == 2 ? TileShape{16, 15, 512, 1}
+         : k == 3 ? TileShape{8, 15, 256, 1}
+         : k == 4 ? TileShape{16, 7, 256, 1}
+         : k == 5 ? TileShape{24, 15, 384, 1}
+                  : TileShape{8, 15, 128, 1};
 }
 
 // Per-case status bits.

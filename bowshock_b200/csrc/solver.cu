@@ -1186,9 +1186,11 @@ class Solver final : public SolverBase {
         switch (rshape_) {
           case 0: bsd::tile_kernel<R, MODE, 1><<<n, bsd::TILE_THREADS, 0, lane.stream>>>(A); break;
           case 1: bsd::tile_kernel<R, MODE, 4><<<n, bsd::TILE_THREADS, 0, lane.stream>>>(A); break;
-          case 2: bsd::tile_kernel<R, MODE, 1, 16, 7, 128><<<n, 128, 0, lane.stream>>>(A); break;
-          case 3: bsd::tile_kernel<R, MODE, 1, 8, 15, 128><<<n, 128, 0, lane.stream>>>(A); break;
-          default: bsd::tile_kernel<R, MODE, 1, 24, 15, 384><<<n, 384, 0, lane.stream>>>(A); break;
+          case 2: bsd::tile_kernel<R, MODE, 1, 16, 15, 512><<<n, 512, 0, lane.stream>>>(A); break;
+          case 3: bsd::tile_kernel<R, MODE, 1, 8, 15, 256><<<n, 256, 0, lane.stream>>>(A); break;
+          case 4: bsd::tile_kernel<R, MODE, 1, 16, 7, 256><<<n, 256, 0, lane.stream>>>(A); break;
+          case 5: bsd::tile_kernel<R, MODE, 1, 24, 15, 384><<<n, 384, 0, lane.stream>>>(A); break;
+          default: bsd::tile_kernel<R, MODE, 1, 8, 15, 128><<<n, 128, 0, lane.stream>>>(A); break;
         }
       }
     }

@@ -401,9 +401,10 @@ BS_API bs_status bs_batch_set_anderson(bs_batch *batch, int32_t depth, int32_t p
 BS_API bs_status bs_batch_set_metric_precision(bs_batch *batch, int32_t bits);
 /* The tile shape of the batch's residual passes and explicit stages: -1 the
  * default (16 x 15 cells on 256 threads, four resident CTAs asked for on
- * launches of four waves or more), 0 .. 4 the autotuner's choices (16 x 15
- * with one or four resident CTAs asked for, 16 x 7 and 8 x 15 on 128
- * threads, 24 x 15 on 384). Every shape computes the same residual, cell
+ * launches of four waves or more), 0 .. 6 the autotuner's choices: 16 x 15
+ * on 256 threads with one or four resident CTAs asked for, 16 x 15 on 512,
+ * 8 x 15 and 16 x 7 on 256 (about one face per thread), 24 x 15 on 384 (the
+ * least halo), 8 x 15 on 128. Every shape computes the same residual, cell
  * for cell; bs_batch_autotune picks the fastest. FP32 batches keep -1. No
  * counterpart in the reference (its passes are one dispatch per face
  * direction, src/engine-gpu/shaders/euler2d.wgsl:316-367). */
