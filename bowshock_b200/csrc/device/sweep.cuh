@@ -395,8 +395,11 @@ static __global__ void __launch_bounds__(32 * kMaxSweepWarps) lusgs_sweep_kernel
         failed = true;
         break;
       }
-      // The neighbours' diagonal u = s was the last of its chunk: free it.
+      // The neighbours' diagonal u = s was the last of its chunk: free it,
+      // once every lane's reads of it are ordered before the copy that
+      // overwrites it.
       if (new_chunk && cc > 0) {
+        __syncwarp();
         released = pass * nch + cc;
         try_issue();
       }
