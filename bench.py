@@ -556,7 +556,9 @@ def run_warmstart(args) -> None:
     tr = train_on_solves(train, args.cells_per_case, args.train_steps, args.max_steps)
     net = tr.net
 
+    t0 = time.perf_counter()
     cold = solve_cases(held, max_steps=args.max_steps)
+    cold_wall_s = time.perf_counter() - t0
     good = [k for k, s in enumerate(cold.status) if s == 0]
     t0 = time.perf_counter()
     warm, fell_back = warm_solve(net, held, max_steps=args.max_steps)
@@ -575,6 +577,7 @@ def run_warmstart(args) -> None:
         "train": {"solve_device_ms": tr.solve_device_ms, "seconds": tr.seconds,
                   "loss_first": tr.loss_first, "loss_last": tr.loss_last},
         "cold": {"solves_per_s": len(good) / (cold.device_ms / 1000), "device_ms": cold.device_ms,
+                 "wall_s": cold_wall_s,
                  "steps_median": int(statistics.median([cold.steps[k] for k in good])),
                  "steps_total": int(sum(cold.steps[k] for k in good)),
                  "initial_residual_median": float(statistics.median([cold.initial_residual[k] for k in good]))},
