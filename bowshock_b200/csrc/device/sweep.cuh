@@ -32,6 +32,7 @@
 #pragma once
 
 #include <algorithm>
+#include <type_traits>
 
 #include "layout.cuh"
 
@@ -319,92 +320,85 @@ static __global__ void __launch_bounds__(32 * kMaxSweepWarps) lusgs_sweep_kernel
 
   const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
   const int j = 32 * w + le;
-  for (int pass = 0; pass < 2 && !failed; pass++) {
-    const bool fwd = pass == 0;
-    const float sgn = fwd ? -1.f : 1.f;
+  // One pass, its direction a compile-time constant. Steps go chunk by chunk
+  // (the chunk holding the lane's own diagonal u = s + 1), so a step needs
+  // no division: the neighbours' diagonal u - 1 is the element before (or,
+  // at a chunk's first step, the previous chunk's last; forward elements run
+  // up a buffer, backward ones down it).
+  auto run_pass = [&](auto direction) -> bool {
+    constexpr bool fwd = decltype(direction)::value;
+    constexpr int pass = fwd ? 0 : 1;
+    constexpr float sgn = fwd ? -1.f : 1.f;
     // Block rows: forward, own row l + 1 and the neighbour below at l (row 0
     // is the ghost of the previous warp's last row); backward, own row l and
     // the neighbour above at l + 1 (row `rows` is the ghost of the next
     // warp's first row).
     const int r_own = fwd ? le + 1 : le;
     const int r_nb = fwd ? le : le + 1;
-    // Slot row of pass index u in chunk cc, within its buffer.
-    auto elem = [&](int cc, int u) {
-      int u0, n;
-      chunk_span(cc, u0, n);
-      return fwd ? u - u0 : u0 + n - 1 - u;
-    };
-    auto buf_of = [&](int cc) { return wbuf + size_t((pass * nch + cc) % NB) * buf_stride; };
-    if (!wait_chunk(pass * nch)) {
-      failed = true;
-      break;
-    }
+    float4* ring_in = fwd ? ring_f_in : ring_b_in;
+    float4* ring_out = fwd ? ring_f_out : ring_b_out;
+    const bool edge_in_lane = fwd ? l == 0 : l == 31;
+    const bool edge_out_lane = fwd ? l == 31 : l == 0;
+    if (!wait_chunk(pass * nch)) return false;
     // The lane's previous cell (its neighbour along the row): state and dQ.
     float4 pq = make_float4(1.f, 0.f, 0.f, 1.f), pw = make_float4(0.f, 0.f, 1.f, 1.f), pd = zero;
-    for (int s = 0; s < nT - 1; s++) {
-      const int u = s + 1;
-      const int cc = u / K;
-      const bool new_chunk = u == cc * K;
-      if (new_chunk && !wait_chunk(pass * nch + cc)) {
-        failed = true;
-        break;
-      }
-      const int i = fwd ? s - l : nT - 2 - s - l;
-      const bool active = l < rows && i >= 0 && i < ni;
-      const float4* own = buf_of(cc) + size_t(elem(cc, u) * R1 + r_own) * REC_SIZE;
-      const int ccn = s / K;
-      const float4* nb = buf_of(ccn) + size_t(elem(ccn, s) * R1 + r_nb) * REC_SIZE;
-      const float4 base = own[REC_R], q = own[REC_Q], wv = own[REC_W], fa = own[REC_FA], fb = own[REC_FB];
-      const float4 nq = nb[REC_Q], nwv = nb[REC_W];
-      // dQ of the neighbour across rows, finished by the next lane on the
-      // previous step (or by the next warp, through the ring).
-      float4 dn = fwd ? shfl4_up(pd) : shfl4_down(pd);
-      bool ok = true;
-      if (fwd && l == 0) {
-        dn = zero;
-        if (active && ring_f_in != nullptr) ok = edge_get(ring_f_in, i, dn, A.wait_limit, abort_word);
-      } else if (!fwd && l == 31) {
-        dn = zero;
-        if (active && ring_b_in != nullptr) ok = edge_get(ring_b_in, i, dn, A.wait_limit, abort_word);
-      }
-      float4 sum = zero;
-      add_neighbour(sum, neighbour_term(pq, pw, fa, sgn), pd, gm1);
-      add_neighbour(sum, neighbour_term(nq, nwv, fb, sgn), dn, gm1);
-      const float inv_d = wv.w;
-      float4 dq;
-      if (fwd) {
-        dq = make_float4((base.x - sum.x) * inv_d, (base.y - sum.y) * inv_d, (base.z - sum.z) * inv_d,
-                         (base.w - sum.w) * inv_d);
-      } else {
-        dq = make_float4(base.x - sum.x * inv_d, base.y - sum.y * inv_d, base.z - sum.z * inv_d,
-                         base.w - sum.w * inv_d);
-      }
-      if (active) {
-        if (fwd) {
-          A.rec_b[REC_SIZE * (block + int64_t(i + le) * R1 + le) + REC_R] = dq;
-          if (l == 31 && ring_f_out != nullptr) ok = ok && edge_put(ring_f_out, i, dq, A.wait_limit, abort_word);
-        } else {
-          A.dq[cd.cell + i + int64_t(j) * ni] = dq;
-          if (l == 0 && ring_b_out != nullptr) ok = ok && edge_put(ring_b_out, i, dq, A.wait_limit, abort_word);
+    const float4* prev = nullptr;
+    for (int cc = 0; cc < nch; cc++) {
+      if (cc > 0 && !wait_chunk(pass * nch + cc)) return false;
+      const int u0 = cc * K, n = min(K, nT - u0);
+      const float4* cur = wbuf + size_t((pass * nch + cc) % NB) * buf_stride;
+      for (int u = max(1, u0); u < u0 + n; u++) {
+        const int s = u - 1;
+        const int e = fwd ? u - u0 : u0 + n - 1 - u;
+        const int i = fwd ? s - l : nT - 2 - s - l;
+        const bool active = l < rows && i >= 0 && i < ni;
+        const float4* own = cur + size_t(e * R1 + r_own) * REC_SIZE;
+        const float4* nb = u > u0 ? cur + size_t((fwd ? e - 1 : e + 1) * R1 + r_nb) * REC_SIZE
+                                  : prev + size_t((fwd ? K - 1 : 0) * R1 + r_nb) * REC_SIZE;
+        const float4 base = own[REC_R], q = own[REC_Q], wv = own[REC_W], fa = own[REC_FA], fb = own[REC_FB];
+        const float4 nq = nb[REC_Q], nwv = nb[REC_W];
+        // dQ of the neighbour across rows, finished by the next lane on the
+        // previous step (or by the next warp, through the ring).
+        float4 dn = fwd ? shfl4_up(pd) : shfl4_down(pd);
+        bool ok = true;
+        if (edge_in_lane) {
+          dn = zero;
+          if (active && ring_in != nullptr) ok = edge_get(ring_in, i, dn, A.wait_limit, abort_word);
         }
-        pq = q;
-        pw = wv;
-        pd = dq;
+        float4 sum = zero;
+        add_neighbour(sum, neighbour_term(pq, pw, fa, sgn), pd, gm1);
+        add_neighbour(sum, neighbour_term(nq, nwv, fb, sgn), dn, gm1);
+        const float inv_d = wv.w;
+        float4 dq;
+        if (fwd) {
+          dq = make_float4((base.x - sum.x) * inv_d, (base.y - sum.y) * inv_d, (base.z - sum.z) * inv_d,
+                           (base.w - sum.w) * inv_d);
+        } else {
+          dq = make_float4(base.x - sum.x * inv_d, base.y - sum.y * inv_d, base.z - sum.z * inv_d,
+                           base.w - sum.w * inv_d);
+        }
+        if (active) {
+          if (fwd)
+            A.rec_b[REC_SIZE * (block + int64_t(i + le) * R1 + le) + REC_R] = dq;
+          else
+            A.dq[cd.cell + i + int64_t(j) * ni] = dq;
+          if (edge_out_lane && ring_out != nullptr) ok = ok && edge_put(ring_out, i, dq, A.wait_limit, abort_word);
+          pq = q;
+          pw = wv;
+          pd = dq;
+        }
+        if (__any_sync(0xffffffffu, !ok)) return false;
+        // The neighbours' diagonal u - 1 was the last of the previous chunk:
+        // free it, once every lane's reads of it are ordered before the copy
+        // that overwrites it.
+        if (u == u0) {
+          __syncwarp();
+          released = pass * nch + cc;
+          try_issue();
+        }
       }
-      if (__any_sync(0xffffffffu, !ok)) {
-        failed = true;
-        break;
-      }
-      // The neighbours' diagonal u = s was the last of its chunk: free it,
-      // once every lane's reads of it are ordered before the copy that
-      // overwrites it.
-      if (new_chunk && cc > 0) {
-        __syncwarp();
-        released = pass * nch + cc;
-        try_issue();
-      }
+      prev = cur;
     }
-    if (failed) break;
     released = pass * nch + nch;
     if (fwd) {
       // dQ* written above is read by the backward pass's bulk copies.
@@ -413,7 +407,9 @@ static __global__ void __launch_bounds__(32 * kMaxSweepWarps) lusgs_sweep_kernel
       fwd_done = true;
     }
     try_issue();
-  }
+    return true;
+  };
+  failed = !run_pass(std::true_type{}) || !run_pass(std::false_type{});
   if (failed) {
     if (l == 0) {
       atomicExch(abort_word, 1);
