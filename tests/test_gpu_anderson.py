@@ -44,12 +44,15 @@ def test_accelerated_lusgs_reaches_the_explicit_drag():
     assert abs(cd / cd_ref - 1) < 1e-7
 
 
-def _oracle_anderson_run(case, depth=8, cfl=5.0, tol=1e-8, max_steps=4000, plain_steps=30):
+def _oracle_anderson_run(case, depth=8, cfl=5.0, tol=1e-8, max_steps=4000, plain_steps=30, start=None):
     """The oracle's LU-SGS steps accelerated by oracle.anderson, applied as
-    src/analysis/transonic-flow.ts:183-206 applies it; returns the oracle
-    and the steps taken."""
+    src/analysis/transonic-flow.ts:183-206 applies it, from the free stream
+    or from the primitives `start`; returns the oracle and the steps taken."""
     o = OracleEuler2D(case.config)
-    o.set_uniform(case.free.state)
+    if start is None:
+        o.set_uniform(case.free.state)
+    else:
+        o.set_primitives(start)
     a = AndersonMixing(4 * o.n_cells, depth)
     best, c, n = np.inf, 1.0, 0
     while n < max_steps:
@@ -84,7 +87,11 @@ def _oracle_anderson_steps(case):
 def test_cases_that_cycle_under_plain_steps_converge(seed):
     # Ellipsoid noses above Mach 4 on 40 x 20 cells: plain LU-SGS settles
     # into a cycle (residual 0.3-0.5 after thousands of steps, the oracle's
-    # too); accelerated, they converge.
+    # too); accelerated, they converge. Such a case can have more than one
+    # steady state, and the accelerated path (chaotic while the iteration
+    # cycles) may end on another one than the oracle's own path from the free
+    # stream: where the drags differ, the oracle's accelerated iteration
+    # started from the GPU's field must hold that field as its steady state.
     case = case_from(draw_nose_case(seed, levels=(0,)))
     with CudaBatch([case.config], precision=64) as b:
         b.set_free_stream()
@@ -93,13 +100,19 @@ def test_cases_that_cycle_under_plain_steps_converge(seed):
         b.set_anderson(8, 30)
         acc = b.solve("lusgs", 1e-8, max_steps=4000, cfl=5.0)[0]
         cd = b.forebody_drag(0, case.free, case.body.nose.base_radius)
+        field = b.primitives(0)
         restarts = b.anderson_restarts()
     assert plain.status != 0 and plain.residual > 1e-3
     assert acc.status == 0 and acc.residual < 1e-8
     assert restarts.shape == (1,) and restarts[0] >= 0
     r_oracle, cd_oracle = _oracle_anderson(case)
     assert r_oracle < 1e-8
-    assert abs(cd / cd_oracle - 1) < 1e-6
+    if abs(cd / cd_oracle - 1) >= 1e-6:
+        o, _ = _oracle_anderson_run(case, plain_steps=0, start=field.reshape(-1))
+        f = case.free
+        assert o.density_residual_norm() < 1e-8
+        cd_held = o.forebody_drag(f.pressure, f.dynamic_pressure, case.body.nose.base_radius)
+        assert abs(cd / cd_held - 1) < 1e-6, (cd, cd_held, cd_oracle)
 
 
 @pytest.mark.parametrize("mach", [1.5, 2.5])
