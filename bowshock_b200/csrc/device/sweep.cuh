@@ -143,22 +143,28 @@ __device__ __forceinline__ bool aborted(const int* abort_word) {
   return *reinterpret_cast<const volatile int*>(abort_word) != 0;
 }
 
-// Puts dQ of cell column i into its slot once the consumer has emptied it.
-// Each of the four words is checked, so a slot is taken only when the
-// consumer's emptying store has landed in full.
-__device__ __forceinline__ bool edge_put(float4* ring, int i, float4 d, int limit, const int* abort_word) {
+// Warp-collective handoffs of one column's dQ at a warp edge. Every lane of
+// the warp polls the slot with the same (broadcast) read, so the loop and its
+// outcome are the same in every lane and the warp never diverges; only the
+// edge lane (`me`) stores. Put: once all four words of the slot read empty
+// (the consumer's emptying store has landed in full), the edge lane stores
+// its dQ. Get: once none of the four words is empty, the edge lane takes the
+// dQ and empties the slot. False if the wait gave up (the limit, or another
+// warp's abort).
+__device__ __forceinline__ bool warp_edge_put(float4* ring, int i, float4 d, bool me, int limit,
+                                              const int* abort_word) {
   float4* s = ring + (i & (kEdgeRing - 1));
   for (int k = 0;; k++) {
     if (all_empty(lds_volatile_u4(s))) break;
     if (k >= limit || ((k & 63) == 63 && aborted(abort_word))) return false;
   }
-  sts_volatile_u4(s, make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z),
-                                __float_as_uint(d.w)));
+  if (me)
+    sts_volatile_u4(s, make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z),
+                                  __float_as_uint(d.w)));
   return true;
 }
-// Takes dQ of cell column i once all four words of the slot hold it, and
-// empties the slot.
-__device__ __forceinline__ bool edge_get(float4* ring, int i, float4& d, int limit, const int* abort_word) {
+__device__ __forceinline__ bool warp_edge_get(float4* ring, int i, float4& d, bool me, int limit,
+                                              const int* abort_word) {
   float4* s = ring + (i & (kEdgeRing - 1));
   uint4 v;
   for (int k = 0;; k++) {
@@ -166,8 +172,10 @@ __device__ __forceinline__ bool edge_get(float4* ring, int i, float4& d, int lim
     if (none_empty(v)) break;
     if (k >= limit || ((k & 63) == 63 && aborted(abort_word))) return false;
   }
-  sts_volatile_u4(s, make_uint4(kEdgeEmpty, kEdgeEmpty, kEdgeEmpty, kEdgeEmpty));
-  d = make_float4(__uint_as_float(v.x), __uint_as_float(v.y), __uint_as_float(v.z), __uint_as_float(v.w));
+  if (me) {
+    sts_volatile_u4(s, make_uint4(kEdgeEmpty, kEdgeEmpty, kEdgeEmpty, kEdgeEmpty));
+    d = make_float4(__uint_as_float(v.x), __uint_as_float(v.y), __uint_as_float(v.z), __uint_as_float(v.w));
+  }
   return true;
 }
 
@@ -351,20 +359,22 @@ static __global__ void __launch_bounds__(32 * kMaxSweepWarps) lusgs_sweep_kernel
         const int s = u - 1;
         const int e = fwd ? u - u0 : u0 + n - 1 - u;
         const int i = fwd ? s - l : nT - 2 - s - l;
-        const bool active = l < rows && i >= 0 && i < ni;
+        const bool active = (l < rows) & (i >= 0) & (i < ni);
         const float4* own = cur + size_t(e * R1 + r_own) * REC_SIZE;
         const float4* nb = u > u0 ? cur + size_t((fwd ? e - 1 : e + 1) * R1 + r_nb) * REC_SIZE
                                   : prev + size_t((fwd ? K - 1 : 0) * R1 + r_nb) * REC_SIZE;
         const float4 base = own[REC_R], q = own[REC_Q], wv = own[REC_W], fa = own[REC_FA], fb = own[REC_FB];
         const float4 nq = nb[REC_Q], nwv = nb[REC_W];
         // dQ of the neighbour across rows, finished by the next lane on the
-        // previous step (or by the next warp, through the ring).
+        // previous step, or, for the edge lane, by the other warp: taken from
+        // the ring when that lane's cell is on the grid (a warp-uniform test).
         float4 dn = fwd ? shfl4_up(pd) : shfl4_down(pd);
+        dn = edge_in_lane ? zero : dn;
+        const int i_in = fwd ? s : nT - 2 - s - 31;    // the edge-in lane's column
+        const int i_out = fwd ? s - 31 : nT - 2 - s;   // the edge-out lane's column
         bool ok = true;
-        if (edge_in_lane) {
-          dn = zero;
-          if (active && ring_in != nullptr) ok = edge_get(ring_in, i, dn, A.wait_limit, abort_word);
-        }
+        if (ring_in != nullptr && i_in >= 0 && i_in < ni)
+          ok = warp_edge_get(ring_in, i_in, dn, edge_in_lane, A.wait_limit, abort_word);
         float4 sum = zero;
         add_neighbour(sum, neighbour_term(pq, pw, fa, sgn), pd, gm1);
         add_neighbour(sum, neighbour_term(nq, nwv, fb, sgn), dn, gm1);
@@ -382,12 +392,13 @@ static __global__ void __launch_bounds__(32 * kMaxSweepWarps) lusgs_sweep_kernel
             A.rec_b[REC_SIZE * (block + int64_t(i + le) * R1 + le) + REC_R] = dq;
           else
             A.dq[cd.cell + i + int64_t(j) * ni] = dq;
-          if (edge_out_lane && ring_out != nullptr) ok = ok && edge_put(ring_out, i, dq, A.wait_limit, abort_word);
-          pq = q;
-          pw = wv;
-          pd = dq;
         }
-        if (__any_sync(0xffffffffu, !ok)) return false;
+        if (ok && ring_out != nullptr && i_out >= 0 && i_out < ni)
+          ok = warp_edge_put(ring_out, i_out, dq, edge_out_lane, A.wait_limit, abort_word);
+        pq = active ? q : pq;
+        pw = active ? wv : pw;
+        pd = active ? dq : pd;
+        if (!ok) return false;  // the same in every lane
         // The neighbours' diagonal u - 1 was the last of the previous chunk:
         // free it, once every lane's reads of it are ordered before the copy
         // that overwrites it.
