@@ -42,15 +42,15 @@ MAX_STEPS = 20000
 CHECK_EVERY = 20
 # Algorithmic bytes per cell of each LU-SGS kernel launch: every array
 # element a pass reads or writes, counted once (FP64 state, FP32 sweep
-# records, float4 face metrics), halo re-reads and the records' padding and
-# ghost rows not counted.
+# records, float4 face metrics), halo re-reads not counted (the records hold
+# one slot per cell, no padding).
 #   residual pass, with the previous step's update applied as it reads:
 #                  state 32 + dQ 16 + i-face 16 + j-face 16 + cell 8
-#                  + updated state 32 + forward record 80 (residual, state,
-#                  u/v/p/(1/D), west and south faces) + backward record 64
-#                  (state, u/v/p/(1/D), east and north faces) = 264
+#                  + updated state 32 + forward record 80 (residual, 1/D,
+#                  west and south neighbour terms) + backward record 64
+#                  (1/D, east and north neighbour terms) = 264
 #   sweeps: forward  record 80 + dQ* 16 = 96
-#           backward record 80 (dQ*, state, u/v/p/(1/D), 2 faces) + dQ 16 = 96
+#           backward record 80 (dQ*, 1/D, two neighbour terms) + dQ 16 = 96
 #   closing update, once per run of up to 16 steps: state 32 + dQ 16 + state 32 = 80
 BYTES_PREPARE = 264
 BYTES_SWEEP = 192

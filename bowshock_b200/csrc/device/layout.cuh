@@ -6,10 +6,9 @@
 //   i-faces    float4 (nx, ny, area, 0), (ni + 1) nj at `iface`;
 //   j-faces    float4 (nx, ny, area, 0), ni (nj + 1) at `jface`;
 //   cells      float2 (volume, planar area) at `cell`;
-//   LU-SGS     per-cell sweep records, one block per warp of 32 rows in
-//              diagonal-major order (sweep_block_slot), sweep_slots(ni, nj)
-//              slots at `slot`; the final correction dQ is row-major like
-//              the state.
+//   LU-SGS     per-cell sweep records in anti-diagonal order (sweep_slot),
+//              ni nj slots at `slot`; the final correction dQ is row-major
+//              like the state.
 // Metrics are computed in FP64 on the host and stored as FP32; with the
 // two-float metrics on, also each value's FP32 low part (the FP64 value less
 // the FP32 one), which the residual adds back (about 48 bits). The state is
@@ -62,40 +61,36 @@ constexpr unsigned STATUS_NON_PHYSICAL = 1u;
 // A kernel gave up waiting for an asynchronous copy (bounded wait).
 constexpr unsigned STATUS_TIMEOUT = 2u;
 
-// LU-SGS sweep records. The rows of a case are cut into warps of 32 (the
-// last may hold fewer); warp w owns rows 32 w .. 32 w + rows - 1 and a block
-// of records of ni + rows diagonals by rows + 1 record rows, diagonal-major,
-// so that any run of diagonals is one contiguous range that a single bulk
-// copy brings into shared memory. Record row r of block diagonal t holds
-// cell (t - r, 32 w + r - 1) in the forward records (row 0 is a ghost: the
-// previous warp's last row) and cell (t - r, 32 w + r) in the backward
-// records (row `rows` is a ghost: the next warp's first row).
-__host__ __device__ __forceinline__ int sweep_warps(int nj) { return (nj + 31) / 32; }
-__host__ __device__ __forceinline__ int sweep_rows(int nj, int w) {
-  return nj - 32 * w < 32 ? nj - 32 * w : 32;
+// LU-SGS sweep records: one per cell and direction, stored by anti-diagonal
+// d = i + j (the order the sweeps visit them) and along a diagonal by row j,
+// with no slot for cells off the grid, so that any run of diagonals is one
+// contiguous range that a single bulk copy brings into shared memory and a
+// case has exactly ni nj slots. Diagonal d holds rows max(0, d - ni + 1) ..
+// min(d, nj - 1) and starts after diag_cells(ni, nj, d) slots: the diagonals
+// before it have min(k + 1, ni, nj, ni + nj - 1 - k) cells each, which sums
+// to T(d) - T(d - min) - T(d - max) with T(x) = x (x + 1) / 2 for x > 0.
+// 32-bit: the sweep launch requires ni + nj <= 65536 (so x (x + 1) < 2^32).
+__host__ __device__ __forceinline__ unsigned diag_cells(int ni, int nj, int d) {
+  const int a = ni < nj ? ni : nj, b = ni < nj ? nj : ni;
+  const unsigned x = unsigned(d), xa = unsigned(d > a ? d - a : 0), xb = unsigned(d > b ? d - b : 0);
+  return ((x * (x + 1)) >> 1) - ((xa * (xa + 1)) >> 1) - ((xb * (xb + 1)) >> 1);
 }
-// First slot of warp w's block (the warps before it are full).
-__host__ __device__ __forceinline__ int64_t sweep_block_base(int ni, int w) {
-  return int64_t(w) * (ni + 32) * 33;
-}
-// Slot of record row r for column i in warp w's block.
-__host__ __device__ __forceinline__ int64_t sweep_block_slot(int ni, int nj, int w, int i, int r) {
-  const int rows = sweep_rows(nj, w);
-  return sweep_block_base(ni, w) + int64_t(i + r) * (rows + 1) + r;
+// Slot of cell (i, j) within its case's records.
+__host__ __device__ __forceinline__ int64_t sweep_slot(int ni, int nj, int i, int j) {
+  const int d = i + j;
+  return int64_t(diag_cells(ni, nj, d)) + (j - (d - ni + 1 > 0 ? d - ni + 1 : 0));
 }
 // Slots of a case's records.
-__host__ __device__ __forceinline__ int64_t sweep_slots(int ni, int nj) {
-  const int last = sweep_warps(nj) - 1;
-  const int rows = sweep_rows(nj, last);
-  return sweep_block_base(ni, last) + int64_t(ni + rows) * (rows + 1);
-}
+__host__ __device__ __forceinline__ int64_t sweep_slots(int ni, int nj) { return int64_t(ni) * nj; }
+// float4 fields of a record (listed with the sweep kernel).
+constexpr int REC_SIZE = 5;
 
 struct CaseDev {
   int32_t ni, nj;
   int64_t cell;   // offset of the case's cell arrays
   int64_t iface;  // offset of its i-face arrays
   int64_t jface;  // offset of its j-face arrays
-  int64_t slot;   // offset of its LU-SGS sweep records, sweep_slots(ni, nj) slots
+  int64_t slot;   // offset of its LU-SGS sweep records, sweep_slots(ni, nj) = ni nj slots
   int32_t bc[4];  // bs_bc_kind per side
   int32_t flux, limiter, recon, axisym;
   int32_t integrator, local_dt;

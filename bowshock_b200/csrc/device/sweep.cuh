@@ -5,24 +5,25 @@
 // The forward sweep solves (D + L) dQ* = R cell by cell in the order j, then
 // i; cell (i, j) needs only (i - 1, j) and (i, j - 1), both on the previous
 // anti-diagonal, so the sweep is ni + nj - 1 dependent steps. One CTA owns a
-// case and thread j owns grid row j; the rows are cut into warps of 32, and
-// the warps run decoupled, with no CTA-wide barrier in the sweeps:
-//   - a warp walks its own rows' cells diagonal by diagonal; the neighbour
-//     along the row is the lane's own previous cell (registers), the
-//     neighbour across rows is the next lane's previous cell: its dQ by warp
-//     shuffle, its state from the records in shared memory;
-//   - at a warp edge the neighbour row belongs to the next warp: its state
-//     is a ghost row of this warp's records (the residual pass writes that
-//     row's records twice), and its dQ arrives through a small ring of
-//     shared-memory slots, one per cell column, that the producing lane
-//     fills and the consuming lane empties (a slot holds a NaN sentinel
-//     while empty, so one 16-byte slot is both the flag and the data);
-//   - each warp stages its own records into shared memory by TMA bulk
-//     copies, a chunk of diagonals at a time, with a ring of chunk buffers
-//     whose mbarriers only that warp waits on.
-// The warps of a case therefore form a pipeline whose rate is one warp's
-// step, not a CTA barrier's. Every wait is bounded: a wait that gives up sets
-// STATUS_TIMEOUT and the kernel drains its copies and leaves.
+// case; thread j of its consumer warps owns grid row j and walks it one
+// diagonal per step:
+//   - its neighbour along the row is the cell it finished on the previous
+//     step (registers); its neighbour across rows is the one the next lane
+//     finished, by warp shuffle, or at a warp edge through a two-slot
+//     exchange in shared memory, ordered by one named barrier per step among
+//     the consumer warps (a case of up to 32 rows has no barrier at all);
+//   - everything a step needs that does not depend on dQ - the residual (or
+//     dQ*), 1/D and the constants of the two neighbour terms - is one
+//     80-byte record per cell that the residual pass wrote, stored by
+//     anti-diagonal (sweep_slot) so that a run of diagonals is one
+//     contiguous range;
+//   - a producer warp stages those ranges into shared memory by TMA bulk
+//     copies, K diagonals at a time into a ring of buffers with full and
+//     empty mbarriers, so the consumers' steps carry no copy logic: the K
+//     steps of a chunk are unrolled at compile time and have no branch.
+// Every wait is bounded: a consumer wait that gives up sets STATUS_TIMEOUT
+// (the case's state is then left alone), and the producer lets every copy it
+// issued land (bounded) before the CTA leaves.
 //
 // The operator runs in FP32. The neighbour term is the change of the
 // physical flux, F(Q + dQ) - F(Q), exactly as the reference forms it, but
@@ -42,7 +43,7 @@ struct SweepArgs {
   const CaseDev* cases;
   const int* case_list;   // blockIdx.x -> case
   const int* active;      // per case (may be null)
-  const float4* rec_f;    // forward records (sweep_block_slot layout, 5 float4 per slot)
+  const float4* rec_f;    // forward records (sweep_slot order, REC_SIZE float4 each)
   float4* rec_b;          // backward records; the forward sweep writes dQ* into field 0
   float4* dq;             // final dQ, one float4 per cell at the case's cell offset (row-major)
   float* cfl;             // per case current CFL number (ramped after the sweep)
@@ -50,24 +51,28 @@ struct SweepArgs {
   const float* growth;    // per case
   const float* omega;     // per case
   unsigned* status;       // per case
-  int chunk;              // diagonals per bulk copy (K)
-  int buffers;            // chunk buffers per warp (NB, 2..kMaxSweepBuffers)
-  int wait_limit;         // polls before a wait gives up
-  int drain_limit;        // polls per copy when draining after a failure
+  int buffers;            // chunk buffers (NB, 2..kMaxSweepBuffers)
+  int wait_limit;         // polls before a consumer's wait gives up
+  int drain_limit;        // polls per copy for the producer's waits
 };
 
-// Fields of the records (five float4 per slot, written by the residual pass):
-//   forward:  residual | state | (u, v, p, 1/D) | west face | south face
-//   backward: dQ*      | state | (u, v, p, 1/D) | east face | north face
-// with each face as (nx, ny, A/2, omega lambda A / 2).
-enum { REC_R = 0, REC_Q = 1, REC_W = 2, REC_FA = 3, REC_FB = 4, REC_SIZE = 5 };
+// Fields of a record (five float4, written by the residual pass):
+//   0: residual (forward) / dQ* (backward, written by the forward sweep)
+//   1: (1/D, a.rho, a.u, a.v)     2: (a.H, a.hnx, a.hny, a.hud)
+//   3: (b.rho, b.u, b.v, b.H)     4: (b.hnx, b.hny, b.hud, 0)
+// for the neighbour along the row (a: west forward, east backward) and the
+// one across rows (b: south forward, north backward): its density,
+// velocity and total enthalpy per volume H = E + p, the face normal times
+// A/2 signed for the direction the flux leaves (-n forward, +n backward),
+// and hud = (u, v) . (hnx, hny) - omega lambda A/2. An absent neighbour has
+// (1, 0, 0, 0) and (0, 0, 0): with its zero correction it adds exactly
+// nothing. REC_SIZE (layout.cuh) is the record's five float4.
 
 constexpr int kMaxSweepWarps = 16;    // nj <= 512
-constexpr int kMaxSweepBuffers = 4;
-constexpr int kEdgeRing = 32;         // slots per warp-edge ring (a power of two)
-constexpr unsigned kEdgeEmpty = 0x7f80beefu;  // a NaN no arithmetic produces
-// Header: the warps' chunk mbarriers and the abort word.
-constexpr size_t kSweepHeader = 8 * kMaxSweepWarps * kMaxSweepBuffers + 128;
+constexpr int kMaxSweepBuffers = 8;
+// Header: full[8], empty[8] and the forward-done mbarrier, then the two
+// exchange rows of 16 float4.
+constexpr size_t kSweepHeader = 256 + 2 * 16 * 16;
 
 // ---- TMA bulk copies and mbarriers (sm_90 and later; no multicast) --------
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -119,117 +124,53 @@ __device__ __forceinline__ float approx_rcp(float x) {
   return r;
 }
 
-// ---- the warp-edge rings ----------------------------------------------------
-__device__ __forceinline__ uint4 lds_volatile_u4(const float4* p) {
-  uint4 v;
-  asm volatile("ld.volatile.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n"
-               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-               : "r"(smem_u32(p))
-               : "memory");
-  return v;
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
-__device__ __forceinline__ void sts_volatile_u4(float4* p, uint4 v) {
-  asm volatile("st.volatile.shared.v4.u32 [%0], {%1, %2, %3, %4};\n" ::"r"(smem_u32(p)), "r"(v.x),
-               "r"(v.y), "r"(v.z), "r"(v.w)
-               : "memory");
-}
-__device__ __forceinline__ bool all_empty(uint4 v) {
-  return v.x == kEdgeEmpty && v.y == kEdgeEmpty && v.z == kEdgeEmpty && v.w == kEdgeEmpty;
-}
-__device__ __forceinline__ bool none_empty(uint4 v) {
-  return v.x != kEdgeEmpty && v.y != kEdgeEmpty && v.z != kEdgeEmpty && v.w != kEdgeEmpty;
-}
-__device__ __forceinline__ bool aborted(const int* abort_word) {
-  return *reinterpret_cast<const volatile int*>(abort_word) != 0;
+// Barrier 1 among the consumer warps only (the producer warp never joins).
+__device__ __forceinline__ void consumer_sync(int threads) {
+  asm volatile("bar.sync 1, %0;\n" ::"r"(threads) : "memory");
 }
 
-// Warp-collective handoffs of one column's dQ at a warp edge. Every lane of
-// the warp polls the slot with the same (broadcast) read, so the loop and its
-// outcome are the same in every lane and the warp never diverges; only the
-// edge lane (`me`) stores. Put: once all four words of the slot read empty
-// (the consumer's emptying store has landed in full), the edge lane stores
-// its dQ. Get: once none of the four words is empty, the edge lane takes the
-// dQ and empties the slot. False if the wait gave up (the limit, or another
-// warp's abort).
-__device__ __forceinline__ bool warp_edge_put(float4* ring, int i, float4 d, bool me, int limit,
-                                              const int* abort_word) {
-  float4* s = ring + (i & (kEdgeRing - 1));
-  for (int k = 0;; k++) {
-    if (all_empty(lds_volatile_u4(s))) break;
-    if (k >= limit || ((k & 63) == 63 && aborted(abort_word))) return false;
-  }
-  if (me)
-    sts_volatile_u4(s, make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z),
-                                  __float_as_uint(d.w)));
-  return true;
-}
-__device__ __forceinline__ bool warp_edge_get(float4* ring, int i, float4& d, bool me, int limit,
-                                              const int* abort_word) {
-  float4* s = ring + (i & (kEdgeRing - 1));
-  uint4 v;
-  for (int k = 0;; k++) {
-    v = lds_volatile_u4(s);
-    if (none_empty(v)) break;
-    if (k >= limit || ((k & 63) == 63 && aborted(abort_word))) return false;
-  }
-  if (me) {
-    sts_volatile_u4(s, make_uint4(kEdgeEmpty, kEdgeEmpty, kEdgeEmpty, kEdgeEmpty));
-    d = make_float4(__uint_as_float(v.x), __uint_as_float(v.y), __uint_as_float(v.z), __uint_as_float(v.w));
-  }
-  return true;
-}
-
-// Shared memory of the sweep for cases of up to `nj` rows, chunks of `chunk`
-// diagonals and `buffers` chunk buffers per warp: the header, two rings per
-// warp edge and the warps' chunk buffers (a warp of `rows` rows holds
-// rows + 1 record rows per diagonal).
-__host__ __device__ inline size_t sweep_smem_bytes(int nj, int chunk, int buffers) {
-  const int nw = sweep_warps(nj);
-  const size_t rows_sum = size_t(nj) + nw;
-  return kSweepHeader + 2 * size_t(nw - 1) * kEdgeRing * 16 + size_t(buffers) * chunk * rows_sum * 16 * REC_SIZE;
-}
-
-// The d-independent part of a neighbour's term: its state, the face normal
-// (signed for the direction the flux leaves), A/2, omega lambda A/2, its
-// normal velocity and the momentum and kinetic-energy weights of dK.
-struct NeighbourTerm {
-  float4 q;
-  float nx, ny, half_area, damp, un, ku, kv, kk, p;
-};
-
-__device__ __forceinline__ NeighbourTerm neighbour_term(const float4 q, const float4 w, const float4 f,
-                                                        float sgn) {
-  NeighbourTerm t;
-  t.q = q;
-  t.nx = sgn * f.x;
-  t.ny = sgn * f.y;
-  t.half_area = f.z;
-  t.damp = f.w;
-  t.un = w.x * t.nx + w.y * t.ny;
-  t.ku = q.x * w.x;
-  t.kv = q.x * w.y;
-  t.kk = q.x * (0.5f * (w.x * w.x + w.y * w.y));
-  t.p = w.z;
-  return t;
+// Shared memory of the sweep for chunks of `chunk` diagonals of up to
+// `max_len` cells (the longest diagonal, min(ni, nj), of the launch's cases)
+// in `buffers` buffers.
+__host__ __device__ inline size_t sweep_smem_bytes(int max_len, int chunk, int buffers) {
+  return kSweepHeader + size_t(buffers) * chunk * max_len * 16 * REC_SIZE;
 }
 
 // The neighbour term of src/engine-cpu/euler2d.ts:977-1005 - the change of
 // the physical flux across the face, F(Q + d) - F(Q), times A/2, less
-// omega lambda A/2 d - added to `sum`. The exact difference is written so
-// that every term is proportional to d (no difference of two O(|F|)
-// numbers), so FP32 rounding is relative to the term and d = 0 adds exactly
-// nothing, which stands for an absent neighbour.
-__device__ __forceinline__ void add_neighbour(float4& sum, const NeighbourTerm& t, const float4 d,
-                                              float gm1) {
-  const float inv1 = approx_rcp(t.q.x + d.x);
-  const float dmn = d.y * t.nx + d.z * t.ny;
-  const float dun = (dmn - t.un * d.x) * inv1;
-  const float dk = (t.ku * d.y + t.kv * d.z - t.kk * d.x + 0.5f * (d.y * d.y + d.z * d.z)) * inv1;
-  const float dp = gm1 * (d.w - dk);
-  sum.x += t.half_area * dmn - t.damp * d.x;
-  sum.y += t.half_area * (d.y * t.un + (t.q.y + d.y) * dun + dp * t.nx) - t.damp * d.y;
-  sum.z += t.half_area * (d.z * t.un + (t.q.z + d.z) * dun + dp * t.ny) - t.damp * d.z;
-  sum.w += t.half_area * ((d.w + dp) * t.un + (t.q.w + d.w + t.p + dp) * dun) - t.damp * d.w;
+// omega lambda A/2 d - added to `sum`, for a neighbour stored as (rho, u, v,
+// H) and (hnx, hny, hud). With m = rho (u, v), hun = (u, v) . (hnx, hny):
+//   dK = (m . d_m - |m|^2/rho d_rho + |d_m|^2 / 2) / (rho + d_rho),
+//   dp = (gamma - 1) (d_E - dK),
+//   d(A/2 rho u_n) = hdmn = d_m . (hnx, hny),
+//   A/2 d(u_n) = hdun = (hdmn - hun d_rho) / (rho + d_rho),
+// and the term is (hdmn, d_m hun + (m + d_m) hdun + dp (hnx, hny),
+// (d_E + dp) hun + (H + d_E + dp) hdun) - damp d, the damping folded into
+// hud = hun - damp. Every term is proportional to d (no difference of two
+// O(|F|) numbers), so FP32 rounding is relative to the term and d = 0 adds
+// exactly nothing.
+__device__ __forceinline__ void add_neighbour(float4& sum, float rho, float u, float v, float H, float hnx,
+                                              float hny, float hud, const float4 d, float gm1, float hg) {
+  const float mx = rho * u, my = rho * v;
+  const float hun = hnx * u + hny * v;
+  const float kk2 = mx * u + my * v;  // |m|^2 / rho
+  const float inv1 = approx_rcp(rho + d.x);
+  const float hdmn = d.y * hnx + d.z * hny;
+  const float X = hdmn - hun * d.x;
+  const float hdun = X * inv1;
+  // 2 dK (rho + d_rho) = d_mx (2 mx + d_mx) + d_my (2 my + d_my) - kk2 d_rho
+  float s = d.y * fmaf(2.f, mx, d.y);
+  s = fmaf(d.z, fmaf(2.f, my, d.z), s);
+  s = fmaf(-kk2, d.x, s);
+  const float dp = fmaf(-hg, s * inv1, gm1 * d.w);  // hg = (gamma - 1) / 2
+  sum.x += fmaf(hud, d.x, X);
+  sum.y += fmaf(d.y, hud, fmaf(mx + d.y, hdun, dp * hnx));
+  sum.z += fmaf(d.z, hud, fmaf(my + d.z, hdun, dp * hny));
+  sum.w += fmaf(d.w, hud, fmaf(dp, hun, (H + d.w + dp) * hdun));
 }
 
 __device__ __forceinline__ float4 shfl4_up(float4 v) {
@@ -241,193 +182,167 @@ __device__ __forceinline__ float4 shfl4_down(float4 v) {
                      __shfl_down_sync(0xffffffffu, v.z, 1), __shfl_down_sync(0xffffffffu, v.w, 1));
 }
 
-// The forward and backward sweeps of every active case, one CTA per case and
-// one warp per 32 rows, leaving the final correction dQ in A.dq (row-major).
+// The forward and backward sweeps of every active case, one CTA per case,
+// leaving the final correction dQ in A.dq (row-major). The CTA has
+// kWarps + 1 warps for the launch's widest case: warps 0 .. W - 1 sweep the
+// case's W = ceil(nj / 32) warps of rows, the last warp issues the copies,
+// and the ones between (for narrower cases) leave at once.
 //
-// Indexing: a warp of `rows` rows owns a block of records of nT = ni + rows
-// diagonals by rows + 1 record rows (sweep_block_slot). Each pass visits the
-// block's diagonals in the order of a pass index u = 0 .. nT - 1 (forward:
-// the block diagonal; backward: nT - 1 less it); step s = 0 .. nT - 2 works on
-// the lane's cell at u = s + 1, whose neighbours are at u = s. Chunk cc of a
-// pass holds u in [cc K, cc K + K); the pass's chunks are numbered on from the
-// previous pass's (g = pass nch + cc) and cycle through the warp's buffers.
-static __global__ void __launch_bounds__(32 * kMaxSweepWarps) lusgs_sweep_kernel(const SweepArgs A) {
+// Chunks: a pass's diagonals in sweep order, K per chunk (the last may hold
+// fewer); chunk g of the sequence (forward chunks, then backward ones) goes
+// to buffer g % NB. Each chunk is one contiguous range of records: forward
+// chunk cc holds diagonals [cc K, cc K + n), backward chunk cc the n
+// diagonals ending at ndiag - cc K, both in memory order, the backward pass
+// visiting its chunk from the top down.
+template <int K, bool SOLO>
+static __global__ void __launch_bounds__(32 * (kMaxSweepWarps + 1), 1) lusgs_sweep_kernel(const SweepArgs A) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int c = A.case_list[blockIdx.x];
   if (A.active != nullptr && A.active[c] == 0) return;
   const CaseDev& cd = A.cases[c];
   const int ni = cd.ni, nj = cd.nj;
-  const int nw = sweep_warps(nj);
-  const int w = threadIdx.x >> 5;
-  const int l = threadIdx.x & 31;
-  const int K = A.chunk, NB = A.buffers;
-  const float gm1 = float(cd.gamma) - 1.f;
-
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);  // [kMaxSweepWarps][kMaxSweepBuffers]
-  int* abort_word = reinterpret_cast<int*>(smem_raw + 8 * kMaxSweepWarps * kMaxSweepBuffers);
-  float4* rings = reinterpret_cast<float4*>(smem_raw + kSweepHeader);  // [2][nw - 1][kEdgeRing]
-  float4* bufs = rings + 2 * (nw - 1) * kEdgeRing;
-  const int n_ring_words = 2 * (nw - 1) * kEdgeRing;
-  for (int k = threadIdx.x; k < n_ring_words; k += blockDim.x)
-    sts_volatile_u4(rings + k, make_uint4(kEdgeEmpty, kEdgeEmpty, kEdgeEmpty, kEdgeEmpty));
+  const int P = (blockDim.x >> 5) - 1;  // the producer warp
+  const int W = SOLO ? 1 : (nj + 31) >> 5;
+  const int j = threadIdx.x, w = j >> 5, l = j & 31;
+  const int NB = A.buffers;
+  const int len_max = min(ni, nj);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);  // [kMaxSweepBuffers]
+  uint64_t* empty = full + kMaxSweepBuffers;                // [kMaxSweepBuffers]
+  uint64_t* fwd_done = empty + kMaxSweepBuffers;
+  float4* xch = reinterpret_cast<float4*>(smem_raw + 256);  // [2][16]
+  float4* bufs = reinterpret_cast<float4*>(smem_raw + kSweepHeader);
   if (threadIdx.x == 0) {
-    *abort_word = 0;
-    for (int b = 0; b < kMaxSweepWarps * kMaxSweepBuffers; b++) mbar_init(&bars[b], 1);
+    for (int b = 0; b < NB; b++) {
+      mbar_init(&full[b], 1);
+      mbar_init(&empty[b], W);
+    }
+    mbar_init(fwd_done, W);
     mbar_fence_init();
   }
   __syncthreads();
-  if (w >= nw) return;
+  const int ndiag = ni + nj - 1;
+  const int nch = (ndiag + K - 1) / K;
+  const int buf_stride = K * len_max * REC_SIZE;
 
-  const int rows = sweep_rows(nj, w);
-  const int R1 = rows + 1;
-  const int nT = ni + rows;
-  const int nch = (nT + K - 1) / K;
-  const int le = min(l, rows - 1);  // the lane's row for addressing (lanes past the rows idle)
-  uint64_t* full = bars + w * kMaxSweepBuffers;
-  // This warp's chunk buffers: the warps before it hold rows' + 1 rows each.
-  float4* wbuf = bufs + size_t(NB) * K * REC_SIZE * (size_t(32 * w) + w);
-  const size_t buf_stride = size_t(K) * R1 * REC_SIZE;
-  float4* ring_f_in = w > 0 ? rings + (w - 1) * kEdgeRing : nullptr;            // from warp w - 1
-  float4* ring_f_out = w < nw - 1 ? rings + w * kEdgeRing : nullptr;            // to warp w + 1
-  float4* ring_b_in = w < nw - 1 ? rings + (nw - 1 + w) * kEdgeRing : nullptr;  // from warp w + 1
-  float4* ring_b_out = w > 0 ? rings + (nw - 1 + w - 1) * kEdgeRing : nullptr;  // to warp w - 1
-  const int64_t block = cd.slot + sweep_block_base(ni, w);
-
-  // Copies: chunk g of the sequence (forward chunks, then backward ones).
-  auto chunk_span = [&](int cc, int& u0, int& n) {
-    u0 = cc * K;
-    n = min(K, nT - u0);
-  };
-  auto issue = [&](int g) {
-    const int pass = g / nch, cc = g - pass * nch;
-    int u0, n;
-    chunk_span(cc, u0, n);
-    const int t_lo = pass == 0 ? u0 : nT - u0 - n;  // block diagonal of the chunk's first slot row
-    const float4* src = (pass == 0 ? A.rec_f : A.rec_b) + REC_SIZE * (block + int64_t(t_lo) * R1);
-    const unsigned bytes = unsigned(n) * unsigned(R1) * 16u * REC_SIZE;
-    if (l == 0) {
-      uint64_t* bar = &full[g % NB];
-      mbar_arrive_expect_tx(bar, bytes);
-      bulk_load(wbuf + size_t(g % NB) * buf_stride, src, bytes, bar);
+  if (w == P) {
+    // Producer: one lane issues every chunk of both passes in order; a
+    // buffer is refilled once all W consumer warps have released it, and the
+    // backward chunks wait until the forward pass's dQ* is written.
+    if (l != 0) return;
+    const float4* src_f = A.rec_f + REC_SIZE * cd.slot;
+    const float4* src_b = A.rec_b + REC_SIZE * cd.slot;
+    int issued = 0;
+    for (int g = 0; g < 2 * nch; g++) {
+      const int b = g % NB;
+      if (g >= NB && !mbar_wait(&empty[b], unsigned(g / NB - 1) & 1u, A.drain_limit)) break;
+      if (g == nch) {
+        if (!mbar_wait(fwd_done, 0u, A.drain_limit)) break;
+        fence_proxy_async();
+      }
+      const int pass = g / nch, cc = g - pass * nch;
+      const int n = min(K, ndiag - cc * K);
+      const int dlo = pass == 0 ? cc * K : ndiag - cc * K - n;
+      const unsigned lo = diag_cells(ni, nj, dlo), hi = diag_cells(ni, nj, dlo + n);
+      const unsigned bytes = (hi - lo) * 16u * REC_SIZE;
+      mbar_arrive_expect_tx(&full[b], bytes);
+      bulk_load(bufs + size_t(b) * buf_stride, (pass == 0 ? src_f : src_b) + size_t(REC_SIZE) * lo, bytes, &full[b]);
+      issued = g + 1;
     }
-  };
-  int next = 0;      // next chunk to issue
-  int released = 0;  // chunks whose buffers are free again
-  int waited = 0;    // chunks waited for
-  bool fwd_done = false;
-  auto try_issue = [&]() {
-    while (next < 2 * nch && next < released + NB && (next < nch || fwd_done)) issue(next++);
-  };
-  bool failed = false;
-  auto wait_chunk = [&](int g) -> bool {
-    const bool ok = mbar_wait(&full[g % NB], unsigned(g / NB) & 1u, A.wait_limit);
-    if (ok) waited = g + 1;
-    return __all_sync(0xffffffffu, ok);
-  };
-  try_issue();
+    // The last NB copies issued are the only ones that can be in flight
+    // (each buffer holds one at a time): let them land before leaving.
+    for (int g = max(0, issued - NB); g < issued; g++)
+      mbar_wait(&full[g % NB], unsigned(g / NB) & 1u, A.drain_limit);
+    return;
+  }
+  if (w >= W) return;
 
+  const float gm1 = float(cd.gamma) - 1.f, hg = 0.5f * gm1;
+  float4* rec_b = A.rec_b + REC_SIZE * cd.slot;
+  float4* dq_case = A.dq + cd.cell;
   const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-  const int j = 32 * w + le;
-  // One pass, its direction a compile-time constant. Steps go chunk by chunk
-  // (the chunk holding the lane's own diagonal u = s + 1), so a step needs
-  // no division: the neighbours' diagonal u - 1 is the element before (or,
-  // at a chunk's first step, the previous chunk's last; forward elements run
-  // up a buffer, backward ones down it).
-  auto run_pass = [&](auto direction) -> bool {
+  bool failed = false;
+  auto run_pass = [&](auto direction) {
     constexpr bool fwd = decltype(direction)::value;
     constexpr int pass = fwd ? 0 : 1;
-    constexpr float sgn = fwd ? -1.f : 1.f;
-    // Block rows: forward, own row l + 1 and the neighbour below at l (row 0
-    // is the ghost of the previous warp's last row); backward, own row l and
-    // the neighbour above at l + 1 (row `rows` is the ghost of the next
-    // warp's first row).
-    const int r_own = fwd ? le + 1 : le;
-    const int r_nb = fwd ? le : le + 1;
-    float4* ring_in = fwd ? ring_f_in : ring_b_in;
-    float4* ring_out = fwd ? ring_f_out : ring_b_out;
-    const bool edge_in_lane = fwd ? l == 0 : l == 31;
-    const bool edge_out_lane = fwd ? l == 31 : l == 0;
-    if (!wait_chunk(pass * nch)) return false;
-    // The lane's previous cell (its neighbour along the row): state and dQ.
-    float4 pq = make_float4(1.f, 0.f, 0.f, 1.f), pw = make_float4(0.f, 0.f, 1.f, 1.f), pd = zero;
-    const float4* prev = nullptr;
+    // The row neighbour's lane is the one below (forward) / above (backward);
+    // the edge lane takes it from the neighbouring warp's exchange slot, and
+    // the first (last) row has none.
+    const bool edge_lane = fwd ? l == 0 : l == 31;
+    const bool edge_warp = fwd ? w == 0 : w == W - 1;
+    const int wn = fwd ? max(w - 1, 0) : min(w + 1, kMaxSweepWarps - 1);
+    float4 pd = zero;  // the lane's previous cell's dQ (zero before its row starts)
+    int t = 0;         // step of the pass (exchange parity)
     for (int cc = 0; cc < nch; cc++) {
-      if (cc > 0 && !wait_chunk(pass * nch + cc)) return false;
-      const int u0 = cc * K, n = min(K, nT - u0);
-      const float4* cur = wbuf + size_t((pass * nch + cc) % NB) * buf_stride;
-      for (int u = max(1, u0); u < u0 + n; u++) {
-        const int s = u - 1;
-        const int e = fwd ? u - u0 : u0 + n - 1 - u;
-        const int i = fwd ? s - l : nT - 2 - s - l;
-        const bool active = (l < rows) & (i >= 0) & (i < ni);
-        const float4* own = cur + size_t(e * R1 + r_own) * REC_SIZE;
-        const float4* nb = u > u0 ? cur + size_t((fwd ? e - 1 : e + 1) * R1 + r_nb) * REC_SIZE
-                                  : prev + size_t((fwd ? K - 1 : 0) * R1 + r_nb) * REC_SIZE;
-        const float4 base = own[REC_R], q = own[REC_Q], wv = own[REC_W], fa = own[REC_FA], fb = own[REC_FB];
-        const float4 nq = nb[REC_Q], nwv = nb[REC_W];
-        // dQ of the neighbour across rows, finished by the next lane on the
-        // previous step, or, for the edge lane, by the other warp: taken from
-        // the ring when that lane's cell is on the grid (a warp-uniform test).
-        float4 dn = fwd ? shfl4_up(pd) : shfl4_down(pd);
-        dn = edge_in_lane ? zero : dn;
-        const int i_in = fwd ? s : nT - 2 - s - 31;    // the edge-in lane's column
-        const int i_out = fwd ? s - 31 : nT - 2 - s;   // the edge-out lane's column
-        bool ok = true;
-        if (ring_in != nullptr && i_in >= 0 && i_in < ni)
-          ok = warp_edge_get(ring_in, i_in, dn, edge_in_lane, A.wait_limit, abort_word);
+      const int g = pass * nch + cc;
+      const int b = g % NB;
+      if (!failed) failed = !__all_sync(0xffffffffu, mbar_wait(&full[b], unsigned(g / NB) & 1u, A.wait_limit));
+      const int n = min(K, ndiag - cc * K);
+      const int dlo = fwd ? cc * K : ndiag - cc * K - n;
+      const unsigned off_lo = diag_cells(ni, nj, dlo);
+      int d = fwd ? dlo : dlo + n - 1;
+      int boff = fwd ? 0 : int(diag_cells(ni, nj, d) - off_lo);  // d's first record in the chunk
+      const float4* buf = bufs + b * buf_stride;
+#pragma unroll
+      for (int s = 0; s < K; s++) {
+        // Steps past the chunk's end (its last) repeat its last diagonal
+        // with nothing stored, so every warp meets the same barriers.
+        const bool live = s < n;
+        const int jlo = max(0, d - ni + 1), jhi = min(d, nj - 1);
+        const int e = min(max(j - jlo, 0), jhi - jlo);  // in-range for rows off the diagonal
+        const float4* r = buf + REC_SIZE * (boff + e);
+        const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
+        const float4 sh = fwd ? shfl4_up(pd) : shfl4_down(pd);
+        const float4 xv = SOLO ? zero : xch[((t & 1) ^ 1) * 16 + wn];
+        const float4 dn = edge_lane ? (edge_warp ? zero : xv) : sh;
         float4 sum = zero;
-        add_neighbour(sum, neighbour_term(pq, pw, fa, sgn), pd, gm1);
-        add_neighbour(sum, neighbour_term(nq, nwv, fb, sgn), dn, gm1);
-        const float inv_d = wv.w;
+        add_neighbour(sum, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, pd, gm1, hg);
+        add_neighbour(sum, r3.x, r3.y, r3.z, r3.w, r4.x, r4.y, r4.z, dn, gm1, hg);
+        const float inv_d = r1.x;
         float4 dq;
-        if (fwd) {
-          dq = make_float4((base.x - sum.x) * inv_d, (base.y - sum.y) * inv_d, (base.z - sum.z) * inv_d,
-                           (base.w - sum.w) * inv_d);
-        } else {
-          dq = make_float4(base.x - sum.x * inv_d, base.y - sum.y * inv_d, base.z - sum.z * inv_d,
-                           base.w - sum.w * inv_d);
-        }
+        if (fwd)
+          dq = make_float4((r0.x - sum.x) * inv_d, (r0.y - sum.y) * inv_d, (r0.z - sum.z) * inv_d,
+                           (r0.w - sum.w) * inv_d);
+        else
+          dq = make_float4(fmaf(-sum.x, inv_d, r0.x), fmaf(-sum.y, inv_d, r0.y), fmaf(-sum.z, inv_d, r0.z),
+                           fmaf(-sum.w, inv_d, r0.w));
+        const bool active = live & (j >= jlo) & (j <= jhi);
         if (active) {
           if (fwd)
-            A.rec_b[REC_SIZE * (block + int64_t(i + le) * R1 + le) + REC_R] = dq;
+            rec_b[size_t(REC_SIZE) * (off_lo + unsigned(boff + j - jlo))] = dq;
           else
-            A.dq[cd.cell + i + int64_t(j) * ni] = dq;
+            dq_case[unsigned(d - j) + unsigned(j) * unsigned(ni)] = dq;
         }
-        if (ok && ring_out != nullptr && i_out >= 0 && i_out < ni)
-          ok = warp_edge_put(ring_out, i_out, dq, edge_out_lane, A.wait_limit, abort_word);
-        pq = active ? q : pq;
-        pw = active ? wv : pw;
         pd = active ? dq : pd;
-        if (!ok) return false;  // the same in every lane
-        // The neighbours' diagonal u - 1 was the last of the previous chunk:
-        // free it, once every lane's reads of it are ordered before the copy
-        // that overwrites it.
-        if (u == u0) {
-          __syncwarp();
-          released = pass * nch + cc;
-          try_issue();
+        if (!SOLO) {
+          if (fwd ? l == 31 : l == 0) xch[(t & 1) * 16 + w] = pd;
+          consumer_sync(32 * W);
         }
+        if (s + 1 < n) {
+          if (fwd) {
+            boff += jhi - jlo + 1;
+            d++;
+          } else {
+            d--;
+            boff -= min(d, nj - 1) - max(0, d - ni + 1) + 1;
+          }
+        }
+        t++;
       }
-      prev = cur;
+      // Every lane's reads of the buffer are done: release it.
+      __syncwarp();
+      if (l == 0) mbar_arrive(&empty[b]);
     }
-    released = pass * nch + nch;
     if (fwd) {
       // dQ* written above is read by the backward pass's bulk copies.
       fence_proxy_async();
       __syncwarp();
-      fwd_done = true;
+      if (l == 0) mbar_arrive(fwd_done);
     }
-    try_issue();
-    return true;
   };
-  failed = !run_pass(std::true_type{}) || !run_pass(std::false_type{});
+  run_pass(std::true_type{});
+  run_pass(std::false_type{});
   if (failed) {
-    if (l == 0) {
-      atomicExch(abort_word, 1);
-      atomicOr(&A.status[c], STATUS_TIMEOUT);
-    }
-    // Let this warp's copies still in flight land (bounded) before leaving.
-    for (int g = waited; g < next; g++) mbar_wait(&full[g % NB], unsigned(g / NB) & 1u, A.drain_limit);
+    if (l == 0) atomicOr(&A.status[c], STATUS_TIMEOUT);
     return;
   }
   if (threadIdx.x == 0) A.cfl[c] = fminf(A.cfl_max[c], A.cfl[c] * A.growth[c]);
@@ -465,60 +380,67 @@ __global__ void __launch_bounds__(TILE_THREADS) lusgs_update_kernel(const CaseDe
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&status[c], STATUS_NON_PHYSICAL);
 }
 
-// Launch shape of the sweep: diagonals per bulk copy and chunk buffers per
-// warp.
+// Launch shape of the sweep: diagonals per chunk and chunk buffers.
 struct SweepShape {
   int chunk = 0, buffers = 0;
 };
 
-// The shape for cases of up to `nj` rows when `cases_in_flight` cases sweep
-// at once: within the shared memory each CTA may take (the resident cases,
-// up to 8 per SM, share an SM's), the one whose copies run furthest ahead of
-// the diagonal being swept ((buffers - 1) chunk - 1 diagonals), the smaller
-// footprint on a tie; chunks of up to `max_chunk` diagonals.
-inline SweepShape sweep_shape(int nj, int cases_in_flight, int max_chunk = 8) {
+// The shape for cases whose longest diagonal is `max_len` cells when
+// `cases_in_flight` cases sweep at once: within the shared memory each CTA
+// may take (the resident cases, up to 8 per SM, share an SM's), the longest
+// chunk (up to `max_chunk` diagonals; a chunk's steps are unrolled, so
+// longer chunks amortise its wait and schedule better) in at least two
+// buffers, then as many buffers as fit, up to four.
+inline SweepShape sweep_shape(int max_len, int cases_in_flight, int max_chunk = 16) {
   const int per_sm = std::min(8, std::max(1, (cases_in_flight + 147) / 148));
-  for (size_t budget : {size_t(200 * 1024) / per_sm, size_t(200 * 1024)}) {
-    SweepShape best;
-    int best_lead = -1;
-    size_t best_bytes = 0;
-    for (int nb = 2; nb <= kMaxSweepBuffers; nb++)
-      for (int k = 1; k <= max_chunk; k++) {
-        const size_t bytes = sweep_smem_bytes(nj, k, nb);
-        if (bytes > budget) continue;
-        const int lead = (nb - 1) * k - 1;
-        if (lead > best_lead || (lead == best_lead && bytes < best_bytes)) {
-          best = {k, nb};
-          best_lead = lead;
-          best_bytes = bytes;
-        }
-      }
-    if (best.chunk > 0) return best;
-  }
+  for (size_t budget : {size_t(220 * 1024) / per_sm, size_t(220 * 1024)})
+    for (int k = 16; k >= 1; k /= 2) {
+      if (k > max_chunk || sweep_smem_bytes(max_len, k, 2) > budget) continue;
+      int nb = 2;
+      while (nb < 4 && sweep_smem_bytes(max_len, k, nb + 1) <= budget) nb++;
+      return {k, nb};
+    }
   return {};
 }
 
 constexpr int kSweepWaitLimit = 1 << 22;
 
+template <int K>
+inline cudaError_t launch_sweep_k(const SweepArgs& A, int n_cases, int warps, size_t bytes, cudaStream_t stream) {
+  cudaError_t e;
+  if (warps == 1) {
+    e = cudaFuncSetAttribute(lusgs_sweep_kernel<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    if (e != cudaSuccess) return e;
+    lusgs_sweep_kernel<K, true><<<n_cases, 64, bytes, stream>>>(A);
+  } else {
+    e = cudaFuncSetAttribute(lusgs_sweep_kernel<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    if (e != cudaSuccess) return e;
+    lusgs_sweep_kernel<K, false><<<n_cases, 32 * (warps + 1), bytes, stream>>>(A);
+  }
+  return cudaGetLastError();
+}
+
+// `max_nj` and `max_len`: the launch's widest case and longest diagonal;
 // `cases_in_flight`: cases of the whole batch sweeping at the same time
 // (other lanes included), which sets the shared memory each CTA may take.
 // `wait_limit` < 0 keeps the default bound.
-inline cudaError_t launch_sweep(SweepArgs A, int n_cases, int max_nj, int cases_in_flight,
-                                cudaStream_t stream, int wait_limit = -1, int max_chunk = 8) {
-  const int nw = sweep_warps(max_nj);
-  if (nw > kMaxSweepWarps) return cudaErrorInvalidConfiguration;
-  const SweepShape shape = sweep_shape(max_nj, cases_in_flight, max_chunk);
+inline cudaError_t launch_sweep(SweepArgs A, int n_cases, int max_nj, int max_len, int cases_in_flight,
+                                cudaStream_t stream, int wait_limit = -1, int max_chunk = 16) {
+  const int warps = (max_nj + 31) / 32;
+  if (warps > kMaxSweepWarps || max_nj + max_len > 65536) return cudaErrorInvalidConfiguration;
+  const SweepShape shape = sweep_shape(max_len, cases_in_flight, max_chunk);
   if (shape.chunk == 0) return cudaErrorInvalidConfiguration;
-  A.chunk = shape.chunk;
   A.buffers = shape.buffers;
   A.wait_limit = wait_limit < 0 ? kSweepWaitLimit : wait_limit;
   A.drain_limit = kSweepWaitLimit;
-  const size_t bytes = sweep_smem_bytes(max_nj, shape.chunk, shape.buffers);
-  const cudaError_t e = cudaFuncSetAttribute(lusgs_sweep_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
-  if (e != cudaSuccess) return e;
-  lusgs_sweep_kernel<<<n_cases, 32 * nw, bytes, stream>>>(A);
-  return cudaGetLastError();
+  const size_t bytes = sweep_smem_bytes(max_len, shape.chunk, shape.buffers);
+  switch (shape.chunk) {
+    case 16: return launch_sweep_k<16>(A, n_cases, warps, bytes, stream);
+    case 8: return launch_sweep_k<8>(A, n_cases, warps, bytes, stream);
+    case 4: return launch_sweep_k<4>(A, n_cases, warps, bytes, stream);
+    case 2: return launch_sweep_k<2>(A, n_cases, warps, bytes, stream);
+    default: return launch_sweep_k<1>(A, n_cases, warps, bytes, stream);
+  }
 }
 
 }  // namespace bsd

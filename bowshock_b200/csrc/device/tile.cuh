@@ -6,8 +6,9 @@
 // residual with the axisymmetric source (:1287-1295), and then, by MODE:
 //   STAGE    - one SSP-RK stage, out = a u0 + b (src + dt/V R) (:1160-1175),
 //              with the local time step of the first stage fused (:1183-1205);
-//   PREPARE  - LU-SGS pass A: the residual (FP32 copy), an FP32 copy of the
-//              state and the scalar diagonal (:926-971) for the sweeps;
+//   PREPARE  - LU-SGS pass A: each cell's two sweep records - the residual
+//              (FP32 copy), the scalar diagonal (:926-971) and the
+//              constants of the neighbour terms the sweeps will meet;
 //   RESIDUAL - the residual itself, in FP64 (residualVector, :456-472).
 // Every mode can add sum (R_rho / V)^2 of its cells to a per-case FP64 slot
 // (densityResidualNorm, :480-491) with warp-shuffle reductions.
@@ -36,7 +37,7 @@ struct TileArgs {
   double a, b;            // STAGE coefficients
   int first_stage;        // STAGE: compute the time step from src (== u0)
   float4* rec_f;          // PREPARE output: each cell's forward sweep record (5 float4)
-  float4* rec_b;          // PREPARE output: its backward record, fields 1-4
+  float4* rec_b;          // PREPARE output: its backward record, fields 1-4 (sweep_slot order)
   const float* cfl;       // PREPARE: per case current implicit CFL number
   const float* omega;     // PREPARE: per case omega
   double* res_out;        // RESIDUAL: 4 values per cell, arena like the state
@@ -240,10 +241,12 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) tile_kernel(const TileAr
       A.out.store(k, o);
       if (!is_physical(o, gamma)) atomicOr(&A.status[c], STATUS_NON_PHYSICAL);
     } else if (MODE == MODE_PREPARE) {
-      // The sweep record (see lusgs_sweep_kernel): residual, state, (u, v,
-      // p, 1/D), and the west and south faces with their half areas and
-      // damping omega lambda A / 2 - everything the sweeps need that does
-      // not depend on dQ, computed here where every cell is independent.
+      // The sweep records (see lusgs_sweep_kernel): the residual, 1/D and,
+      // for each neighbour the sweep meets, its density, velocity and
+      // H = E + p with the face's signed normal times A/2 and hud =
+      // (u, v) . (hnx, hny) - omega lambda A/2 - everything the sweeps need
+      // that does not depend on dQ, computed here where every cell is
+      // independent and the neighbours' states are in the tile.
       const float g = float(gamma);
       const float4 fw = A.m.iface[cd.iface + i + int64_t(j) * (ni + 1)];
       const float4 fe = A.m.iface[cd.iface + i + 1 + int64_t(j) * (ni + 1)];
@@ -260,36 +263,40 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) tile_kernel(const TileAr
       const float omega = A.omega[c];
       const float scale = 0.5f * (omega + 1.f / A.cfl[c]);
       const float diag = scale * (lw + le + ls + ln) + (cd.axisym ? cm.y * rad(sj, si, 0.f, 1.f) : 0.f);
-      const float4 st = make_float4(float(qs.rho), float(qs.mu), float(qs.mv), float(qs.e));
-      const float4 wv = make_float4(float(W[1][sj][si]), float(W[2][sj][si]), float(W[3][sj][si]), 1.f / diag);
-      // The records of the warp of 32 rows that sweeps row j (sweep_block_slot):
-      // forward at record row j % 32 + 1, backward at j % 32.
-      const int w = j >> 5, l = j & 31;
-      const int64_t base = cd.slot;
-      float4* rf = A.rec_f + 5 * (base + sweep_block_slot(ni, nj, w, i, l + 1));
-      rf[0] = make_float4(float(res[0]), float(res[1]), float(res[2]), float(res[3]));
-      rf[1] = st;
-      rf[2] = wv;
-      rf[3] = make_float4(fw.x, fw.y, 0.5f * fw.z, 0.5f * omega * lw);
-      rf[4] = make_float4(fs.x, fs.y, 0.5f * fs.z, 0.5f * omega * ls);
-      float4* rb = A.rec_b + 5 * (base + sweep_block_slot(ni, nj, w, i, l));
-      rb[1] = st;
-      rb[2] = wv;
-      rb[3] = make_float4(fe.x, fe.y, 0.5f * fe.z, 0.5f * omega * le);
-      rb[4] = make_float4(fn.x, fn.y, 0.5f * fn.z, 0.5f * omega * ln);
-      // Ghost rows: the state of the neighbour row that belongs to the next
-      // (forward) or previous (backward) warp. Row 0 and the last row have
-      // no such neighbour; their ghost holds the cell's own state, which a
-      // zero correction turns into an exactly zero term.
-      auto put_ghost = [&](float4* rec, int wg, int r) {
-        float4* gr = rec + 5 * (base + sweep_block_slot(ni, nj, wg, i, r));
-        gr[1] = st;
-        gr[2] = wv;
+      const float hk = g / (g - 1.f);
+      // (rho, u, v, H) and (hnx, hny, hud, 0) of the neighbour at (aj, ai)
+      // across face f, the flux leaving through sgn n; an absent neighbour
+      // gets the inert (1, 0, 0, 0), (0, 0, 0, 0).
+      auto term = [&](bool present, int aj, int ai, float4 f, float sgn, float lam, float4& q4, float4& f4) {
+        if (!present) {
+          q4 = make_float4(1.f, 0.f, 0.f, 0.f);
+          f4 = make_float4(0.f, 0.f, 0.f, 0.f);
+          return;
+        }
+        const float rho = float(W[0][aj][ai]), u = float(W[1][aj][ai]), v = float(W[2][aj][ai]);
+        const float p = float(W[3][aj][ai]);
+        const float h = 0.5f * f.z * sgn;
+        const float hnx = h * f.x, hny = h * f.y;
+        q4 = make_float4(rho, u, v, fmaf(hk, p, 0.5f * rho * (u * u + v * v)));
+        f4 = make_float4(hnx, hny, (hnx * u + hny * v) - 0.5f * omega * lam, 0.f);
       };
-      if (l == 31 && j + 1 < nj) put_ghost(A.rec_f, w + 1, 0);
-      if (j == 0) put_ghost(A.rec_f, 0, 0);
-      if (l == 0 && j > 0) put_ghost(A.rec_b, w - 1, 32);
-      if (j == nj - 1) put_ghost(A.rec_b, w, sweep_rows(nj, w));
+      float4 aq, af, bq, bf;
+      const int64_t slot = REC_SIZE * (cd.slot + sweep_slot(ni, nj, i, j));
+      float4* rf = A.rec_f + slot;
+      term(i > 0, sj, si - 1, fw, -1.f, lw, aq, af);
+      term(j > 0, sj - 1, si, fs, -1.f, ls, bq, bf);
+      rf[0] = make_float4(float(res[0]), float(res[1]), float(res[2]), float(res[3]));
+      rf[1] = make_float4(1.f / diag, aq.x, aq.y, aq.z);
+      rf[2] = make_float4(aq.w, af.x, af.y, af.z);
+      rf[3] = bq;
+      rf[4] = make_float4(bf.x, bf.y, bf.z, 0.f);
+      float4* rb = A.rec_b + slot;
+      term(i + 1 < ni, sj, si + 1, fe, 1.f, le, aq, af);
+      term(j + 1 < nj, sj + 1, si, fn, 1.f, ln, bq, bf);
+      rb[1] = make_float4(1.f / diag, aq.x, aq.y, aq.z);
+      rb[2] = make_float4(aq.w, af.x, af.y, af.z);
+      rb[3] = bq;
+      rb[4] = make_float4(bf.x, bf.y, bf.z, 0.f);
     } else if (A.res_out != nullptr) {
       double* o = A.res_out + 4 * k;
       o[0] = double(res[0]);

@@ -117,6 +117,7 @@ struct LaneView {
   const int* case_list;
   int n_cases;
   int max_nj;
+  int max_len;  // longest anti-diagonal, max min(ni, nj), of its cases
   cudaStream_t stream;
   // The residual pass's tiles when the batch runs a tuned tile shape (else
   // the default tiles above).
@@ -211,6 +212,7 @@ class Solver final : public SolverBase {
       ifc += int64_t(cfg.ni + 1) * cfg.nj;
       jfc += int64_t(cfg.ni) * (cfg.nj + 1);
       max_nj_ = std::max(max_nj_, cfg.nj);
+      max_len_ = std::max(max_len_, std::min(cfg.ni, cfg.nj));
       max_along_ = std::max(max_along_, std::max(cfg.ni, cfg.nj));
     }
     total_cells_ = cell;
@@ -360,6 +362,7 @@ class Solver final : public SolverBase {
         const int ti = (hc[c].ni + bsd::TI - 1) / bsd::TI, tj = (hc[c].nj + bsd::TJ - 1) / bsd::TJ;
         for (int t = 0; t < ti * tj; t++) tiles.push_back(make_int2(c, t));
         lane->max_nj = std::max(lane->max_nj, hc[c].nj);
+        lane->max_len = std::max(lane->max_len, std::min(hc[c].ni, hc[c].nj));
       }
       lane->n_cases = int(members[l].size());
       lane->n_tiles = int(tiles.size());
@@ -1055,8 +1058,12 @@ class Solver final : public SolverBase {
 
   bs_status ensure_implicit() {
     if (rec_f_.p != nullptr) return BS_OK;
-    BS_CUDA(rec_f_.alloc(5 * size_t(total_slots_)));
-    BS_CUDA(rec_b_.alloc(5 * size_t(total_slots_)));
+    // The sweep indexes a case's anti-diagonals in 32 bits.
+    for (const auto& c : hc_)
+      if (c.ni + c.nj > 65536)
+        return fail(BS_INVALID_ARGUMENT, "the LU-SGS sweep takes grids of at most 65536 cells along plus across (ni + nj)");
+    BS_CUDA(rec_f_.alloc(bsd::REC_SIZE * size_t(total_slots_)));
+    BS_CUDA(rec_b_.alloc(bsd::REC_SIZE * size_t(total_slots_)));
     BS_CUDA(dq_.alloc(total_cells_));
     for (int v = 0; v < 4; v++) BS_CUDA(qb_[v].alloc(total_cells_));
     return BS_OK;
@@ -1139,7 +1146,7 @@ class Solver final : public SolverBase {
   }
 
   LaneView whole() const {
-    return {d_tiles_.p, n_tiles_, d_case_list_.p, n_, max_nj_, stream_, d_rtiles_.p, n_rtiles_};
+    return {d_tiles_.p, n_tiles_, d_case_list_.p, n_, max_nj_, max_len_, stream_, d_rtiles_.p, n_rtiles_};
   }
 
   template <int MODE>
@@ -1319,7 +1326,7 @@ class Solver final : public SolverBase {
     S.growth = growth_.p;
     S.omega = omega_.p;
     S.status = status_.p;
-    BS_CUDA(bsd::launch_sweep(S, lane.n_cases, lane.max_nj, n_, lane.stream, sweep_wait_limit_));
+    BS_CUDA(bsd::launch_sweep(S, lane.n_cases, lane.max_nj, lane.max_len, n_, lane.stream, sweep_wait_limit_));
     launches_++;
     return BS_OK;
   }
@@ -1358,7 +1365,7 @@ class Solver final : public SolverBase {
     for (auto& l : lanes_) BS_CUDA(cudaStreamWaitEvent(l->stream, ev_fork_, 0));
     for (auto& l : lanes_) {
       const LaneView lane{l->tiles.p,  l->n_tiles, l->case_list.p, l->n_cases,
-                          l->max_nj,   l->stream,  l->rtiles.p,    l->n_rtiles};
+                          l->max_nj,   l->max_len, l->stream,      l->rtiles.p, l->n_rtiles};
       for (int s = 0; s < count; s++) {
         const bool norm = norm_last && s == count - 1;
         if (method == kMethodExplicit)
@@ -1457,7 +1464,7 @@ class Solver final : public SolverBase {
   int64_t total_cells_ = 0;
   int64_t total_slots_ = 0;
   int n_tiles_ = 0;
-  int max_nj_ = 0, max_along_ = 0;
+  int max_nj_ = 0, max_len_ = 0, max_along_ = 0;
   bool any_global_dt_ = false;
   std::vector<int64_t> boundary_off_, cell_off_;
   std::vector<int64_t> steps_;
@@ -1482,7 +1489,7 @@ class Solver final : public SolverBase {
     DevBuf<int2> tiles, rtiles;
     DevBuf<int> case_list;
     std::vector<int> members;
-    int n_tiles = 0, n_rtiles = 0, n_cases = 0, max_nj = 0;
+    int n_tiles = 0, n_rtiles = 0, n_cases = 0, max_nj = 0, max_len = 0;
     cudaStream_t stream = nullptr;
   };
   std::vector<std::unique_ptr<Lane>> lanes_;

@@ -11,9 +11,8 @@
 // kernels) lives in one file-scope static device array of fixed size that the
 // library reserves on every GPU that loads it, for as long as the process runs.
 //
-// Limits and sharing: at most kStaticMaxCells cells (ni nj), kStaticMaxSlots
-// sweep-record slots (bsd::sweep_slots(ni, nj), a little over ni nj plus 33
-// per row: 128 x 512 needs 84,480 and is refused) and 512 cells across (nj).
+// Limits and sharing: at most kStaticMaxCells cells (ni nj; the sweep records
+// take one slot per cell) and 512 cells across (nj).
 // Every call uses the same array, which keeps the last call's contents; the
 // per-call words that must start at zero are cleared by each call. Calls
 // whose work overlaps on the GPU (from several threads, or on several streams
@@ -40,8 +39,8 @@
 namespace {
 
 constexpr int64_t kStaticMaxCells = 65536;
-// Slots of the LU-SGS sweep records (bsd::sweep_slots).
-constexpr int64_t kStaticMaxSlots = 81920;
+// Slots of the LU-SGS sweep records (bsd::sweep_slots: one per cell).
+constexpr int64_t kStaticMaxSlots = kStaticMaxCells;
 constexpr int kStaticMaxTiles = 4096;
 constexpr int kMaxDevices = 64;
 
@@ -56,7 +55,7 @@ constexpr size_t kOffRecB = kOffRecF + align_up(5 * sizeof(float4) * kStaticMaxS
 constexpr size_t kOffDq = kOffRecB + align_up(5 * sizeof(float4) * kStaticMaxSlots);
 constexpr size_t kStaticBytes = kOffDq + align_up(sizeof(float4) * kStaticMaxCells);
 
-// The scratch: about 14.2 MB on every device that loads the library.
+// The scratch: about 11.6 MB on every device that loads the library.
 static __device__ __align__(256) unsigned char g_step_scratch[kStaticBytes];
 
 // The per-case words inside the kOffWords region.
@@ -126,12 +125,7 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
                     "the grid has " + std::to_string(n_cells) +
                         " cells; the allocation-free step takes at most " +
                         std::to_string(kStaticMaxCells));
-  const int64_t n_slots = bsd::sweep_slots(ni, nj);
-  if (n_slots > kStaticMaxSlots)
-    return bs::fail(BS_INVALID_ARGUMENT,
-                    "the grid needs " + std::to_string(n_slots) +
-                        " sweep-record slots; the allocation-free step takes at most " +
-                        std::to_string(kStaticMaxSlots));
+  static_assert(kStaticMaxSlots >= kStaticMaxCells, "one sweep-record slot per cell");
   const int n_tiles = ((ni + bsd::TI - 1) / bsd::TI) * ((nj + bsd::TJ - 1) / bsd::TJ);
   if (n_tiles > kStaticMaxTiles)
     return bs::fail(BS_INVALID_ARGUMENT, "the grid needs more tiles than the static scratch holds");
@@ -219,7 +213,7 @@ bs_status bs_lusgs_step_static(const bs_config* config, const float* iface, cons
     S.growth = &d_words->growth;
     S.omega = &d_words->omega;
     S.status = &d_words->status;
-    err = bsd::launch_sweep(S, 1, nj, 1, st);
+    err = bsd::launch_sweep(S, 1, nj, std::min(ni, nj), 1, st);
   }
   if (err == cudaSuccess) {
     bsd::lusgs_update_kernel<double><<<n_tiles, bsd::TILE_THREADS, 0, st>>>(

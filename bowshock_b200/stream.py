@@ -26,12 +26,10 @@ SLOT_BYTES = 160
 
 
 def sweep_slots(ni: int, nj: int) -> int:
-    """Record slots of a case: per warp of 32 rows (the last may hold
-    fewer) a block of ni + rows diagonals by rows + 1 record rows, as the
-    device layout (sweep_slots in device/layout.cuh)."""
-    nw = (nj + 31) // 32
-    rows = nj - 32 * (nw - 1)
-    return (nw - 1) * (ni + 32) * 33 + (ni + rows) * (rows + 1)
+    """Record slots of a case: one per cell, stored by anti-diagonal with no
+    slot off the grid, as the device layout (sweep_slots in
+    device/layout.cuh)."""
+    return ni * nj
 
 
 def case_device_bytes(ni: int, nj: int) -> int:

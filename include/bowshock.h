@@ -318,11 +318,9 @@ BS_API bs_status bs_engine_set_sweep_wait_limit(bs_engine *engine, int32_t polls
  * that hand out all GPU memory from their own pool (cudaMalloc would bypass
  * their budget, and cudaMalloc/cudaFree synchronise the device) and solver
  * loops that must not allocate once running. All scratch lives in one static
- * device array of the library (about 14.2 MB), reserved on every GPU that
- * loads it until the process exits: at most 65536 cells (ni nj), 512 cells
- * across (nj) and 81920 sweep-record slots (33 (ni + 32) per 32 rows, the
- * last warp's rows r taking (ni + r)(r + 1): 256 x 256 needs 76032,
- * 128 x 512 needs 84480); larger grids return BS_INVALID_ARGUMENT. The first
+ * device array of the library (about 11.6 MB), reserved on every GPU that
+ * loads it until the process exits: at most 65536 cells (ni nj) and 512
+ * cells across (nj); larger grids return BS_INVALID_ARGUMENT. The first
  * call on a device looks up the array's device address with that device
  * current; after cudaDeviceReset that address is stale and the entry point
  * must not be called again in the process. Each call waits for `stream` (it

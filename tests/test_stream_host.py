@@ -39,13 +39,12 @@ def test_a_case_larger_than_the_budget_is_a_wave_of_its_own():
 
 
 def test_device_bytes_grow_with_the_sweep_record_slots():
-    # 80 x 40: 3,200 cells; rows 0-31 a block of 112 x 33 slots, rows 32-39 one of 88 x 9.
-    assert sweep_slots(80, 40) == 112 * 33 + 88 * 9
-    assert sweep_slots(160, 80) == 2 * 192 * 33 + 176 * 17
-    assert sweep_slots(40, 32) == 72 * 33
+    # One record slot per cell: 80 x 40 has 3,200 cells.
+    assert sweep_slots(80, 40) == 3200
+    assert sweep_slots(160, 80) == 12800
     b = case_device_bytes(80, 40)
-    assert b == 3200 * 124 + 120 * 16 + (112 * 33 + 88 * 9) * 160 + 64 * 120
-    assert case_device_bytes(640, 320) > 50 * b
+    assert b == 3200 * 124 + 120 * 16 + 3200 * 160 + 64 * 120
+    assert case_device_bytes(640, 320) > 60 * b
 
 
 def test_waves_by_grid_size_hold_one_size_where_the_budget_allows():

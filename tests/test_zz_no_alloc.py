@@ -53,8 +53,8 @@ def primitives_of(state, gamma) -> np.ndarray:
 
 @pytest.mark.parametrize("ni, nj", [(96, 48), (512, 128)])
 def test_static_step_matches_the_engine_step_twice_in_a_row(ni, nj):
-    # 512 x 128 fills the scratch's cell limit (65,536) and takes 71,808 of
-    # its 81,920 sweep-record slots.
+    # 512 x 128 fills the scratch's cell limit (65,536), one sweep-record
+    # slot per cell.
     torch = pytest.importorskip("torch")
     lib = _native.load()
     case = ogive_case(2.2, ni, nj)
@@ -97,14 +97,14 @@ def test_static_step_refuses_grids_beyond_its_scratch():
                                   C.byref(residual), C.byref(bad))
     assert st == abi.BS_INVALID_ARGUMENT
     assert "at most 65536" in lib.bs_last_error().decode()
-    # 128 x 512: 65,536 cells, but 84,480 sweep-record slots.
+    # 64 x 513: within the cell limit, but wider than 512 cells across.
     from dataclasses import replace
 
     from bowshock_b200.config import grid_from_function
 
-    wide = replace(case.config, grid=grid_from_function(128, 512, lambda i, j: (i / 128, 1 + j / 512)))
+    wide = replace(case.config, grid=grid_from_function(64, 513, lambda i, j: (i / 64, 1 + j / 513)))
     cfg = wide.to_abi()
     st = lib.bs_lusgs_step_static(C.byref(cfg), p, p, p, p, p, p, p, CFL, OMEGA, None,
                                   C.byref(residual), C.byref(bad))
     assert st == abi.BS_INVALID_ARGUMENT
-    assert "84480 sweep-record slots" in lib.bs_last_error().decode()
+    assert "512 cells across" in lib.bs_last_error().decode()
