@@ -85,6 +85,17 @@ __host__ __device__ __forceinline__ int64_t sweep_slots(int ni, int nj) { return
 // float4 fields of a record (listed with the sweep kernel).
 constexpr int REC_SIZE = 5;
 
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream-serialization attribute may start before the kernel ahead of it in
+// its stream has finished; it must wait (griddep_wait) before it reads what
+// that kernel writes or writes what it reads. Without the attribute both
+// instructions do nothing.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+// Lets the dependent kernel be launched once every CTA of this one has run it.
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 struct CaseDev {
   int32_t ni, nj;
   int64_t cell;   // offset of the case's cell arrays

@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <type_traits>
+#include <utility>
 
 #include "layout.cuh"
 
@@ -220,6 +221,8 @@ static __global__ void __launch_bounds__(32 * (kMaxSweepWarps + 1), 1) lusgs_swe
     mbar_fence_init();
   }
   __syncthreads();
+  // Launched behind the residual pass that writes the records: wait for it.
+  griddep_wait();
   const int ndiag = ni + nj - 1;
   const int nch = (ndiag + K - 1) / K;
   const int buf_stride = K * len_max * REC_SIZE;
@@ -388,10 +391,11 @@ struct SweepShape {
 // The shape for cases whose longest diagonal is `max_len` cells when
 // `cases_in_flight` cases sweep at once: within the shared memory each CTA
 // may take (the resident cases, up to 8 per SM, share an SM's), the longest
-// chunk (up to `max_chunk` diagonals; a chunk's steps are unrolled, so
-// longer chunks amortise its wait and schedule better) in at least two
-// buffers, then as many buffers as fit, up to four.
-inline SweepShape sweep_shape(int max_len, int cases_in_flight, int max_chunk = 16) {
+// chunk of up to `max_chunk` diagonals in at least two buffers, then as many
+// buffers as fit, up to four. A chunk's steps are unrolled, so longer chunks
+// amortise its wait; past 8 the unrolled block schedules worse (one case of
+// 160 x 80: 370 cycles a diagonal with K = 8, 398 with K = 16).
+inline SweepShape sweep_shape(int max_len, int cases_in_flight, int max_chunk = 8) {
   const int per_sm = std::min(8, std::max(1, (cases_in_flight + 147) / 148));
   for (size_t budget : {size_t(220 * 1024) / per_sm, size_t(220 * 1024)})
     for (int k = 16; k >= 1; k /= 2) {
@@ -405,27 +409,49 @@ inline SweepShape sweep_shape(int max_len, int cases_in_flight, int max_chunk = 
 
 constexpr int kSweepWaitLimit = 1 << 22;
 
+// Launches `kernel` with the programmatic stream-serialization attribute when
+// `pdl` (the kernel must then wait with griddep_wait before it touches what
+// the kernel ahead of it in the stream reads or writes).
+template <class... Params, class... Args>
+inline cudaError_t launch_maybe_pdl(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem,
+                                    cudaStream_t stream, bool pdl, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 template <int K>
-inline cudaError_t launch_sweep_k(const SweepArgs& A, int n_cases, int warps, size_t bytes, cudaStream_t stream) {
+inline cudaError_t launch_sweep_k(const SweepArgs& A, int n_cases, int warps, size_t bytes, cudaStream_t stream,
+                                  bool pdl) {
   cudaError_t e;
   if (warps == 1) {
     e = cudaFuncSetAttribute(lusgs_sweep_kernel<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
     if (e != cudaSuccess) return e;
-    lusgs_sweep_kernel<K, true><<<n_cases, 64, bytes, stream>>>(A);
+    e = launch_maybe_pdl(lusgs_sweep_kernel<K, true>, dim3(n_cases), dim3(64), bytes, stream, pdl, A);
   } else {
     e = cudaFuncSetAttribute(lusgs_sweep_kernel<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
     if (e != cudaSuccess) return e;
-    lusgs_sweep_kernel<K, false><<<n_cases, 32 * (warps + 1), bytes, stream>>>(A);
+    e = launch_maybe_pdl(lusgs_sweep_kernel<K, false>, dim3(n_cases), dim3(32 * (warps + 1)), bytes, stream, pdl, A);
   }
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 
 // `max_nj` and `max_len`: the launch's widest case and longest diagonal;
 // `cases_in_flight`: cases of the whole batch sweeping at the same time
 // (other lanes included), which sets the shared memory each CTA may take.
-// `wait_limit` < 0 keeps the default bound.
+// `wait_limit` < 0 keeps the default bound; `pdl`: launched behind the
+// residual pass by programmatic dependent launch.
 inline cudaError_t launch_sweep(SweepArgs A, int n_cases, int max_nj, int max_len, int cases_in_flight,
-                                cudaStream_t stream, int wait_limit = -1, int max_chunk = 16) {
+                                cudaStream_t stream, int wait_limit = -1, int max_chunk = 8, bool pdl = false) {
   const int warps = (max_nj + 31) / 32;
   if (warps > kMaxSweepWarps || max_nj + max_len > 65536) return cudaErrorInvalidConfiguration;
   const SweepShape shape = sweep_shape(max_len, cases_in_flight, max_chunk);
@@ -435,11 +461,11 @@ inline cudaError_t launch_sweep(SweepArgs A, int n_cases, int max_nj, int max_le
   A.drain_limit = kSweepWaitLimit;
   const size_t bytes = sweep_smem_bytes(max_len, shape.chunk, shape.buffers);
   switch (shape.chunk) {
-    case 16: return launch_sweep_k<16>(A, n_cases, warps, bytes, stream);
-    case 8: return launch_sweep_k<8>(A, n_cases, warps, bytes, stream);
-    case 4: return launch_sweep_k<4>(A, n_cases, warps, bytes, stream);
-    case 2: return launch_sweep_k<2>(A, n_cases, warps, bytes, stream);
-    default: return launch_sweep_k<1>(A, n_cases, warps, bytes, stream);
+    case 16: return launch_sweep_k<16>(A, n_cases, warps, bytes, stream, pdl);
+    case 8: return launch_sweep_k<8>(A, n_cases, warps, bytes, stream, pdl);
+    case 4: return launch_sweep_k<4>(A, n_cases, warps, bytes, stream, pdl);
+    case 2: return launch_sweep_k<2>(A, n_cases, warps, bytes, stream, pdl);
+    default: return launch_sweep_k<1>(A, n_cases, warps, bytes, stream, pdl);
   }
 }
 

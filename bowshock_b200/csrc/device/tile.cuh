@@ -71,6 +71,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) tile_kernel(const TileAr
   __shared__ R Fi[4][TJ][TI + 1];
   __shared__ R Fj[4][TJ + 1][TI];
 
+  // Launched behind the previous step's sweep (or a stage): everything below
+  // reads its results. The residual pass then lets the sweep that follows it
+  // be launched, so that kernel's launch and set-up overlap this one.
+  griddep_wait();
+  if (MODE == MODE_PREPARE) griddep_launch_dependents();
   const int2 tile = A.tiles[blockIdx.x];
   const int c = tile.x;
   if (A.active != nullptr && A.active[c] == 0) return;

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "common.hpp"
@@ -1184,6 +1185,13 @@ class Solver final : public SolverBase {
     A.res_out = res_out;
     A.dq_in = dq_in;
     A.upd_out = upd_out;
+    // The residual pass of an LU-SGS step follows the previous step's sweep by
+    // programmatic dependent launch (the kernel waits for it first thing).
+    const bool pdl = MODE == bsd::MODE_PREPARE && pdl_;
+    auto go = [&](auto kernel, int n, int threads) {
+      return bsd::launch_maybe_pdl(kernel, dim3(n), dim3(threads), 0, lane.stream, pdl, A);
+    };
+    cudaError_t e = cudaSuccess;
     bool tuned = false;
     if constexpr (sizeof(R) == sizeof(double) && MODE != bsd::MODE_RESIDUAL) {
       if (rshape_ >= 0) {
@@ -1191,13 +1199,13 @@ class Solver final : public SolverBase {
         A.tiles = lane.rtiles;
         const int n = lane.n_rtiles;
         switch (rshape_) {
-          case 0: bsd::tile_kernel<R, MODE, 1><<<n, bsd::TILE_THREADS, 0, lane.stream>>>(A); break;
-          case 1: bsd::tile_kernel<R, MODE, 4><<<n, bsd::TILE_THREADS, 0, lane.stream>>>(A); break;
-          case 2: bsd::tile_kernel<R, MODE, 1, 16, 15, 512><<<n, 512, 0, lane.stream>>>(A); break;
-          case 3: bsd::tile_kernel<R, MODE, 1, 8, 15, 256><<<n, 256, 0, lane.stream>>>(A); break;
-          case 4: bsd::tile_kernel<R, MODE, 1, 16, 7, 256><<<n, 256, 0, lane.stream>>>(A); break;
-          case 5: bsd::tile_kernel<R, MODE, 1, 24, 15, 384><<<n, 384, 0, lane.stream>>>(A); break;
-          default: bsd::tile_kernel<R, MODE, 1, 8, 15, 128><<<n, 128, 0, lane.stream>>>(A); break;
+          case 0: e = go(bsd::tile_kernel<R, MODE, 1>, n, bsd::TILE_THREADS); break;
+          case 1: e = go(bsd::tile_kernel<R, MODE, 4>, n, bsd::TILE_THREADS); break;
+          case 2: e = go(bsd::tile_kernel<R, MODE, 1, 16, 15, 512>, n, 512); break;
+          case 3: e = go(bsd::tile_kernel<R, MODE, 1, 8, 15, 256>, n, 256); break;
+          case 4: e = go(bsd::tile_kernel<R, MODE, 1, 16, 7, 256>, n, 256); break;
+          case 5: e = go(bsd::tile_kernel<R, MODE, 1, 24, 15, 384>, n, 384); break;
+          default: e = go(bsd::tile_kernel<R, MODE, 1, 8, 15, 128>, n, 128); break;
         }
       }
     }
@@ -1205,11 +1213,12 @@ class Solver final : public SolverBase {
       // Untuned: the default tile, four resident CTAs asked for on launches
       // of at least four waves.
       if (lane.n_tiles >= 4 * sm_count_)
-        bsd::tile_kernel<R, MODE, 4><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
+        e = go(bsd::tile_kernel<R, MODE, 4>, lane.n_tiles, bsd::TILE_THREADS);
       else
-        bsd::tile_kernel<R, MODE><<<lane.n_tiles, bsd::TILE_THREADS, 0, lane.stream>>>(A);
+        e = go(bsd::tile_kernel<R, MODE>, lane.n_tiles, bsd::TILE_THREADS);
     }
     launches_++;
+    BS_CUDA(e);
     BS_CUDA(cudaGetLastError());
     return BS_OK;
   }
@@ -1326,7 +1335,8 @@ class Solver final : public SolverBase {
     S.growth = growth_.p;
     S.omega = omega_.p;
     S.status = status_.p;
-    BS_CUDA(bsd::launch_sweep(S, lane.n_cases, lane.max_nj, lane.max_len, n_, lane.stream, sweep_wait_limit_));
+    BS_CUDA(bsd::launch_sweep(S, lane.n_cases, lane.max_nj, lane.max_len, n_, lane.stream, sweep_wait_limit_, 8,
+                              pdl_));
     launches_++;
     return BS_OK;
   }
@@ -1465,6 +1475,9 @@ class Solver final : public SolverBase {
   int64_t total_slots_ = 0;
   int n_tiles_ = 0;
   int max_nj_ = 0, max_len_ = 0, max_along_ = 0;
+  // Programmatic dependent launch between the residual pass and the sweep
+  // (off with BOWSHOCK_NO_PDL set, to compare).
+  bool pdl_ = std::getenv("BOWSHOCK_NO_PDL") == nullptr;
   bool any_global_dt_ = false;
   std::vector<int64_t> boundary_off_, cell_off_;
   std::vector<int64_t> steps_;
