@@ -58,9 +58,9 @@ BYTES_UPDATE = 80
 # FP64 operations per cell of the residual pass (DADD + DMUL + 2 DFMA,
 # thread instructions counted by ncu on the drag curve's residual pass with
 # the update fused in, halo cells' updates and conversions included, divided
-# by its 204,800 cells: (29.40 M + 48.97 M + 2 x 106.59 M) / 204,800; the
+# by its 204,800 cells: (30.11 M + 48.97 M + 2 x 106.89 M) / 204,800; the
 # summary in profiles/ names the capture).
-FLOPS_PREPARE = 1424
+FLOPS_PREPARE = 1430
 
 
 def workload_config() -> dict:
