@@ -9,9 +9,11 @@
 // diagonal per step:
 //   - its neighbour along the row is the cell it finished on the previous
 //     step (registers); its neighbour across rows is the one the next lane
-//     finished, by warp shuffle, or at a warp edge through a two-slot
-//     exchange in shared memory, ordered by one named barrier per step among
-//     the consumer warps (a case of up to 32 rows has no barrier at all);
+//     finished: in a case of up to 32 rows by warp shuffle, with no barrier
+//     at all; otherwise through an exchange row in shared memory that every
+//     lane writes and reads, ordered by one named barrier per step among the
+//     consumer warps (cheaper on the step's dependent chain than the four
+//     shuffles and the warp-edge special case it replaces);
 //   - everything a step needs that does not depend on dQ - the residual (or
 //     dQ*), 1/D and the constants of the two neighbour terms - is one
 //     80-byte record per cell that the residual pass wrote, stored by
@@ -72,8 +74,9 @@ struct SweepArgs {
 constexpr int kMaxSweepWarps = 16;    // nj <= 512
 constexpr int kMaxSweepBuffers = 8;
 // Header: full[8], empty[8] and the forward-done mbarrier, then the two
-// exchange rows of 16 float4.
-constexpr size_t kSweepHeader = 256 + 2 * 16 * 16;
+// two exchange rows of 32 warps + 2 float4 (row r's correction in slot r + 1,
+// slots 0 and the last zero: the rows outside the grid).
+__host__ __device__ inline size_t sweep_header_bytes(int warps) { return 256 + 2 * size_t(32 * warps + 2) * 16; }
 
 // ---- TMA bulk copies and mbarriers (sm_90 and later; no multicast) --------
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -137,8 +140,8 @@ __device__ __forceinline__ void consumer_sync(int threads) {
 // Shared memory of the sweep for chunks of `chunk` diagonals of up to
 // `max_len` cells (the longest diagonal, min(ni, nj), of the launch's cases)
 // in `buffers` buffers.
-__host__ __device__ inline size_t sweep_smem_bytes(int max_len, int chunk, int buffers) {
-  return kSweepHeader + size_t(buffers) * chunk * max_len * 16 * REC_SIZE;
+__host__ __device__ inline size_t sweep_smem_bytes(int max_len, int warps, int chunk, int buffers) {
+  return sweep_header_bytes(warps) + size_t(buffers) * chunk * max_len * 16 * REC_SIZE;
 }
 
 // The neighbour term of src/engine-cpu/euler2d.ts:977-1005 - the change of
@@ -210,8 +213,10 @@ static __global__ void __launch_bounds__(32 * (kMaxSweepWarps + 1), 1) lusgs_swe
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);  // [kMaxSweepBuffers]
   uint64_t* empty = full + kMaxSweepBuffers;                // [kMaxSweepBuffers]
   uint64_t* fwd_done = empty + kMaxSweepBuffers;
-  float4* xch = reinterpret_cast<float4*>(smem_raw + 256);  // [2][16]
-  float4* bufs = reinterpret_cast<float4*>(smem_raw + kSweepHeader);
+  const int XS = 32 * P + 2;
+  float4* xch = reinterpret_cast<float4*>(smem_raw + 256);  // [2][XS]
+  float4* bufs = reinterpret_cast<float4*>(smem_raw + sweep_header_bytes(P));
+  for (int k = threadIdx.x; k < 2 * XS; k += blockDim.x) xch[k] = make_float4(0.f, 0.f, 0.f, 0.f);
   if (threadIdx.x == 0) {
     for (int b = 0; b < NB; b++) {
       mbar_init(&full[b], 1);
@@ -267,12 +272,10 @@ static __global__ void __launch_bounds__(32 * (kMaxSweepWarps + 1), 1) lusgs_swe
   auto run_pass = [&](auto direction) {
     constexpr bool fwd = decltype(direction)::value;
     constexpr int pass = fwd ? 0 : 1;
-    // The row neighbour's lane is the one below (forward) / above (backward);
-    // the edge lane takes it from the neighbouring warp's exchange slot, and
-    // the first (last) row has none.
+    // The row neighbour's lane is the one below (forward) / above (backward):
+    // one warp takes its correction by shuffle (the first / last lane has
+    // none), several warps through the exchange row.
     const bool edge_lane = fwd ? l == 0 : l == 31;
-    const bool edge_warp = fwd ? w == 0 : w == W - 1;
-    const int wn = fwd ? max(w - 1, 0) : min(w + 1, kMaxSweepWarps - 1);
     float4 pd = zero;  // the lane's previous cell's dQ (zero before its row starts)
     int t = 0;         // step of the pass (exchange parity)
     for (int cc = 0; cc < nch; cc++) {
@@ -294,9 +297,13 @@ static __global__ void __launch_bounds__(32 * (kMaxSweepWarps + 1), 1) lusgs_swe
         const int e = min(max(j - jlo, 0), jhi - jlo);  // in-range for rows off the diagonal
         const float4* r = buf + REC_SIZE * (boff + e);
         const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
-        const float4 sh = fwd ? shfl4_up(pd) : shfl4_down(pd);
-        const float4 xv = SOLO ? zero : xch[((t & 1) ^ 1) * 16 + wn];
-        const float4 dn = edge_lane ? (edge_warp ? zero : xv) : sh;
+        float4 dn;
+        if (SOLO) {
+          const float4 sh = fwd ? shfl4_up(pd) : shfl4_down(pd);
+          dn = edge_lane ? zero : sh;
+        } else {
+          dn = xch[((t & 1) ^ 1) * XS + j + (fwd ? 0 : 2)];
+        }
         float4 sum = zero;
         add_neighbour(sum, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, pd, gm1, hg);
         add_neighbour(sum, r3.x, r3.y, r3.z, r3.w, r4.x, r4.y, r4.z, dn, gm1, hg);
@@ -317,7 +324,7 @@ static __global__ void __launch_bounds__(32 * (kMaxSweepWarps + 1), 1) lusgs_swe
         }
         pd = active ? dq : pd;
         if (!SOLO) {
-          if (fwd ? l == 31 : l == 0) xch[(t & 1) * 16 + w] = pd;
+          xch[(t & 1) * XS + j + 1] = pd;
           consumer_sync(32 * W);
         }
         if (s + 1 < n) {
@@ -395,13 +402,13 @@ struct SweepShape {
 // buffers as fit, up to four. A chunk's steps are unrolled, so longer chunks
 // amortise its wait; past 8 the unrolled block schedules worse (one case of
 // 160 x 80: 370 cycles a diagonal with K = 8, 398 with K = 16).
-inline SweepShape sweep_shape(int max_len, int cases_in_flight, int max_chunk = 8) {
+inline SweepShape sweep_shape(int max_len, int warps, int cases_in_flight, int max_chunk = 8) {
   const int per_sm = std::min(8, std::max(1, (cases_in_flight + 147) / 148));
   for (size_t budget : {size_t(220 * 1024) / per_sm, size_t(220 * 1024)})
     for (int k = 16; k >= 1; k /= 2) {
-      if (k > max_chunk || sweep_smem_bytes(max_len, k, 2) > budget) continue;
+      if (k > max_chunk || sweep_smem_bytes(max_len, warps, k, 2) > budget) continue;
       int nb = 2;
-      while (nb < 4 && sweep_smem_bytes(max_len, k, nb + 1) <= budget) nb++;
+      while (nb < 4 && sweep_smem_bytes(max_len, warps, k, nb + 1) <= budget) nb++;
       return {k, nb};
     }
   return {};
@@ -454,12 +461,12 @@ inline cudaError_t launch_sweep(SweepArgs A, int n_cases, int max_nj, int max_le
                                 cudaStream_t stream, int wait_limit = -1, int max_chunk = 8, bool pdl = false) {
   const int warps = (max_nj + 31) / 32;
   if (warps > kMaxSweepWarps || max_nj + max_len > 65536) return cudaErrorInvalidConfiguration;
-  const SweepShape shape = sweep_shape(max_len, cases_in_flight, max_chunk);
+  const SweepShape shape = sweep_shape(max_len, warps, cases_in_flight, max_chunk);
   if (shape.chunk == 0) return cudaErrorInvalidConfiguration;
   A.buffers = shape.buffers;
   A.wait_limit = wait_limit < 0 ? kSweepWaitLimit : wait_limit;
   A.drain_limit = kSweepWaitLimit;
-  const size_t bytes = sweep_smem_bytes(max_len, shape.chunk, shape.buffers);
+  const size_t bytes = sweep_smem_bytes(max_len, warps, shape.chunk, shape.buffers);
   switch (shape.chunk) {
     case 16: return launch_sweep_k<16>(A, n_cases, warps, bytes, stream, pdl);
     case 8: return launch_sweep_k<8>(A, n_cases, warps, bytes, stream, pdl);
