@@ -9,11 +9,11 @@
 // diagonal per step:
 //   - its neighbour along the row is the cell it finished on the previous
 //     step (registers); its neighbour across rows is the one the next lane
-//     finished: in a case of up to 32 rows by warp shuffle, with no barrier
-//     at all; otherwise through an exchange row in shared memory that every
-//     lane writes and reads, ordered by one named barrier per step among the
-//     consumer warps (cheaper on the step's dependent chain than the four
-//     shuffles and the warp-edge special case it replaces);
+//     finished, through an exchange row in shared memory that every lane
+//     writes and reads, ordered by one named barrier per step among the
+//     consumer warps (a __syncwarp for a case of up to 32 rows); on the
+//     step's dependent chain one 16-byte store and load cost less than four
+//     warp shuffles;
 //   - everything a step needs that does not depend on dQ - the residual (or
 //     dQ*), 1/D and the constants of the two neighbour terms - is one
 //     80-byte record per cell that the residual pass wrote, stored by
@@ -177,15 +177,6 @@ __device__ __forceinline__ void add_neighbour(float4& sum, float rho, float u, f
   sum.w += fmaf(d.w, hud, fmaf(dp, hun, (H + d.w + dp) * hdun));
 }
 
-__device__ __forceinline__ float4 shfl4_up(float4 v) {
-  return make_float4(__shfl_up_sync(0xffffffffu, v.x, 1), __shfl_up_sync(0xffffffffu, v.y, 1),
-                     __shfl_up_sync(0xffffffffu, v.z, 1), __shfl_up_sync(0xffffffffu, v.w, 1));
-}
-__device__ __forceinline__ float4 shfl4_down(float4 v) {
-  return make_float4(__shfl_down_sync(0xffffffffu, v.x, 1), __shfl_down_sync(0xffffffffu, v.y, 1),
-                     __shfl_down_sync(0xffffffffu, v.z, 1), __shfl_down_sync(0xffffffffu, v.w, 1));
-}
-
 // The forward and backward sweeps of every active case, one CTA per case,
 // leaving the final correction dQ in A.dq (row-major). The CTA has
 // kWarps + 1 warps for the launch's widest case: warps 0 .. W - 1 sweep the
@@ -272,10 +263,6 @@ static __global__ void __launch_bounds__(32 * (kMaxSweepWarps + 1), 1) lusgs_swe
   auto run_pass = [&](auto direction) {
     constexpr bool fwd = decltype(direction)::value;
     constexpr int pass = fwd ? 0 : 1;
-    // The row neighbour's lane is the one below (forward) / above (backward):
-    // one warp takes its correction by shuffle (the first / last lane has
-    // none), several warps through the exchange row.
-    const bool edge_lane = fwd ? l == 0 : l == 31;
     float4 pd = zero;  // the lane's previous cell's dQ (zero before its row starts)
     int t = 0;         // step of the pass (exchange parity)
     for (int cc = 0; cc < nch; cc++) {
@@ -288,22 +275,25 @@ static __global__ void __launch_bounds__(32 * (kMaxSweepWarps + 1), 1) lusgs_swe
       int d = fwd ? dlo : dlo + n - 1;
       int boff = fwd ? 0 : int(diag_cells(ni, nj, d) - off_lo);  // d's first record in the chunk
       const float4* buf = bufs + b * buf_stride;
+      // The step's records are in registers: the next step's are loaded
+      // before this step's exchange store, since shared-memory loads cannot
+      // be moved above a shared-memory store, and loaded after it they would
+      // put their latency on the step's dependent chain (357 against 309
+      // cycles a diagonal on 160 x 80).
+      int jlo = max(0, d - ni + 1), jhi = min(d, nj - 1);
+      float4 r0, r1, r2, r3, r4;
+      {
+        const float4* r = buf + REC_SIZE * (boff + min(max(j - jlo, 0), jhi - jlo));
+        r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
+      }
 #pragma unroll
       for (int s = 0; s < K; s++) {
         // Steps past the chunk's end (its last) repeat its last diagonal
         // with nothing stored, so every warp meets the same barriers.
         const bool live = s < n;
-        const int jlo = max(0, d - ni + 1), jhi = min(d, nj - 1);
-        const int e = min(max(j - jlo, 0), jhi - jlo);  // in-range for rows off the diagonal
-        const float4* r = buf + REC_SIZE * (boff + e);
-        const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
-        float4 dn;
-        if (SOLO) {
-          const float4 sh = fwd ? shfl4_up(pd) : shfl4_down(pd);
-          dn = edge_lane ? zero : sh;
-        } else {
-          dn = xch[((t & 1) ^ 1) * XS + j + (fwd ? 0 : 2)];
-        }
+        // Row j - 1's (forward) / j + 1's (backward) correction of the
+        // previous step, from the exchange row (slot r + 1 holds row r).
+        const float4 dn = xch[((t & 1) ^ 1) * XS + j + (fwd ? 0 : 2)];
         float4 sum = zero;
         add_neighbour(sum, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, pd, gm1, hg);
         add_neighbour(sum, r3.x, r3.y, r3.z, r3.w, r4.x, r4.y, r4.z, dn, gm1, hg);
@@ -323,19 +313,27 @@ static __global__ void __launch_bounds__(32 * (kMaxSweepWarps + 1), 1) lusgs_swe
             dq_case[unsigned(d - j) + unsigned(j) * unsigned(ni)] = dq;
         }
         pd = active ? dq : pd;
-        if (!SOLO) {
-          xch[(t & 1) * XS + j + 1] = pd;
-          consumer_sync(32 * W);
-        }
-        if (s + 1 < n) {
-          if (fwd) {
-            boff += jhi - jlo + 1;
-            d++;
-          } else {
-            d--;
-            boff -= min(d, nj - 1) - max(0, d - ni + 1) + 1;
+        if (s + 1 < K) {
+          // The next diagonal (held in place past the chunk's end) and its records.
+          if (s + 1 < n) {
+            if (fwd) {
+              boff += jhi - jlo + 1;
+              d++;
+            } else {
+              d--;
+              boff -= min(d, nj - 1) - max(0, d - ni + 1) + 1;
+            }
           }
+          jlo = max(0, d - ni + 1);
+          jhi = min(d, nj - 1);
+          const float4* r = buf + REC_SIZE * (boff + min(max(j - jlo, 0), jhi - jlo));
+          r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
         }
+        xch[(t & 1) * XS + j + 1] = pd;
+        if (SOLO)
+          __syncwarp();
+        else
+          consumer_sync(32 * W);
         t++;
       }
       // Every lane's reads of the buffer are done: release it.
