@@ -398,8 +398,9 @@ struct SweepShape {
 // may take (the resident cases, up to 8 per SM, share an SM's), the longest
 // chunk of up to `max_chunk` diagonals in at least two buffers, then as many
 // buffers as fit, up to four. A chunk's steps are unrolled, so longer chunks
-// amortise its wait; past 8 the unrolled block schedules worse (one case of
-// 160 x 80: 370 cycles a diagonal with K = 8, 398 with K = 16).
+// amortise its wait (one case of 160 x 80 alone: 301 cycles a diagonal with
+// K = 16 in two buffers, 313 with K = 8 in three), but fewer buffers copy
+// less far ahead, which counts when other kernels load HBM at the same time.
 inline SweepShape sweep_shape(int max_len, int warps, int cases_in_flight, int max_chunk = 8) {
   const int per_sm = std::min(8, std::max(1, (cases_in_flight + 147) / 148));
   for (size_t budget : {size_t(220 * 1024) / per_sm, size_t(220 * 1024)})

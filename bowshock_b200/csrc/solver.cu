@@ -1335,8 +1335,8 @@ class Solver final : public SolverBase {
     S.growth = growth_.p;
     S.omega = omega_.p;
     S.status = status_.p;
-    BS_CUDA(bsd::launch_sweep(S, lane.n_cases, lane.max_nj, lane.max_len, n_, lane.stream, sweep_wait_limit_, 8,
-                              pdl_));
+    BS_CUDA(bsd::launch_sweep(S, lane.n_cases, lane.max_nj, lane.max_len, n_, lane.stream, sweep_wait_limit_,
+                              sweep_max_chunk_, pdl_));
     launches_++;
     return BS_OK;
   }
@@ -1478,6 +1478,11 @@ class Solver final : public SolverBase {
   // Programmatic dependent launch between the residual pass and the sweep
   // (off with BOWSHOCK_NO_PDL set, to compare).
   bool pdl_ = std::getenv("BOWSHOCK_NO_PDL") == nullptr;
+  // Longest sweep chunk (diagonals per bulk copy; BOWSHOCK_SWEEP_CHUNK
+  // overrides the default 8, to compare). With lanes overlapping, chunks of
+  // 8 in four buffers (three chunks of copies ahead) beat chunks of 16 in two
+  // (one ahead), although 16 is faster alone.
+  int sweep_max_chunk_ = std::getenv("BOWSHOCK_SWEEP_CHUNK") ? std::atoi(std::getenv("BOWSHOCK_SWEEP_CHUNK")) : 8;
   bool any_global_dt_ = false;
   std::vector<int64_t> boundary_off_, cell_off_;
   std::vector<int64_t> steps_;
