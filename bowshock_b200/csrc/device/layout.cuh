@@ -41,11 +41,13 @@ static_assert(TI * TJ <= TILE_THREADS, "a tile has at most one cell per thread")
 // with four. Shapes 2 to 4 give each thread about one face, which halves the
 // dependent FP64 work a thread does and so a CTA's latency (a case's pass on
 // idle SMs is latency-bound); shape 5 reads the least halo (43 % of its
-// cells against 52 %) and shape 6 puts twice as many CTAs on a case.
+// cells against 52 %) and shape 6 puts twice as many CTAs on a case. Shape 7
+// is the default tile with two resident CTAs asked for: at most 128 registers
+// a thread, between shape 0's 140 (one CTA an SM) and shape 1's 64 (spilling).
 struct TileShape {
   int ti, tj, threads, min_blocks;
 };
-constexpr int kTileShapes = 7;
+constexpr int kTileShapes = 8;
 __host__ __device__ constexpr TileShape tile_shape(int k) {
   return k == 0   ? TileShape{TI, TJ, TILE_THREADS, 1}
          : k == 1 ? TileShape{TI, TJ, TILE_THREADS, 4}
@@ -53,7 +55,8 @@ __host__ __device__ constexpr TileShape tile_shape(int k) {
          : k == 3 ? TileShape{8, 15, 256, 1}
          : k == 4 ? TileShape{16, 7, 256, 1}
          : k == 5 ? TileShape{24, 15, 384, 1}
-                  : TileShape{8, 15, 128, 1};
+         : k == 6 ? TileShape{8, 15, 128, 1}
+                  : TileShape{TI, TJ, TILE_THREADS, 2};
 }
 
 // Per-case status bits.

@@ -1205,7 +1205,8 @@ class Solver final : public SolverBase {
           case 3: e = go(bsd::tile_kernel<R, MODE, 1, 8, 15, 256>, n, 256); break;
           case 4: e = go(bsd::tile_kernel<R, MODE, 1, 16, 7, 256>, n, 256); break;
           case 5: e = go(bsd::tile_kernel<R, MODE, 1, 24, 15, 384>, n, 384); break;
-          default: e = go(bsd::tile_kernel<R, MODE, 1, 8, 15, 128>, n, 128); break;
+          case 6: e = go(bsd::tile_kernel<R, MODE, 1, 8, 15, 128>, n, 128); break;
+          default: e = go(bsd::tile_kernel<R, MODE, 2>, n, bsd::TILE_THREADS); break;
         }
       }
     }

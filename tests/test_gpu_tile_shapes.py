@@ -16,7 +16,7 @@ from bowshock_b200.workloads import ogive_case
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [-1, 0, 1, 2, 3, 4, 5, 6]
+SHAPES = [-1, 0, 1, 2, 3, 4, 5, 6, 7]
 
 
 def cases():
@@ -60,7 +60,7 @@ def test_autotune_picks_a_shape_and_keeps_the_state():
         before = [b.primitives(k) for k in range(len(cs))]
         lanes, ms = b.autotune("lusgs", 10)
         t = b.tuning()
-        assert t["lanes"] == lanes and -1 <= t["tile_shape"] < 7 and ms > 0
+        assert t["lanes"] == lanes and -1 <= t["tile_shape"] < 8 and ms > 0
         for k in range(len(cs)):
             assert np.array_equal(b.primitives(k), before[k])
     finally:
