@@ -522,7 +522,7 @@ def run_seeded(args) -> None:
                                "the grid generator): nose conical/tangent ogive/parabolic/ellipsoid/"
                                "Von Karman, fineness U[1,5], body length U[2,8], Mach U[1.5,5], "
                                f"ni = 40*2^k (k in 0..3), nj = ni/2, at most {args.max_steps} steps each",
-                   "cells_total": sum(cells), "grid_build_s": grid_s, "lanes": lanes,
+                   "cells_total": sum(cells), "grid_build_s": grid_s, "tuning": batch.tuning(),
                    "l2": "flushed between timed steps (512 MiB device write)"},
         "gpu_launches": launches,
         "converged": len(converged),
