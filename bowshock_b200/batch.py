@@ -73,16 +73,25 @@ class CudaBatch:
         self._call("bs_batch_set_metric_precision", int(bits))
 
     def set_tile_shape(self, shape: int) -> None:
-        """The residual pass's tile shape: -1 the default, 0 .. 6 the
+        """The residual pass's tile shape: -1 the default, 0 .. 7 the
         autotuner's choices (bs_batch_set_tile_shape)."""
         self._call("bs_batch_set_tile_shape", int(shape))
 
+    def set_update_mode(self, fused: bool) -> None:
+        """LU-SGS steps apply their update inside the next residual pass
+        (True, the default) or by a separate kernel after each sweep
+        (bs_batch_set_update_mode); the autotuner chooses."""
+        self._call("bs_batch_set_update_mode", 1 if fused else 0)
+
     def tuning(self) -> dict:
-        """Lanes and tile shape as set or tuned."""
+        """Lanes, tile shape and update mode as set or tuned."""
         v = [C.c_int32() for _ in range(5)]
         self._call("bs_batch_tuning", *[C.byref(x) for x in v])
         lanes, shape, ti, tj, threads = (x.value for x in v)
-        return {"lanes": lanes, "tile_shape": shape, "tile": f"{ti}x{tj}", "threads": threads}
+        fused = C.c_int32()
+        self._call("bs_batch_update_mode", C.byref(fused))
+        return {"lanes": lanes, "tile_shape": shape, "tile": f"{ti}x{tj}", "threads": threads,
+                "fused_update": bool(fused.value)}
 
     def set_sweep_wait_limit(self, polls: int) -> None:
         """As CudaEuler2D.set_sweep_wait_limit, for the batch's sweeps."""

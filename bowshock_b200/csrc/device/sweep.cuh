@@ -401,15 +401,20 @@ struct SweepShape {
 // amortise its wait (one case of 160 x 80 alone: 301 cycles a diagonal with
 // K = 16 in two buffers, 313 with K = 8 in three), but fewer buffers copy
 // less far ahead, which counts when other kernels load HBM at the same time.
+// When not even one diagonal in two buffers fits a CTA's share, the smallest
+// shape is taken rather than the largest: a batch that large is bound by
+// throughput, and a sweep CTA that fills an SM's shared memory leaves no room
+// beside it for the other cases' sweeps or residual passes.
 inline SweepShape sweep_shape(int max_len, int warps, int cases_in_flight, int max_chunk = 8) {
   const int per_sm = std::min(8, std::max(1, (cases_in_flight + 147) / 148));
-  for (size_t budget : {size_t(220 * 1024) / per_sm, size_t(220 * 1024)})
-    for (int k = 16; k >= 1; k /= 2) {
-      if (k > max_chunk || sweep_smem_bytes(max_len, warps, k, 2) > budget) continue;
-      int nb = 2;
-      while (nb < 4 && sweep_smem_bytes(max_len, warps, k, nb + 1) <= budget) nb++;
-      return {k, nb};
-    }
+  const size_t budget = size_t(220 * 1024) / per_sm;
+  for (int k = 16; k >= 1; k /= 2) {
+    if (k > max_chunk || sweep_smem_bytes(max_len, warps, k, 2) > budget) continue;
+    int nb = 2;
+    while (nb < 4 && sweep_smem_bytes(max_len, warps, k, nb + 1) <= budget) nb++;
+    return {k, nb};
+  }
+  if (sweep_smem_bytes(max_len, warps, 1, 2) <= size_t(220 * 1024)) return {1, 2};
   return {};
 }
 

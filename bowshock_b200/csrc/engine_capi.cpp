@@ -412,6 +412,21 @@ bs_status bs_batch_tuning(bs_batch* batch, int32_t* lanes, int32_t* shape, int32
   });
 }
 
+bs_status bs_batch_set_update_mode(bs_batch* batch, int32_t fused) {
+  BS_BATCH_CALL(batch, {
+    if (fused != 0 && fused != 1) return bs::fail(BS_INVALID_ARGUMENT, "update mode: 1 fused, 0 separate");
+    return batch->solver->set_fused_update(fused == 1);
+  });
+}
+
+bs_status bs_batch_update_mode(bs_batch* batch, int32_t* fused) {
+  BS_BATCH_CALL(batch, {
+    if (fused == nullptr) return bs::fail(BS_INVALID_ARGUMENT, "null argument");
+    *fused = batch->solver->fused_update() ? 1 : 0;
+    return BS_OK;
+  });
+}
+
 bs_status bs_batch_set_sweep_wait_limit(bs_batch* batch, int32_t polls) {
   BS_BATCH_CALL(batch, { return batch->solver->set_sweep_wait_limit(polls); });
 }

@@ -477,6 +477,18 @@ class Solver final : public SolverBase {
 
   int tile_shape() const override { return rshape_; }
 
+  bs_status set_fused_update(bool fused) override {
+    BS_CUDA(cudaStreamSynchronize(stream_));
+    fuse_update_ = fused;
+    // Captured graphs hold the old launches.
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+    graph_launches_.clear();
+    return BS_OK;
+  }
+
+  bool fused_update() const override { return fuse_update_; }
+
   // Times `steps` steps from the current state with 1, 2, 4, ... lanes (up to
   // 64 and the case count), then, with the fastest lane count, each tile shape
   // of the residual pass (FP64 batches), each run after one untimed run that
@@ -548,6 +560,26 @@ class Solver final : public SolverBase {
         }
       }
       BS_TRY(set_tile_shape(best_shape));
+    }
+    // Then, for LU-SGS, the update fused into the residual pass (fewer
+    // launches, the latency-bound case) or a separate update kernel (less
+    // work per step: the fused pass updates each halo cell again, which a
+    // batch that fills the GPU pays for).
+    if (method == kMethodImplicit) {
+      float t_mode[2] = {0.f, 0.f};  // [0] separate update, [1] fused
+      for (int fused = 1; fused >= 0; fused--) {
+        BS_TRY(set_fused_update(fused == 1));
+        BS_TRY(restore());
+        BS_TRY(run_steps(method, steps, false));
+        BS_TRY(restore());
+        BS_CUDA(cudaEventRecord(ev0_, stream_));
+        BS_TRY(run_steps(method, steps, false));
+        BS_CUDA(cudaEventRecord(ev1_, stream_));
+        BS_CUDA(cudaEventSynchronize(ev1_));
+        BS_CUDA(cudaEventElapsedTime(&t_mode[fused], ev0_, ev1_));
+      }
+      BS_TRY(set_fused_update(t_mode[1] <= t_mode[0]));
+      best_ms = std::min(t_mode[0], t_mode[1]);
     }
     BS_TRY(restore());
     BS_CUDA(cudaStreamSynchronize(stream_));
@@ -1272,6 +1304,13 @@ class Solver final : public SolverBase {
   // state back into q, so every run begins and ends with the state in q.
   bs_status record_implicit_step_on(const LaneView& lane, bool norm, int s, int count) {
     const bsd::StateView<R> q = q_view(), qb = qb_view();
+    if (!fuse_update_) {
+      // Residual pass, sweeps, then the update in place (three launches).
+      BS_TRY(launch_tile_on<bsd::MODE_PREPARE>(lane, q, q, q, 0, 1, false, norm ? norm_.p : nullptr, nullptr,
+                                               false));
+      BS_TRY(launch_sweep_on(lane));
+      return launch_update_on(lane, q, q);
+    }
     const bsd::StateView<R> src = (s == 0 || s % 2 == 1) ? q : qb;
     const bsd::StateView<R> dst = s % 2 == 1 ? qb : q;
     BS_TRY(launch_tile_on<bsd::MODE_PREPARE>(lane, src, src, src, 0, 1, false, norm ? norm_.p : nullptr,
@@ -1476,6 +1515,9 @@ class Solver final : public SolverBase {
   int64_t total_slots_ = 0;
   int n_tiles_ = 0;
   int max_nj_ = 0, max_len_ = 0, max_along_ = 0;
+  // LU-SGS steps apply the update inside the next residual pass (true) or
+  // by a separate kernel after each sweep; autotune chooses.
+  bool fuse_update_ = true;
   // Programmatic dependent launch between the residual pass and the sweep
   // (off with BOWSHOCK_NO_PDL set, to compare).
   bool pdl_ = std::getenv("BOWSHOCK_NO_PDL") == nullptr;

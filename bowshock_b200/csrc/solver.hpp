@@ -95,6 +95,11 @@ class SolverBase {
   // which autotune also chooses.
   virtual bs_status set_tile_shape(int shape) = 0;
   virtual int tile_shape() const = 0;
+  // Whether an LU-SGS step's residual pass applies the previous step's
+  // update as it reads (two launches a step) or a separate update kernel
+  // follows each sweep (three), which autotune also chooses.
+  virtual bs_status set_fused_update(bool fused) = 0;
+  virtual bool fused_update() const = 0;
 };
 
 // Cells along i and j and threads of a residual-pass tile shape (-1: the

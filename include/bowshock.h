@@ -399,10 +399,11 @@ BS_API bs_status bs_batch_set_anderson(bs_batch *batch, int32_t depth, int32_t p
 BS_API bs_status bs_batch_set_metric_precision(bs_batch *batch, int32_t bits);
 /* The tile shape of the batch's residual passes and explicit stages: -1 the
  * default (16 x 15 cells on 256 threads, four resident CTAs asked for on
- * launches of four waves or more), 0 .. 6 the autotuner's choices: 16 x 15
+ * launches of four waves or more), 0 .. 7 the autotuner's choices: 16 x 15
  * on 256 threads with one or four resident CTAs asked for, 16 x 15 on 512,
  * 8 x 15 and 16 x 7 on 256 (about one face per thread), 24 x 15 on 384 (the
- * least halo), 8 x 15 on 128. Every shape computes the same residual, cell
+ * least halo), 8 x 15 on 128, 16 x 15 on 256 with two resident CTAs asked
+ * for. Every shape computes the same residual, cell
  * for cell; bs_batch_autotune picks the fastest. FP32 batches keep -1. No
  * counterpart in the reference (its passes are one dispatch per face
  * direction, src/engine-gpu/shaders/euler2d.wgsl:316-367). */
@@ -411,6 +412,14 @@ BS_API bs_status bs_batch_set_tile_shape(bs_batch *batch, int32_t shape);
  * along i and j and its threads. */
 BS_API bs_status bs_batch_tuning(bs_batch *batch, int32_t *lanes, int32_t *shape, int32_t *tile_i,
                                  int32_t *tile_j, int32_t *threads);
+/* How the batch's LU-SGS steps apply their update: 1 (the default) inside
+ * the next step's residual pass as it reads each cell, halo cells included
+ * (two launches a step); 0 by a separate kernel after each sweep (three
+ * launches, less work a step). Both give the same state bit for bit;
+ * bs_batch_autotune picks the faster. No counterpart in the reference. */
+BS_API bs_status bs_batch_set_update_mode(bs_batch *batch, int32_t fused);
+/* The update mode as set or tuned. */
+BS_API bs_status bs_batch_update_mode(bs_batch *batch, int32_t *fused);
 /* As bs_engine_set_sweep_wait_limit, for the batch's later LU-SGS sweeps; a
  * solve reports a case whose sweep gave up as BS_EXECUTION in its result. */
 BS_API bs_status bs_batch_set_sweep_wait_limit(bs_batch *batch, int32_t polls);

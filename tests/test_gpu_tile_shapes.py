@@ -4,7 +4,9 @@ The autotuner picks the tile shape the residual pass and the explicit stages
 run with (bs_batch_set_tile_shape); the shape only decides which CTA
 computes which cell, so the state after any number of steps must be the
 same bit for bit whatever the shape, on grids whose sizes are multiples of
-no tile size and in a batch of uneven cases.
+no tile size and in a batch of uneven cases. The same holds for the LU-SGS
+update mode the autotuner also picks: the update applied inside the next
+residual pass or by a separate kernel after each sweep.
 """
 from __future__ import annotations
 
@@ -23,13 +25,14 @@ def cases():
     return [ogive_case(2.2, 40, 20), ogive_case(1.7, 58, 27), ogive_case(3.1, 100, 45)]
 
 
-def states_after(shape: int, method: str) -> list[np.ndarray]:
+def states_after(shape: int, method: str, fused: bool = True) -> list[np.ndarray]:
     cs = cases()
     b = CudaBatch([c.config for c in cs], precision=64)
     try:
         b.set_tile_shape(shape)
+        b.set_update_mode(fused)
         t = b.tuning()
-        assert t["tile_shape"] == shape
+        assert t["tile_shape"] == shape and t["fused_update"] == fused
         b.set_free_stream()
         if method == "lusgs":
             # 40 steps: tolerance out of reach, so every case takes them all.
@@ -49,6 +52,17 @@ def test_every_tile_shape_takes_the_same_steps(method):
         got = states_after(shape, method)
         for a, b in zip(ref, got):
             assert np.array_equal(a, b), (method, shape)
+
+
+@pytest.mark.parametrize("shape", [-1, 2])
+def test_the_update_applied_in_the_residual_pass_or_after_the_sweep_gives_the_same_steps(shape):
+    # The fused residual pass applies the previous step's correction to every
+    # cell it reads with the update kernel's own arithmetic, so 40 steps end
+    # on the same state either way, bit for bit.
+    fused = states_after(shape, "lusgs", True)
+    separate = states_after(shape, "lusgs", False)
+    for a, b in zip(fused, separate):
+        assert np.array_equal(a, b), shape
 
 
 def test_autotune_picks_a_shape_and_keeps_the_state():
