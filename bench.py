@@ -574,7 +574,9 @@ def run_warmstart(args) -> None:
         "n_gpus": 1, "higher_is_better": True, "dtype": "f64 solve, bf16/fp32 network", "data": "synthetic",
         "config": {"workload": f"train on {tr.solved} converged of {len(train)} seeded 160x80 cases "
                                f"({args.cells_per_case} random cells each, {tr.samples} samples), "
-                               f"evaluate on {n} held-out seeds", "network": "5 x 256 GELU, Fourier features",
+                               f"evaluate on {n} held-out cases ({args.eval_cases} seeds, "
+                               f"{args.eval_cases - n} refused by the grid generator)",
+                   "network": "5 x 256 GELU, Fourier features",
                    "train_steps": tr.steps, "batch": 16384, "grid_build_s": grid_s},
         "train": {"solve_device_ms": tr.solve_device_ms, "seconds": tr.seconds,
                   "loss_first": tr.loss_first, "loss_last": tr.loss_last},
