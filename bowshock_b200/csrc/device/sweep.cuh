@@ -178,10 +178,10 @@ __device__ __forceinline__ void add_neighbour(float4& sum, float rho, float u, f
 }
 
 // The forward and backward sweeps of every active case, one CTA per case,
-// leaving the final correction dQ in A.dq (row-major). The CTA has
-// kWarps + 1 warps for the launch's widest case: warps 0 .. W - 1 sweep the
-// case's W = ceil(nj / 32) warps of rows, the last warp issues the copies,
-// and the ones between (for narrower cases) leave at once.
+// leaving the final correction dQ in A.dq (row-major). The CTA has P + 1
+// warps, P = ceil(nj / 32) of the launch's widest case: warps 0 .. W - 1
+// sweep this case's W = ceil(nj / 32) warps of rows, warp P issues the
+// copies, and the ones between (for narrower cases) leave at once.
 //
 // Chunks: a pass's diagonals in sweep order, K per chunk (the last may hold
 // fewer); chunk g of the sequence (forward chunks, then backward ones) goes
