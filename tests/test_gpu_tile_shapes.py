@@ -65,6 +65,42 @@ def test_the_update_applied_in_the_residual_pass_or_after_the_sweep_gives_the_sa
         assert np.array_equal(a, b), shape
 
 
+@pytest.mark.parametrize("env", [{"BOWSHOCK_NO_PDL": "1"}, {"BOWSHOCK_SWEEP_CHUNK": "16"},
+                                 {"BOWSHOCK_SWEEP_CHUNK": "2"}])
+def test_launch_modes_leave_the_steps_unchanged(env, monkeypatch):
+    # The launch switches (read when a batch is created) change how the
+    # residual pass and the sweep are launched and how many diagonals one
+    # bulk copy brings, not what they compute: 40 steps end on the same state.
+    ref = states_after(-1, "lusgs")
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    got = states_after(-1, "lusgs")
+    for a, b in zip(ref, got):
+        assert np.array_equal(a, b), env
+
+
+def test_one_diagonal_chunks_reach_the_same_steady_state(monkeypatch):
+    # Chunks of one diagonal leave the sweep's step loop without unrolling, and
+    # its FP32 operator then rounds a little differently (about 1e-8 after two
+    # steps, the same in every run): the path to the steady state moves at
+    # that level, the steady state and its drag do not.
+    def drags():
+        cs = cases()
+        b = CudaBatch([c.config for c in cs], precision=64)
+        try:
+            b.set_free_stream()
+            res = b.solve("lusgs", 1e-10, max_steps=4000)
+            assert all(r.status == 0 for r in res)
+            return [b.forebody_drag(k, c.free, c.body.nose.base_radius) for k, c in enumerate(cs)]
+        finally:
+            b.destroy()
+
+    ref = drags()
+    monkeypatch.setenv("BOWSHOCK_SWEEP_CHUNK", "1")
+    for a, b in zip(ref, drags()):
+        assert abs(b / a - 1) < 1e-12
+
+
 def test_autotune_picks_a_shape_and_keeps_the_state():
     cs = cases()
     b = CudaBatch([c.config for c in cs], precision=64)
