@@ -5,11 +5,15 @@
 // max(0, d - ni + 1) .. min(d, nj - 1) in order; and the chunk ranges the
 // sweep's producer copies (K diagonals, forward from diagonal 0, backward
 // ending at the last) stay inside the case and within K * min(ni, nj)
-// records, the buffer size. Prints "ok" or the first failure.
+// records, the buffer size. Also the sweep's launch shape (sweep_shape):
+// within a CTA's share of shared memory the longest chunk of up to 8
+// diagonals in at least two buffers, then up to four buffers, and the
+// smallest shape when not even one diagonal in two buffers fits the share. Prints "ok" or the first failure.
 #include <cstdio>
 #include <vector>
 
 #include "device/layout.cuh"
+#include "device/sweep.cuh"
 
 static int check(int ni, int nj) {
   const int ndiag = ni + nj - 1;
@@ -45,7 +49,27 @@ static int check(int ni, int nj) {
   return 0;
 }
 
+static int check_shape(int max_len, int warps, int cases, int want_chunk, int want_buffers) {
+  const bsd::SweepShape s = bsd::sweep_shape(max_len, warps, cases);
+  const size_t bytes = bsd::sweep_smem_bytes(max_len, warps, s.chunk, s.buffers);
+  if (s.chunk != want_chunk || s.buffers != want_buffers || bytes > 220 * 1024)
+    return printf("shape(%d, %d, %d): K %d NB %d, %zu bytes\n", max_len, warps, cases, s.chunk, s.buffers, bytes), 1;
+  return 0;
+}
+
 int main() {
+  // The drag curve (160 x 80, 16 cases): K 8 in four buffers, 208 KB.
+  if (check_shape(80, 3, 16, 8, 4)) return 1;
+  // 640 x 320 alone: 25.6 KB a diagonal, the longest chunk first: K 4 in two buffers.
+  if (check_shape(320, 10, 16, 4, 2)) return 1;
+  // 300 cases of 160 x 80 (three an SM): K 4 in two buffers within 73 KB.
+  if (check_shape(80, 3, 300, 4, 2)) return 1;
+  // 873 cases of 640 x 320, 1,988 mixed up to 320 x 160: no shape fits a
+  // CTA's share of an SM, so the smallest.
+  if (check_shape(320, 10, 873, 1, 2)) return 1;
+  if (check_shape(160, 5, 1988, 1, 2)) return 1;
+  // A case of up to 32 rows: one consumer warp, K 8 in four buffers.
+  if (check_shape(20, 1, 16, 8, 4)) return 1;
   const int grids[][2] = {{2, 2},   {3, 5},    {5, 3},    {40, 20},  {20, 40},   {160, 80}, {7, 33},
                           {33, 97}, {2, 512},  {512, 2},  {96, 48},  {640, 320}, {512, 128}, {64, 512},
                           {1000, 7}, {7, 1000}, {1280, 512}};
