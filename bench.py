@@ -366,6 +366,17 @@ def run_gpu(args, world, rank, local) -> None:
                 "flops_per_cell": FLOPS_PREPARE}
     else:
         fp64 = {"peak_tflops": rate.value, "peak_source": "measured (bs_fp64_fma_rate)"}
+    # The sweep is bound by its dependent diagonal steps, not by HBM: the
+    # steps of one launch (forward and backward over ni + nj - 1 diagonals
+    # of the widest case) and the SM cycles each took, at the median SM clock
+    # sampled during the timed region.
+    g0 = cases[0].config.grid
+    diag_steps = 2 * (g0.ni + g0.nj - 1)
+    latency = {"kernel": "lusgs_sweep", "diagonal_steps_per_launch": diag_steps,
+               "ns_per_diagonal_step": 1e6 * sweep_ms / diag_steps}
+    mhz = (clock_info or {}).get("sm_mhz")
+    if mhz:
+        latency["cycles_per_diagonal_step"] = latency["ns_per_diagonal_step"] * mhz / 1000
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
@@ -404,7 +415,7 @@ def run_gpu(args, world, rank, local) -> None:
                          "kernel_ms": {k: v[0] for k, v in kernels.items()},
                          "bytes_per_cell": {"lusgs_sweep": BYTES_SWEEP, "lusgs_prepare": BYTES_PREPARE,
                                             "lusgs_update": BYTES_UPDATE},
-                         "fp64": fp64},
+                         "fp64": fp64, "latency": latency},
             "cpu_baseline": cpu,
             "clocks": clock_info,
             "accuracy": {"converged": converged, "lusgs_steps": steps_taken,
