@@ -97,6 +97,7 @@ SIGNATURES: dict[str, list] = {
     "bs_batch_set_tile_shape": [_vp, C.c_int32],
     "bs_batch_tuning": [_vp, _ip, _ip, _ip, _ip, _ip],
     "bs_batch_set_update_mode": [_vp, C.c_int32],
+    "bs_batch_set_lanes": [_vp, C.c_int32],
     "bs_batch_update_mode": [_vp, _ip],
     "bs_batch_set_metric_precision": [_vp, C.c_int32],
     "bs_batch_forebody_drag": [_vp, C.c_int32, C.c_double, C.c_double, C.c_double, _dp],

@@ -12,6 +12,12 @@ from .config import Euler2DConfig, FreeStream
 _dp = C.POINTER(C.c_double)
 
 
+# The autotuner's choices per grid-size class (CudaBatch.size_class), kept for
+# the life of the process: a later batch of the same class applies them
+# instead of timing its candidates again.
+_TUNED: dict[tuple, tuple[dict, float]] = {}
+
+
 class CudaBatch:
     def __init__(self, configs: list[Euler2DConfig], precision: int = 64):
         self._lib = _native.load()
@@ -153,15 +159,41 @@ class CudaBatch:
             raise ValueError("one flag per case")
         self._call("bs_batch_set_active", f.ctypes.data_as(C.POINTER(C.c_int32)))
 
+    def size_class(self, method: str = "lusgs") -> tuple:
+        """The batch's grid-size class for the autotuner's cache: the method,
+        the widest case's ni and nj, and the case count rounded up to a power
+        of two."""
+        ni = max(c.grid.ni for c in self.configs)
+        nj = max(c.grid.nj for c in self.configs)
+        return (method, ni, nj, 1 << max(0, (self.n - 1).bit_length()))
+
     def autotune(self, method: str = "lusgs", steps: int = 40, cfl: float = 5.0,
-                 omega: float = 1.5) -> tuple[int, float]:
-        """Chooses the number of lanes by timing `steps` steps with each
-        candidate (the state is unchanged); returns (lanes, ms per step)."""
+                 omega: float = 1.5, cache: bool = False) -> tuple[int, float]:
+        """Chooses the number of lanes, the residual pass's tile shape and
+        (LU-SGS) the update mode by timing `steps` steps with each candidate
+        (the state is unchanged); returns (lanes, ms per step). With `cache`,
+        a batch of a grid-size class tuned before in this process takes the
+        stored choice without timing (ms per step is then the stored one)."""
+        key = self.size_class(method)
+        if cache and key in _TUNED:
+            t, ms_stored = _TUNED[key]
+            self.set_lanes(t["lanes"])
+            self.set_tile_shape(t["tile_shape"])
+            if method == "lusgs":
+                self.set_update_mode(t["fused_update"])
+            return t["lanes"], ms_stored
         lanes = C.c_int32()
         ms = C.c_double()
         self._call("bs_batch_autotune", 1 if method == "lusgs" else 0, steps, cfl, omega,
                    C.byref(lanes), C.byref(ms))
+        if cache:
+            _TUNED[key] = (self.tuning(), ms.value)
         return lanes.value, ms.value
+
+    def set_lanes(self, lanes: int) -> None:
+        """The number of lanes, as the autotuner would set it
+        (bs_batch_set_lanes)."""
+        self._call("bs_batch_set_lanes", int(lanes))
 
     def kernel_times(self, method: str = "lusgs", cfl: float = 5.0, omega: float = 1.5,
                      iterations: int = 20) -> tuple[float, float, float]:

@@ -412,6 +412,10 @@ bs_status bs_batch_tuning(bs_batch* batch, int32_t* lanes, int32_t* shape, int32
   });
 }
 
+bs_status bs_batch_set_lanes(bs_batch* batch, int32_t lanes) {
+  BS_BATCH_CALL(batch, { return batch->solver->set_lanes(lanes); });
+}
+
 bs_status bs_batch_set_update_mode(bs_batch* batch, int32_t fused) {
   BS_BATCH_CALL(batch, {
     if (fused != 0 && fused != 1) return bs::fail(BS_INVALID_ARGUMENT, "update mode: 1 fused, 0 separate");

@@ -590,6 +590,13 @@ class Solver final : public SolverBase {
 
   int lanes() const override { return std::max<int>(1, int(lanes_.size())); }
 
+  bs_status set_lanes(int lanes) override {
+    if (lanes < 1 || lanes > std::min(n_, kMaxLanes))
+      return fail(BS_INVALID_ARGUMENT, "lanes: 1 .. " + std::to_string(std::min(n_, kMaxLanes)));
+    release_lanes();
+    return init_lanes(hc_, lanes);
+  }
+
   bs_status flow_field(int c, int field, const bs_primitive& free, double length, double* out) override {
     if (field < bsd::FIELD_SCHLIEREN || field > bsd::FIELD_DENSITY)
       return fail(BS_INVALID_ARGUMENT, "field: 0 schlieren, 1 mach, 2 cp, 3 density");

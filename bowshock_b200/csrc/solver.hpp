@@ -71,6 +71,8 @@ class SolverBase {
   virtual bs_status autotune(int method, int steps, double cfl, double omega, int* lanes,
                              double* ms_per_step) = 0;
   virtual int lanes() const = 0;
+  // Sets the number of lanes (1 .. min(cases, 64)), as autotune would.
+  virtual bs_status set_lanes(int lanes) = 0;
   // Which cases later iterate calls advance (1 active, 0 frozen); a solve
   // sets its own.
   virtual bs_status set_active(const int* flags) = 0;

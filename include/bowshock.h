@@ -412,6 +412,10 @@ BS_API bs_status bs_batch_set_tile_shape(bs_batch *batch, int32_t shape);
  * along i and j and its threads. */
 BS_API bs_status bs_batch_tuning(bs_batch *batch, int32_t *lanes, int32_t *shape, int32_t *tile_i,
                                  int32_t *tile_j, int32_t *threads);
+/* Sets the number of lanes (concurrent groups of cases, each on its own
+ * stream), 1 .. min(cases, 64), as bs_batch_autotune would choose it: for a
+ * caller that applies a choice it tuned before on a batch of the same kind. */
+BS_API bs_status bs_batch_set_lanes(bs_batch *batch, int32_t lanes);
 /* How the batch's LU-SGS steps apply their update: 1 (the default) inside
  * the next step's residual pass as it reads each cell, halo cells included
  * (two launches a step); 0 by a separate kernel after each sweep (three

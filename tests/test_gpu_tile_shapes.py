@@ -115,3 +115,35 @@ def test_autotune_picks_a_shape_and_keeps_the_state():
             assert np.array_equal(b.primitives(k), before[k])
     finally:
         b.destroy()
+
+
+def test_autotune_cache_applies_a_grid_size_class_choice():
+    # A batch of a class tuned before takes the stored lanes, tile shape and
+    # update mode instead of timing them, and steps to the same state as an
+    # untuned batch.
+    from bowshock_b200 import abi, batch as batch_module
+
+    cs = cases()
+    first = CudaBatch([c.config for c in cs], precision=64)
+    try:
+        first.set_free_stream()
+        batch_module._TUNED.pop(first.size_class("lusgs"), None)
+        first.autotune("lusgs", 20, cache=True)
+        chosen = first.tuning()
+    finally:
+        first.destroy()
+    assert first.size_class("lusgs") in batch_module._TUNED
+    ref = states_after(-1, "lusgs")
+    second = CudaBatch([c.config for c in cs], precision=64)
+    try:
+        second.set_free_stream()
+        second.autotune("lusgs", 20, cache=True)
+        assert second.tuning() == chosen
+        res = second.solve("lusgs", 1e-14, max_steps=40, check_every=20)
+        assert all(r.steps == 40 for r in res)
+        for k in range(len(cs)):
+            assert np.array_equal(second.primitives(k), ref[k])
+        for bad in (0, len(cs) + 1):
+            assert second._lib.bs_batch_set_lanes(second._h, bad) == abi.BS_INVALID_ARGUMENT
+    finally:
+        second.destroy()
