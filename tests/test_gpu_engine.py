@@ -232,6 +232,32 @@ def test_lusgs_step_matches_the_oracle_early_on():
     assert np.max(np.abs(w - wc)) < 1e-5
 
 
+@pytest.mark.parametrize("ni, nj", [(48, 512), (40, 481)])
+def test_lusgs_steps_on_grids_512_rows_wide_match_the_oracle(ni, nj):
+    # The widest cases the sweep takes: 16 consumer warps (512 rows), and 15
+    # full warps and one of a single row (481), with a pulse and a variation
+    # along j so that every row's residual is not zero.
+    height = 2.0 * nj / ni
+    grid = distorted_grid(ni, nj, 0, 2, 0, height)
+    cfg = Euler2DConfig(grid=grid, geometry="planar", gamma=GAMMA, flux="hllc", limiter="vanAlbada",
+                        reconstruction="perVariable", time_integrator="ssprk2", cfl=0.6,
+                        time_stepping="local", boundaries=all_sides(Boundary("outflow")))
+
+    def field(x, y):
+        return Primitive2D(1.0 + 0.05 * math.sin(6 * y / height), 0.3, 0.1,
+                           1 + 0.3 * math.exp(-8 * ((x - 1) ** 2 + (y - height / 2) ** 2)))
+
+    o = OracleEuler2D(cfg)
+    o.set_initial_condition(lambda x, y: tuple(field(x, y).__dict__.values()))
+    o.iterate_implicit(5, 5.0)
+    with CudaEuler2D(cfg, 64) as e:
+        e.set_primitives(field_primitives(e, field))
+        e.iterate_implicit(5, 5.0)
+        w = e.primitives()
+    wc = o.primitives().reshape(-1, 4)
+    assert np.max(np.abs(w - wc)) < 1e-5
+
+
 def test_config1_converges_to_1e6_with_the_oracle_drag():
     cfg, free, body = config1()
     with CudaEuler2D(cfg, 64) as e:
