@@ -232,6 +232,22 @@ def test_lusgs_step_matches_the_oracle_early_on():
     assert np.max(np.abs(w - wc)) < 1e-5
 
 
+def test_fp32_engine_lusgs_steps_match_the_fp32_oracle():
+    # The all-FP32 engine (the reference GPU engine's arithmetic) through the
+    # same residual pass, records and sweep: five LU-SGS steps against the
+    # oracle's FP32 instantiation, to FP32 rounding.
+    cfg, free, _ = config1(40, 20)
+    o = OracleEuler2D(cfg, 32)
+    o.set_uniform(free.state)
+    o.iterate_implicit(5, 5.0)
+    with CudaEuler2D(cfg, 32) as e:
+        e.set_uniform(free.state)
+        e.iterate_implicit(5, 5.0)
+        w = e.primitives()
+    wc = o.primitives().reshape(-1, 4)
+    assert np.max(np.abs(w - wc)) < 1e-4
+
+
 @pytest.mark.parametrize("ni, nj", [(48, 512), (40, 481)])
 def test_lusgs_steps_on_grids_512_rows_wide_match_the_oracle(ni, nj):
     # The widest cases the sweep takes: 16 consumer warps (512 rows), and 15
